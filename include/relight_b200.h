@@ -1,0 +1,232 @@
+/*
+ * relight_b200 — C ABI of the B200 (sm_100a) lightmap baker.
+ *
+ * This is the drop-in boundary for Relight's ray-bound bake passes.  Every
+ * entry point replaces one reference interface, cited beside it
+ * (dmsovetov/Relight, path:line).  Signatures use plain pointers, sizes and
+ * opaque handles only.  Every call returns an int status (RL_OK = 0), and
+ * rl_last_error() gives the message of the calling thread's last failure.
+ * No exception crosses the ABI.
+ *
+ * Memory: an rl_scene owns the device copy of the geometry and its BVH.  An
+ * rl_map owns the device lumel arrays of one lightmap, photonmap or
+ * radiancemap.  Host pointers passed in are borrowed for the duration of the
+ * call only.  Device pointers (`d_*`) stay owned by the caller.
+ *
+ * Streams: `stream` is a cudaStream_t (NULL = legacy default stream).  Work is
+ * enqueued on it, so a call may return before its kernels finish.  The calls
+ * that return data in host memory (rl_map_download, rl_ff_*,
+ * rl_radiosity_solve) synchronise the stream.  One handle must not be used
+ * from two threads at once.
+ */
+#ifndef RELIGHT_B200_H
+#define RELIGHT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------ status */
+
+/* RelightStatus (Relight.h:82-86) plus the errors a GPU call can raise. */
+enum {
+    RL_OK = 0,              /* RelightSuccess */
+    RL_INVALID_CALL = 1,    /* RelightInvalidCall: bad handle/argument or state */
+    RL_NOT_IMPLEMENTED = 2, /* RelightNotImplemented */
+    RL_OUT_OF_MEMORY = 3,
+    RL_CUDA_ERROR = 4,
+    RL_CAPACITY = 5         /* an output did not fit the caller's capacity */
+};
+
+/* rt::HitFlags (rt/Tracer.h:65-72). */
+enum {
+    RL_HIT_POINT = 1,
+    RL_HIT_UV = 2,
+    RL_HIT_COLOR = 4,
+    RL_HIT_NORMAL = 8,
+    RL_HIT_USE_ALPHA = 16,
+    RL_HIT_ALL = 15
+};
+
+/* Message of the calling thread's last failed call ("" if none). */
+int rl_last_error(char* buf, size_t len);
+/* Library version string and the device the library was built for. */
+const char* rl_version(void);
+
+/* ------------------------------------------------------------- scene */
+
+/* The flat scene: all meshes concatenated, in scene space (after
+   Scene::addMesh's Mesh::transformed, scene/Scene.cpp:98-107).  Replaces
+   the per-mesh registration of rt::Embree::addMesh (rt/Embree.cpp:180-217):
+   geometry id = mesh index, primitive id = face index within the mesh. */
+typedef struct {
+    int32_t nverts;
+    const float* pos;          /* [nverts][3] Vertex::position */
+    const float* nrm;          /* [nverts][3] Vertex::normal */
+    const float* uv0;          /* [nverts][2] Vertex::uv[Diffuse] */
+    const float* uv1;          /* [nverts][2] Vertex::uv[Lightmap] */
+    const int32_t* vmat;       /* [nverts] material index or -1 (Vertex::material) */
+    int32_t ntris;
+    const int32_t* tris;       /* [ntris][3] global vertex ids in index-buffer order */
+    int32_t nmeshes;
+    const int32_t* mesh_first_tri;  /* [nmeshes + 1] */
+    const int32_t* mesh_lightmap;   /* [nmeshes] lightmap slot or -1 (Mesh::lightmap) */
+    const int32_t* mesh_photonmap;  /* [nmeshes] photonmap slot or -1 (Mesh::photonmap) */
+    int32_t nmats;
+    const float* mat_rgb;      /* [nmats][3] Material::color */
+    const int32_t* mat_tex;    /* [nmats] texture index or -1 (TexturedMaterial) */
+    int32_t ntex;
+    const int32_t* tex_dims;   /* [ntex][3] width, height, channels (3 or 4) */
+    const int64_t* tex_offset; /* [ntex] byte offset into tex_pixels */
+    const uint8_t* tex_pixels;
+    float bounds_lo[3];        /* Scene::bounds() (scene/Scene.cpp:81-88) */
+    float bounds_hi[3];
+} rl_scene_desc;
+
+/* A light with its model objects (scene/Light.h:228-336). */
+typedef struct {
+    int32_t influence;        /* 0 none, 1 LightInfluence, 2 DirectionalLightInfluence */
+    int32_t casts_shadow;
+    float position[3];
+    float color[3];
+    float intensity;
+    float direction[3];       /* directional influence / emitter direction */
+    int32_t attenuation;      /* 0 none, 1 LinearLightAttenuation */
+    float att_radius, att_const, att_linear, att_quadratic;
+    int32_t cutoff;           /* 0 none, 1 LightCutoff, 2 LightSpotCutoff */
+    float spot_direction[3];
+    float spot_cutoff, spot_exponent;
+    int32_t emitter;          /* 0 none, 1 PhotonEmitter, 2 DirectionalPhotonEmitter */
+    float emitter_plane[4];   /* DirectionalPhotonEmitter plane: normal, distance */
+    int32_t vertex_first;     /* LightVertexGenerator samples in the light-vertex pool */
+    int32_t vertex_count;     /* 0 = no vertex generator */
+} rl_light;
+
+typedef struct rl_scene rl_scene;
+
+/* Scene::end -> new rt::Embree; addMesh...; rtcCommit (scene/Scene.cpp:122-142,
+   rt/Embree.cpp:49-58): upload the geometry and build the BVH on the device.
+   `builder`: 0 = binned SAH (host), 1 = LBVH (device). */
+int rl_scene_create(const rl_scene_desc* desc, int builder, void* stream, rl_scene** out);
+int rl_scene_destroy(rl_scene* scene);
+/* BVH statistics: node count, leaf count, max depth, SAH cost. */
+int rl_scene_bvh_stats(const rl_scene* scene, int64_t* nodes, int64_t* leaves, int32_t* depth, double* sah);
+
+/* ------------------------------------------------------------ tracing */
+
+/* rt::ITracer::traceSegment (rt/Tracer.h:87; rt::Embree::traceSegment +
+   initializeRay, rt/Embree.cpp:107-177) for a batch of segments:
+   closest hit on (0.01, |end - start|), with the reference's hit
+   post-processing (point = start + dir * t, Barycentric(u, v) attribute
+   interpolation, HitUseAlpha restarts).  Device arrays:
+     d_seg     [n][6]  start xyz, end xyz
+     d_hit     [n]     1 hit / 0 miss
+     d_t_uv    [n][3]  t, u, v of the final segment (may be NULL)
+     d_mesh_face [n][2] mesh, face (-1 on a miss) (may be NULL)
+     d_point, d_normal [n][3], d_rgba [n][4], d_uv [n][2] (may be NULL) */
+int rl_trace_segments(const rl_scene* scene, int64_t n, const float* d_seg, int flags, int32_t* d_hit,
+                      float* d_t_uv, int32_t* d_mesh_face, float* d_point, float* d_normal, float* d_rgba,
+                      float* d_uv, void* stream);
+
+/* ----------------------------------------------------------- lumel maps */
+
+typedef struct rl_map rl_map;
+
+/* Relight::createLightmap / createPhotonmap (Relight.cpp:193-202); kind
+   0 = Lightmap, 1 = Photonmap, 2 = Radiancemap (Lightmap.h:58-184). */
+int rl_map_create(int kind, int width, int height, rl_map** out);
+int rl_map_destroy(rl_map* map);
+/* Lightmap::addMesh / Photonmap::addMesh -> initializeLumels
+   (Lightmap.cpp:93-164, 360-373): rasterise the mesh's faces into lumels
+   (last face wins).  Call once per mesh, in the reference's addMesh order. */
+int rl_map_add_mesh(rl_map* map, const rl_scene* scene, int mesh, void* stream);
+/* Lumel read-back / upload (Lightmap::lumels(), Lightmap.cpp:55-58, and
+   toHdr(), :332-349).  Host arrays [w*h] or [w*h][3]; any may be NULL. */
+int rl_map_download(const rl_map* map, int32_t* flags, int32_t* face, float* position, float* normal, float* color,
+                    int32_t* photons, float* gathered, void* stream);
+int rl_map_upload(rl_map* map, const int32_t* flags, const int32_t* face, const float* position,
+                  const float* normal, const float* color, const int32_t* photons, const float* gathered,
+                  void* stream);
+/* Set every lumel colour / photon accumulator to zero. */
+int rl_map_clear(rl_map* map, int colors, int photons, void* stream);
+/* Device pointers of the lumel arrays (SoA, [w*h] or [w*h][3]); any may be NULL. */
+int rl_map_device_arrays(const rl_map* map, int32_t** flags, float** position, float** normal, float** color,
+                         int32_t** photons, float** gathered);
+/* Number of valid lumels (after rl_map_add_mesh). */
+int rl_map_valid_count(const rl_map* map, int64_t* count);
+
+/* --------------------------------------------------------------- passes */
+
+/* Relight::bakeDirectLight with LumelBakeIterator(first, step)
+   (Relight.cpp:216-227; baker/DirectLight.cpp:46-125;
+   scene/Light.cpp:372-500).  Adds every light's influence to the lumel
+   colours.  `lights` and `light_vertices` ([nverts][3]) are host arrays. */
+int rl_bake_direct(const rl_scene* scene, rl_map* lightmap, const rl_light* lights, int nlights,
+                   const float* light_vertices, int nlight_vertices, int first, int step, void* stream);
+
+/* Relight::bakeAmbientOcclusion (Relight.cpp:260-271;
+   baker/AmbientOcclusion.cpp:46-66): colour *= 1 - occluded/(samples*fraction),
+   optionally raised to `exponent`.  Directions are Philox-keyed by (seed,
+   lumel index, sample). */
+int rl_bake_ao(const rl_scene* scene, rl_map* lightmap, int samples, float occluded_fraction, float max_distance,
+               float exponent, uint64_t seed, int first, int step, void* stream);
+
+/* Relight::emitPhotons minus the gather (Relight.cpp:244-250;
+   baker/Photons.cpp:50-144; scene/Light.cpp:334-361): trace
+   pass_count x sum_l int(intensity*25000) photons and deposit colour+count
+   into each hit mesh's photonmap (maps[] indexed by the scene's photonmap
+   slot).  *stored (host, may be NULL) receives the deposit count. */
+int rl_emit_photons(const rl_scene* scene, rl_map* const* photonmaps, int nmaps, const rl_light* lights,
+                    int nlights, int pass_count, int max_depth, float energy_threshold, float max_distance,
+                    uint64_t seed, int64_t* stored, void* stream);
+
+/* Photonmap::gather(radius) (Lightmap.cpp:376-413), the loop-bound quirk
+   of :379 included. */
+int rl_photonmap_gather(rl_map* photonmap, int radius, void* stream);
+
+/* Relight::bakeIndirectLight (Relight.cpp:230-241;
+   baker/IndirectLight.cpp:47-75): final gather against the gathered
+   photonmaps (maps[] by photonmap slot). */
+int rl_bake_indirect(const rl_scene* scene, rl_map* lightmap, rl_map* const* photonmaps, int nmaps, int samples,
+                     float max_distance, const float sky[3], const float ambient[3], uint64_t seed, int first,
+                     int step, void* stream);
+
+/* ------------------------------------------------------------- radiosity */
+
+/* RadiosityBuilder::computeFormFactors + distanceFormFactor +
+   refineFormFactors with maxFormFactors = 0
+   (radiosity/RadiosityBuilder.cpp:99-176): pairwise point-to-point form
+   factors over `n` patches (device arrays d_pos, d_nrm [n][3]), visibility
+   by segment, each row normalised to sum 1.  Output CSR in host memory,
+   columns ascending (the reference's list order).  Call with cols == NULL
+   to get *nnz only; then with arrays of that capacity. */
+int rl_ff_pairwise(const rl_scene* scene, int n, const float* d_pos, const float* d_nrm, float threshold,
+                   int64_t* row_ptr, int32_t* cols, float* vals, int64_t capacity, int64_t* nnz, void* stream);
+
+/* Hemisphere-cast form factors (no reference counterpart; cosine-weighted
+   variant of the form factors above): `rays` cosine-distributed rays per
+   patch; F_ij = (rays from i whose hit maps to patch j) / rays.  A hit maps
+   to a patch through the hit mesh's map (mesh_map[mesh], map_dims[map] =
+   w,h), the lumel at the hit's lightmap uv (Lightmap::lumel(const Uv&),
+   Lightmap.cpp:61-67) and patch_of_texel[map_base[map] + texel] (-1 none).
+   All arrays are host arrays.  Output CSR as for rl_ff_pairwise. */
+int rl_ff_hemisphere(const rl_scene* scene, int n, const float* d_pos, const float* d_nrm, int rays,
+                     float max_distance, uint64_t seed, const int32_t* mesh_map, int nmaps, const int32_t* map_dims,
+                     const int64_t* map_base, const int32_t* patch_of_texel, int64_t ntexels, int64_t* row_ptr,
+                     int32_t* cols, float* vals, int64_t capacity, int64_t* nnz, void* stream);
+
+/* Radiosity gather iterations (RadiositySolver::solve is an empty stub,
+   radiosity/RadiositySolver.cpp:34-36; the gather math is the legacy
+   cRadiositySolver::Solve, src/relight/Radiosity.cpp:130-146, iterated):
+   B <- E + rho .* (F B) over RGB, B0 = E, `iters` Jacobi steps.  CSR and
+   vectors are device arrays; d_B [n][3] receives the result. */
+int rl_radiosity_solve(int n, const int64_t* d_row_ptr, const int32_t* d_cols, const float* d_vals,
+                       const float* d_E, const float* d_rho, int iters, float* d_B, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RELIGHT_B200_H */

@@ -1,0 +1,21 @@
+// BVH construction for the B200 traversal kernels.
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+namespace rl {
+
+struct BvhBuild {
+    std::vector<float> nodes;  // 16 floats per node (four float4, see rl_device.cuh)
+    std::vector<float> tris;   // 12 floats per triangle in leaf order (three float4)
+    int64_t leaves = 0;
+    int depth = 0;
+    double sah = 0.0;
+};
+
+// Binned-SAH build over `ntris` triangles given as three vertex ids into
+// `pos` ([nverts][3]); triangle ids are the global ids (position in `tris`).
+bool build_bvh_sah(const float* pos, int nverts, const int32_t* tris, int ntris, BvhBuild& out, const char** err);
+
+}  // namespace rl

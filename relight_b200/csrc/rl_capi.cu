@@ -1,0 +1,1252 @@
+// C ABI and pass kernels of the B200 lightmap baker (include/relight_b200.h).
+//
+// Kernel map (reference function -> kernel):
+//   rt::Embree::traceSegment           k_trace_segments
+//   Lightmap::initializeLumels         k_raster_owner + k_raster_init
+//   DirectLight::bakeLumel             k_direct
+//   AmbientOcclusion::bakeLumel        k_ao
+//   Photons::emit/trace/store          k_photons
+//   Photonmap::gather                  k_gather
+//   IndirectLight::bakeLumel           k_indirect
+//   RadiosityBuilder form factors      k_ff_pairs (+ host CSR assembly)
+//   hemisphere form factors            k_ff_hemi_rays + k_ff_hemi_rle + k_ff_hemi_compact
+//   radiosity gather iterations        k_jacobi
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/relight_b200.h"
+#include "rl_bvh.h"
+#include "rl_device.cuh"
+
+using namespace rl;
+
+// ------------------------------------------------------------ errors
+
+namespace {
+
+thread_local std::string g_error;
+
+int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_error = buf;
+    return code;
+}
+
+#define CK(call)                                                                                   \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess)                                                                     \
+            return fail(e_ == cudaErrorMemoryAllocation ? RL_OUT_OF_MEMORY : RL_CUDA_ERROR,        \
+                        "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+    } while (0)
+
+#define CK_LAUNCH(name)                                                                            \
+    do {                                                                                           \
+        cudaError_t e_ = cudaGetLastError();                                                       \
+        if (e_ != cudaSuccess)                                                                     \
+            return fail(RL_CUDA_ERROR, "launch of %s failed: %s", name, cudaGetErrorString(e_));   \
+    } while (0)
+
+inline cudaStream_t S(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+inline unsigned blocks_for(long long n, int threads) { return (unsigned)((n + threads - 1) / threads); }
+
+template <typename T>
+int dalloc(T** p, size_t count) {
+    *p = nullptr;
+    if (count == 0) return RL_OK;
+    CK(cudaMalloc((void**)p, sizeof(T) * count));
+    return RL_OK;
+}
+
+template <typename T>
+int dupload(T** p, const T* host, size_t count, cudaStream_t st) {
+    int rc = dalloc(p, count);
+    if (rc) return rc;
+    if (count && host) CK(cudaMemcpyAsync(*p, host, sizeof(T) * count, cudaMemcpyHostToDevice, st));
+    return RL_OK;
+}
+
+// A stream-ordered scratch buffer freed when it goes out of scope.
+struct Scratch {
+    void* p = nullptr;
+    cudaStream_t st = nullptr;
+    ~Scratch() {
+        if (p) cudaFreeAsync(p, st);
+    }
+};
+
+template <typename T>
+int scratch(Scratch& s, T** out, size_t count, cudaStream_t st) {
+    s.st = st;
+    *out = nullptr;
+    if (count == 0) return RL_OK;
+    CK(cudaMallocAsync(&s.p, sizeof(T) * count, st));
+    *out = (T*)s.p;
+    return RL_OK;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------- handles
+
+struct rl_scene {
+    DevScene dev{};
+    std::vector<void*> owned;
+    int* d_status = nullptr;  // bit 0: traversal stack overflow
+    int64_t nnodes = 0, leaves = 0;
+    int depth = 0;
+    double sah = 0.0;
+    int nmeshes = 0;
+    std::vector<int> mesh_first_tri;
+    std::vector<int> mesh_photonmap;
+    ~rl_scene() {
+        for (void* p : owned) cudaFree(p);
+        if (d_status) cudaFree(d_status);
+    }
+};
+
+struct rl_map {
+    int kind = 0;
+    DevMap dev{};
+    int* d_owner = nullptr;  // rasterisation scratch: winning face per texel
+    ~rl_map() {
+        cudaFree(dev.flags); cudaFree(dev.face); cudaFree(dev.position); cudaFree(dev.normal);
+        cudaFree(dev.color); cudaFree(dev.photons); cudaFree(dev.gathered); cudaFree(d_owner);
+    }
+};
+
+extern "C" int rl_last_error(char* buf, size_t len) {
+    if (buf && len) {
+        snprintf(buf, len, "%s", g_error.c_str());
+    }
+    return (int)g_error.size();
+}
+
+extern "C" const char* rl_version(void) { return "relight_b200 0.1 (sm_100a)"; }
+
+// ------------------------------------------------------------- scene
+
+extern "C" int rl_scene_create(const rl_scene_desc* d, int builder, void* stream, rl_scene** out) {
+    if (!d || !out) return fail(RL_INVALID_CALL, "rl_scene_create: null argument");
+    *out = nullptr;
+    if (d->ntris < 0 || d->nverts < 0 || d->nmeshes < 0) return fail(RL_INVALID_CALL, "negative counts");
+    if (d->ntris > 0 && (!d->pos || !d->tris || !d->mesh_first_tri))
+        return fail(RL_INVALID_CALL, "rl_scene_create: missing geometry arrays");
+    if (d->nmeshes > 0 && d->mesh_first_tri[d->nmeshes] != d->ntris)
+        return fail(RL_INVALID_CALL, "mesh_first_tri[nmeshes] must equal ntris");
+    if (builder != 0) return fail(RL_NOT_IMPLEMENTED, "only the binned-SAH builder (0) is available");
+    cudaStream_t st = S(stream);
+    rl_scene* s = new (std::nothrow) rl_scene;
+    if (!s) return fail(RL_OUT_OF_MEMORY, "host allocation failed");
+    BvhBuild b;
+    const char* err = "";
+    if (!build_bvh_sah(d->pos, d->nverts, d->tris, d->ntris, b, &err)) {
+        delete s;
+        return fail(RL_INVALID_CALL, "BVH build: %s", err);
+    }
+    s->nnodes = (int64_t)(b.nodes.size() / 16);
+    s->leaves = b.leaves;
+    s->depth = b.depth;
+    s->sah = b.sah;
+    if (b.depth >= kStackSize - 1) {
+        delete s;
+        return fail(RL_NOT_IMPLEMENTED, "BVH depth %d exceeds the traversal stack", b.depth);
+    }
+    // per-triangle vertex ids + mesh
+    std::vector<int4> vidx(d->ntris);
+    for (int m = 0; m < d->nmeshes; m++)
+        for (int t = d->mesh_first_tri[m]; t < d->mesh_first_tri[m + 1]; t++)
+            vidx[t] = make_int4(d->tris[3 * t], d->tris[3 * t + 1], d->tris[3 * t + 2], m);
+    int has_alpha = 0;
+    for (int m = 0; m < d->nmats; m++) {
+        int t = d->mat_tex ? d->mat_tex[m] : -1;
+        if (t >= 0 && d->tex_dims[3 * t + 2] == 4) has_alpha = 1;
+    }
+    std::vector<int> mat_tex(d->mat_tex ? d->mat_tex : nullptr, d->mat_tex ? d->mat_tex + d->nmats : nullptr);
+    if (mat_tex.empty()) mat_tex.assign(d->nmats, -1);
+    std::vector<int> vmat(d->vmat ? d->vmat : nullptr, d->vmat ? d->vmat + d->nverts : nullptr);
+    if (vmat.empty()) vmat.assign(d->nverts, -1);
+    std::vector<float> zeros2(2 * (size_t)d->nverts, 0.0f);
+    std::vector<float> zeros3(d->nrm ? 0 : 3 * (size_t)d->nverts, 0.0f);
+    std::vector<int> pmap(d->mesh_photonmap ? d->mesh_photonmap : nullptr,
+                          d->mesh_photonmap ? d->mesh_photonmap + d->nmeshes : nullptr);
+    if (pmap.empty()) pmap.assign(d->nmeshes, -1);
+    s->mesh_first_tri.assign(d->mesh_first_tri, d->mesh_first_tri + d->nmeshes + 1);
+    s->mesh_photonmap = pmap;
+    s->nmeshes = d->nmeshes;
+
+    int rc = RL_OK;
+    auto up = [&](auto** dst, const auto* src, size_t count) {
+        if (rc) return;
+        rc = dupload(dst, src, count, st);
+        if (!rc && *dst) s->owned.push_back((void*)*dst);
+    };
+    float4* nodes = nullptr; float4* tris = nullptr; int4* dvidx = nullptr;
+    float *pos = nullptr, *nrm = nullptr, *uv0 = nullptr, *uv1 = nullptr, *mat_rgb = nullptr;
+    int *dvmat = nullptr, *first = nullptr, *dpmap = nullptr, *dmat_tex = nullptr, *tex_dims = nullptr;
+    long long* tex_off = nullptr;
+    unsigned char* tex_px = nullptr;
+    up(&nodes, (const float4*)b.nodes.data(), b.nodes.size() / 4);
+    up(&tris, (const float4*)b.tris.data(), b.tris.size() / 4);
+    up(&dvidx, vidx.data(), vidx.size());
+    up(&pos, d->pos, 3 * (size_t)d->nverts);
+    up(&nrm, d->nrm ? d->nrm : zeros3.data(), 3 * (size_t)d->nverts);
+    up(&uv0, d->uv0 ? d->uv0 : zeros2.data(), 2 * (size_t)d->nverts);
+    up(&uv1, d->uv1 ? d->uv1 : zeros2.data(), 2 * (size_t)d->nverts);
+    up(&dvmat, vmat.data(), vmat.size());
+    up(&first, d->mesh_first_tri, (size_t)d->nmeshes + 1);
+    up(&dpmap, pmap.data(), pmap.size());
+    up(&mat_rgb, d->mat_rgb, 3 * (size_t)d->nmats);
+    up(&dmat_tex, mat_tex.data(), mat_tex.size());
+    if (d->ntex > 0) {
+        up(&tex_dims, d->tex_dims, 3 * (size_t)d->ntex);
+        up(&tex_off, (const long long*)d->tex_offset, (size_t)d->ntex);
+        size_t bytes = 0;
+        for (int t = 0; t < d->ntex; t++)
+            bytes = std::max(bytes, (size_t)d->tex_offset[t] + (size_t)d->tex_dims[3 * t] * d->tex_dims[3 * t + 1] *
+                                        d->tex_dims[3 * t + 2]);
+        up(&tex_px, d->tex_pixels, bytes);
+    }
+    if (!rc) {
+        cudaError_t e = cudaMalloc(&s->d_status, sizeof(int));
+        if (e == cudaSuccess) e = cudaMemsetAsync(s->d_status, 0, sizeof(int), st);
+        if (e != cudaSuccess) rc = fail(RL_CUDA_ERROR, "status word: %s", cudaGetErrorString(e));
+    }
+    if (!rc) {
+        cudaError_t e = cudaStreamSynchronize(st);  // host staging vectors die at return
+        if (e != cudaSuccess) rc = fail(RL_CUDA_ERROR, "scene upload: %s", cudaGetErrorString(e));
+    }
+    if (rc) {
+        delete s;
+        return rc;
+    }
+    DevScene& v = s->dev;
+    v.nodes = nodes; v.tris = tris; v.tri_vidx = dvidx;
+    v.pos = pos; v.nrm = nrm; v.uv0 = uv0; v.uv1 = uv1; v.vmat = dvmat;
+    v.mesh_first_tri = first; v.mesh_photonmap = dpmap;
+    v.mat_rgb = mat_rgb; v.mat_tex = dmat_tex; v.tex_dims = tex_dims; v.tex_offset = tex_off; v.tex_pixels = tex_px;
+    for (int k = 0; k < 3; k++) { v.bounds_lo[k] = d->bounds_lo[k]; v.bounds_hi[k] = d->bounds_hi[k]; }
+    v.ntris = d->ntris;
+    v.nmeshes = d->nmeshes;
+    v.has_alpha = has_alpha;
+    *out = s;
+    return RL_OK;
+}
+
+extern "C" int rl_scene_destroy(rl_scene* s) {
+    if (!s) return fail(RL_INVALID_CALL, "null scene");
+    cudaDeviceSynchronize();
+    delete s;
+    return RL_OK;
+}
+
+extern "C" int rl_scene_bvh_stats(const rl_scene* s, int64_t* nodes, int64_t* leaves, int32_t* depth, double* sah) {
+    if (!s) return fail(RL_INVALID_CALL, "null scene");
+    if (nodes) *nodes = s->nnodes;
+    if (leaves) *leaves = s->leaves;
+    if (depth) *depth = s->depth;
+    if (sah) *sah = s->sah;
+    return RL_OK;
+}
+
+static int check_status(const rl_scene* s, cudaStream_t st) {
+    int h = 0;
+    CK(cudaMemcpyAsync(&h, s->d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (h & 1) return fail(RL_CUDA_ERROR, "BVH traversal stack overflow (scene too deep)");
+    return RL_OK;
+}
+
+// ------------------------------------------------------------- tracing
+
+__global__ void k_trace_segments(DevScene s, long long n, const float* seg, int flags, int* hit, float* tuv,
+                                 int* mesh_face, float* point, float* normal, float* rgba, float* uv, int* status) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    SegHit r;
+    trace_segment(s, ld3(seg + 6 * i), ld3(seg + 6 * i + 3), flags, r, status);
+    hit[i] = r.hit ? 1 : 0;
+    if (tuv) { tuv[3 * i] = r.hit ? r.t : 0.f; tuv[3 * i + 1] = r.hit ? r.u : 0.f; tuv[3 * i + 2] = r.hit ? r.v : 0.f; }
+    if (mesh_face) { mesh_face[2 * i] = r.hit ? r.mesh : -1; mesh_face[2 * i + 1] = r.hit ? r.face : -1; }
+    if (point) st3(point + 3 * i, r.hit ? r.point : mk3(0.f, 0.f, 0.f));
+    if (normal) st3(normal + 3 * i, r.hit && (flags & kHitNormal) ? r.normal : mk3(0.f, 0.f, 0.f));
+    if (rgba) {
+        float4 c = r.hit && (flags & kHitColor) ? r.rgba : make_float4(0.f, 0.f, 0.f, 0.f);
+        rgba[4 * i] = c.x; rgba[4 * i + 1] = c.y; rgba[4 * i + 2] = c.z; rgba[4 * i + 3] = c.w;
+    }
+    if (uv) {
+        uv[2 * i] = r.hit && (flags & kHitUv) ? r.uv.x : 0.f;
+        uv[2 * i + 1] = r.hit && (flags & kHitUv) ? r.uv.y : 0.f;
+    }
+}
+
+extern "C" int rl_trace_segments(const rl_scene* s, int64_t n, const float* d_seg, int flags, int32_t* d_hit,
+                                 float* d_t_uv, int32_t* d_mesh_face, float* d_point, float* d_normal,
+                                 float* d_rgba, float* d_uv, void* stream) {
+    if (!s || (n > 0 && (!d_seg || !d_hit))) return fail(RL_INVALID_CALL, "rl_trace_segments: null argument");
+    if (n <= 0) return RL_OK;
+    k_trace_segments<<<blocks_for(n, 128), 128, 0, S(stream)>>>(s->dev, n, d_seg, flags, d_hit, d_t_uv,
+                                                                d_mesh_face, d_point, d_normal, d_rgba, d_uv,
+                                                                s->d_status);
+    CK_LAUNCH("k_trace_segments");
+    return RL_OK;
+}
+
+// ---------------------------------------------------------------- maps
+
+extern "C" int rl_map_create(int kind, int width, int height, rl_map** out) {
+    if (!out || width <= 0 || height <= 0 || kind < 0 || kind > 2)
+        return fail(RL_INVALID_CALL, "rl_map_create: bad arguments");
+    if ((long long)width * height > (1ll << 30)) return fail(RL_INVALID_CALL, "map too large");
+    rl_map* m = new (std::nothrow) rl_map;
+    if (!m) return fail(RL_OUT_OF_MEMORY, "host allocation failed");
+    m->kind = kind;
+    m->dev.width = width;
+    m->dev.height = height;
+    size_t n = (size_t)width * height;
+    int rc = RL_OK;
+    if (!rc) rc = dalloc(&m->dev.flags, n);
+    if (!rc) rc = dalloc(&m->dev.face, n);
+    if (!rc) rc = dalloc(&m->dev.position, 3 * n);
+    if (!rc) rc = dalloc(&m->dev.normal, 3 * n);
+    if (!rc) rc = dalloc(&m->dev.color, 3 * n);
+    if (!rc) rc = dalloc(&m->dev.photons, n);
+    if (!rc) rc = dalloc(&m->dev.gathered, 3 * n);
+    if (!rc) rc = dalloc(&m->d_owner, n);
+    if (rc) {
+        delete m;
+        return rc;
+    }
+    // Lumel::Lumel (Lightmap.h:52): faceIdx = (Index)-1, photons 0, flags 0, vectors 0
+    cudaMemset(m->dev.flags, 0, 4 * n);
+    cudaMemset(m->dev.face, 0, 4 * n);
+    cudaMemset(m->dev.position, 0, 12 * n);
+    cudaMemset(m->dev.normal, 0, 12 * n);
+    cudaMemset(m->dev.color, 0, 12 * n);
+    cudaMemset(m->dev.photons, 0, 4 * n);
+    cudaMemset(m->dev.gathered, 0, 12 * n);
+    cudaMemset(m->d_owner, 0xff, 4 * n);
+    std::vector<int> face(n, 0xffff);
+    cudaMemcpy(m->dev.face, face.data(), 4 * n, cudaMemcpyHostToDevice);
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) {
+        delete m;
+        return fail(RL_CUDA_ERROR, "map init: %s", cudaGetErrorString(e));
+    }
+    *out = m;
+    return RL_OK;
+}
+
+extern "C" int rl_map_destroy(rl_map* m) {
+    if (!m) return fail(RL_INVALID_CALL, "null map");
+    cudaDeviceSynchronize();
+    delete m;
+    return RL_OK;
+}
+
+// Face::isUvInside (scene/Mesh.cpp:415-438).
+__device__ __forceinline__ bool uv_inside(float2 a, float2 b, float2 c, float2 uv, float& bu, float& bv) {
+    float v0x = c.x - a.x, v0y = c.y - a.y;
+    float v1x = b.x - a.x, v1y = b.y - a.y;
+    float v2x = uv.x - a.x, v2y = uv.y - a.y;
+    float dot00 = v0x * v0x + v0y * v0y;
+    float dot01 = v0x * v1x + v0y * v1y;
+    float dot02 = v0x * v2x + v0y * v2y;
+    float dot11 = v1x * v1x + v1y * v1y;
+    float dot12 = v1x * v2x + v1y * v2y;
+    float invDenom = 1.0f / (dot00 * dot11 - dot01 * dot01);
+    float u = (dot11 * dot02 - dot01 * dot12) * invDenom;
+    float v = (dot00 * dot12 - dot01 * dot02) * invDenom;
+    bu = u;
+    bv = v;
+    return (u >= 0.0f) && (v >= 0.0f) && (u + v < 1.0f);
+}
+
+__device__ __forceinline__ float2 ld2(const float* p) { return make_float2(p[0], p[1]); }
+
+// Lightmap::initializeLumels(face) loop bounds (Lightmap.cpp:118-141): the
+// face's uv rectangle scaled by the map size, clamped to the map.
+__device__ __forceinline__ void face_rect(float2 a, float2 b, float2 c, int W, int H, int& u0, int& v0, int& u1,
+                                          int& v1) {
+    float minx = fminf(a.x, fminf(b.x, c.x)), maxx = fmaxf(a.x, fmaxf(b.x, c.x));
+    float miny = fminf(a.y, fminf(b.y, c.y)), maxy = fmaxf(a.y, fmaxf(b.y, c.y));
+    u0 = (int)(minx * W); u1 = (int)(maxx * W);
+    v0 = (int)(miny * H); v1 = (int)(maxy * H);
+    u1 = u1 < W - 1 ? u1 : W - 1;
+    v1 = v1 < H - 1 ? v1 : H - 1;
+    u0 = u0 < 0 ? 0 : u0;
+    v0 = v0 < 0 ? 0 : v0;
+}
+
+// Pass 1: each face claims the texels whose centre it covers; the largest
+// face index wins, as the reference's in-order loop lets the last face win.
+__global__ void k_raster_owner(DevScene s, int t0, int t1, int W, int H, int* owner) {
+    int t = t0 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= t1) return;
+    int4 f = s.tri_vidx[t];
+    float2 a = ld2(s.uv1 + 2 * f.x), b = ld2(s.uv1 + 2 * f.y), c = ld2(s.uv1 + 2 * f.z);
+    int u0, v0, u1, v1;
+    face_rect(a, b, c, W, H, u0, v0, u1, v1);
+    for (int v = v0; v <= v1; v++)
+        for (int u = u0; u <= u1; u++) {
+            float2 uv = make_float2((u + 0.5f) / (float)W, (v + 0.5f) / (float)H);
+            float bu, bv;
+            if (uv_inside(a, b, c, uv, bu, bv)) atomicMax(&owner[v * W + u], t - t0);
+        }
+}
+
+// Pass 2: Lightmap::initializeLumel (Lightmap.cpp:157-164) for the winner.
+__global__ void k_raster_init(DevScene s, int t0, DevMap m, int* owner) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int W = m.width, H = m.height;
+    if (i >= W * H) return;
+    int fl = owner[i];
+    if (fl < 0) return;
+    owner[i] = -1;
+    int4 f = s.tri_vidx[t0 + fl];
+    float2 a = ld2(s.uv1 + 2 * f.x), b = ld2(s.uv1 + 2 * f.y), c = ld2(s.uv1 + 2 * f.z);
+    int u = i % W, v = i / W;
+    float2 uv = make_float2((u + 0.5f) / (float)W, (v + 0.5f) / (float)H);
+    float bu, bv;
+    uv_inside(a, b, c, uv, bu, bv);
+    m.face[i] = fl & 0xffff;
+    st3(m.position + 3 * (size_t)i, interp3(s.pos, f, bu, bv));
+    st3(m.normal + 3 * (size_t)i, interp3(s.nrm, f, bu, bv));
+    st3(m.color + 3 * (size_t)i, mk3(0.f, 0.f, 0.f));
+    m.flags[i] |= 1;
+}
+
+extern "C" int rl_map_add_mesh(rl_map* m, const rl_scene* s, int mesh, void* stream) {
+    if (!m || !s) return fail(RL_INVALID_CALL, "rl_map_add_mesh: null argument");
+    if (mesh < 0 || mesh >= s->nmeshes) return fail(RL_INVALID_CALL, "rl_map_add_mesh: mesh %d out of range", mesh);
+    int t0 = s->mesh_first_tri[mesh], t1 = s->mesh_first_tri[mesh + 1];
+    if (t1 <= t0) return fail(RL_INVALID_CALL, "rl_map_add_mesh: mesh %d has no faces", mesh);
+    cudaStream_t st = S(stream);
+    k_raster_owner<<<blocks_for(t1 - t0, 128), 128, 0, st>>>(s->dev, t0, t1, m->dev.width, m->dev.height,
+                                                            m->d_owner);
+    CK_LAUNCH("k_raster_owner");
+    long long n = (long long)m->dev.width * m->dev.height;
+    k_raster_init<<<blocks_for(n, 256), 256, 0, st>>>(s->dev, t0, m->dev, m->d_owner);
+    CK_LAUNCH("k_raster_init");
+    return RL_OK;
+}
+
+extern "C" int rl_map_download(const rl_map* m, int32_t* flags, int32_t* face, float* position, float* normal,
+                               float* color, int32_t* photons, float* gathered, void* stream) {
+    if (!m) return fail(RL_INVALID_CALL, "null map");
+    cudaStream_t st = S(stream);
+    size_t n = (size_t)m->dev.width * m->dev.height;
+    if (flags) CK(cudaMemcpyAsync(flags, m->dev.flags, 4 * n, cudaMemcpyDeviceToHost, st));
+    if (face) CK(cudaMemcpyAsync(face, m->dev.face, 4 * n, cudaMemcpyDeviceToHost, st));
+    if (position) CK(cudaMemcpyAsync(position, m->dev.position, 12 * n, cudaMemcpyDeviceToHost, st));
+    if (normal) CK(cudaMemcpyAsync(normal, m->dev.normal, 12 * n, cudaMemcpyDeviceToHost, st));
+    if (color) CK(cudaMemcpyAsync(color, m->dev.color, 12 * n, cudaMemcpyDeviceToHost, st));
+    if (photons) CK(cudaMemcpyAsync(photons, m->dev.photons, 4 * n, cudaMemcpyDeviceToHost, st));
+    if (gathered) CK(cudaMemcpyAsync(gathered, m->dev.gathered, 12 * n, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return RL_OK;
+}
+
+extern "C" int rl_map_upload(rl_map* m, const int32_t* flags, const int32_t* face, const float* position,
+                             const float* normal, const float* color, const int32_t* photons, const float* gathered,
+                             void* stream) {
+    if (!m) return fail(RL_INVALID_CALL, "null map");
+    cudaStream_t st = S(stream);
+    size_t n = (size_t)m->dev.width * m->dev.height;
+    if (flags) CK(cudaMemcpyAsync(m->dev.flags, flags, 4 * n, cudaMemcpyHostToDevice, st));
+    if (face) CK(cudaMemcpyAsync(m->dev.face, face, 4 * n, cudaMemcpyHostToDevice, st));
+    if (position) CK(cudaMemcpyAsync(m->dev.position, position, 12 * n, cudaMemcpyHostToDevice, st));
+    if (normal) CK(cudaMemcpyAsync(m->dev.normal, normal, 12 * n, cudaMemcpyHostToDevice, st));
+    if (color) CK(cudaMemcpyAsync(m->dev.color, color, 12 * n, cudaMemcpyHostToDevice, st));
+    if (photons) CK(cudaMemcpyAsync(m->dev.photons, photons, 4 * n, cudaMemcpyHostToDevice, st));
+    if (gathered) CK(cudaMemcpyAsync(m->dev.gathered, gathered, 12 * n, cudaMemcpyHostToDevice, st));
+    return RL_OK;
+}
+
+extern "C" int rl_map_clear(rl_map* m, int colors, int photons, void* stream) {
+    if (!m) return fail(RL_INVALID_CALL, "null map");
+    cudaStream_t st = S(stream);
+    size_t n = (size_t)m->dev.width * m->dev.height;
+    if (colors) CK(cudaMemsetAsync(m->dev.color, 0, 12 * n, st));
+    if (photons) {
+        CK(cudaMemsetAsync(m->dev.photons, 0, 4 * n, st));
+        CK(cudaMemsetAsync(m->dev.gathered, 0, 12 * n, st));
+        if (!colors) CK(cudaMemsetAsync(m->dev.color, 0, 12 * n, st));
+    }
+    return RL_OK;
+}
+
+extern "C" int rl_map_device_arrays(const rl_map* m, int32_t** flags, float** position, float** normal,
+                                    float** color, int32_t** photons, float** gathered) {
+    if (!m) return fail(RL_INVALID_CALL, "null map");
+    if (flags) *flags = m->dev.flags;
+    if (position) *position = m->dev.position;
+    if (normal) *normal = m->dev.normal;
+    if (color) *color = m->dev.color;
+    if (photons) *photons = m->dev.photons;
+    if (gathered) *gathered = m->dev.gathered;
+    return RL_OK;
+}
+
+extern "C" int rl_map_valid_count(const rl_map* m, int64_t* count) {
+    if (!m || !count) return fail(RL_INVALID_CALL, "null argument");
+    size_t n = (size_t)m->dev.width * m->dev.height;
+    std::vector<int> f(n);
+    CK(cudaMemcpy(f.data(), m->dev.flags, 4 * n, cudaMemcpyDeviceToHost));
+    int64_t c = 0;
+    for (size_t i = 0; i < n; i++) c += f[i] & 1;
+    *count = c;
+    return RL_OK;
+}
+
+// ---------------------------------------------------------- light tables
+
+constexpr int kMaxLights = 64;
+constexpr int kMaxLightVerts = 1024;
+constexpr int kMaxPhotonmaps = 64;
+
+// Lights and area-light sample points, passed to kernels by value
+// (__grid_constant__), so a bake call needs no device copy of host tables.
+struct LightTable {
+    int n;
+    int nverts;
+    rl_light l[kMaxLights];
+    float verts[3 * kMaxLightVerts];
+};
+
+static int make_light_table(const rl_light* lights, int nlights, const float* lverts, int nverts, LightTable& T) {
+    if (nlights < 0 || nlights > kMaxLights) return fail(RL_INVALID_CALL, "at most %d lights per call", kMaxLights);
+    if (nverts < 0 || nverts > kMaxLightVerts)
+        return fail(RL_INVALID_CALL, "at most %d light vertices per call", kMaxLightVerts);
+    if (nlights > 0 && !lights) return fail(RL_INVALID_CALL, "null light array");
+    if (nverts > 0 && !lverts) return fail(RL_INVALID_CALL, "null light-vertex array");
+    memset(&T, 0, sizeof T);
+    T.n = nlights;
+    T.nverts = nverts;
+    for (int l = 0; l < nlights; l++) {
+        if (lights[l].vertex_count > 0 &&
+            (lights[l].vertex_first < 0 || lights[l].vertex_first + lights[l].vertex_count > nverts))
+            return fail(RL_INVALID_CALL, "light %d: vertex range outside the light-vertex pool", l);
+        T.l[l] = lights[l];
+    }
+    if (nverts) memcpy(T.verts, lverts, 12 * (size_t)nverts);
+    return RL_OK;
+}
+
+// ---------------------------------------------------------- direct light
+
+// LightSpotCutoff::cutoffForDirection (scene/Light.cpp:461-476).
+__device__ __forceinline__ float spot_cutoff(const rl_light& L, V3 direction) {
+    float value = dot3(direction, ld3(L.spot_direction));
+    if (value <= L.spot_cutoff) return 0.0f;
+    value = (1.0f - (1.0f - value) * 1.0f / (1.0f - L.spot_cutoff));
+    if (fabsf(1.0f - L.spot_exponent) > 0.01f) value = powf(value, L.spot_exponent);
+    return value;
+}
+
+__device__ __forceinline__ float lambert(V3 dir, V3 n) {
+    float dp = dot3(dir, n);
+    return dp < 0.0f ? 0.0f : dp;
+}
+
+// DirectLight::influenceFromPoint (baker/DirectLight.cpp:101-125) with the
+// light's influence, cutoff and attenuation models (scene/Light.cpp:372-500).
+__device__ float influence_from_point(const DevScene& s, V3 lpos, V3 lnrm, V3 point, const rl_light& L,
+                                      int* status) {
+    float inf = 0.0f, att = 1.0f, cut = 1.0f, distance = 0.0f;
+    if (L.influence == 1) {
+        V3 direction = sub3(point, lpos);
+        distance = normalize3(direction);
+        float intensity = lambert(direction, lnrm);
+        if (intensity <= 0.001f) {
+            inf = 0.0f;
+        } else {
+            if (L.casts_shadow) intensity *= segment_blocked(s, lpos, point, kHitUseAlpha, status) ? 0.0f : 1.0f;
+            inf = intensity;
+        }
+    } else if (L.influence == 2) {
+        V3 ldir = ld3(L.direction);
+        float intensity = lambert(neg3(ldir), lnrm);
+        if (intensity <= 0.001f) {
+            inf = 0.0f;
+        } else {
+            if (L.casts_shadow)
+                intensity *= segment_blocked(s, lpos, sub3(lpos, mul3(ldir, 1000.0f)), kHitUseAlpha, status) ? 0.0f
+                                                                                                           : 1.0f;
+            inf = intensity;
+        }
+    }
+    if (L.cutoff == 2) {
+        V3 dir = sub3(lpos, ld3(L.position));
+        normalize3(dir);
+        cut = spot_cutoff(L, dir);
+    }
+    if (L.attenuation) {
+        float r = distance / L.att_radius;
+        float a = 1.0f / (1.0f + L.att_const + L.att_linear * r + L.att_quadratic * r * r);
+        att = a > 0.0f ? a : 0.0f;
+    }
+    return inf * att * cut;
+}
+
+// DirectLight::bakeLumel (baker/DirectLight.cpp:46-98), one thread per lumel.
+__global__ void k_direct(DevScene s, DevMap m, const __grid_constant__ LightTable T, int first, int step,
+                         long long count, int* status) {
+    long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    long long i = first + k * step;
+    if (!(m.flags[i] & 1)) return;
+    V3 pos = ld3(m.position + 3 * i), nrm = ld3(m.normal + 3 * i);
+    float* col = m.color + 3 * i;
+    float cr = col[0], cg = col[1], cb = col[2];
+    for (int l = 0; l < T.n; l++) {
+        const rl_light& L = T.l[l];
+        V3 lc = ld3(L.color);
+        V3 infl = mk3(0.f, 0.f, 0.f);
+        if (L.vertex_count > 0) {
+            V3 acc = mk3(0.f, 0.f, 0.f);
+            for (int v = 0; v < L.vertex_count; v++) {
+                V3 vp = ld3(T.verts + 3 * (L.vertex_first + v));
+                float inf = influence_from_point(s, pos, nrm, add3(vp, ld3(L.position)), L, status);
+                if (inf > 0.0f) acc = add3(acc, mul3(mul3(lc, L.intensity), inf));
+            }
+            float n = (float)L.vertex_count;
+            infl = mk3(acc.x / n, acc.y / n, acc.z / n);
+        } else {
+            float inf = influence_from_point(s, pos, nrm, ld3(L.position), L, status);
+            if (inf > 0.0f) infl = mul3(mul3(lc, L.intensity), inf);
+        }
+        cr = cr + infl.x; cg = cg + infl.y; cb = cb + infl.z;
+    }
+    col[0] = cr; col[1] = cg; col[2] = cb;
+}
+
+static long long iter_count(long long n, int first, int step) {
+    if (first >= n) return 0;
+    return (n - first + step - 1) / step;
+}
+
+extern "C" int rl_bake_direct(const rl_scene* s, rl_map* lm, const rl_light* lights, int nlights,
+                              const float* light_vertices, int nlight_vertices, int first, int step, void* stream) {
+    if (!s || !lm) return fail(RL_INVALID_CALL, "rl_bake_direct: null argument");
+    if (first < 0 || step <= 0) return fail(RL_INVALID_CALL, "rl_bake_direct: bad iterator (first %d step %d)", first, step);
+    static thread_local LightTable T;
+    int rc = make_light_table(lights, nlights, light_vertices, nlight_vertices, T);
+    if (rc) return rc;
+    long long n = (long long)lm->dev.width * lm->dev.height;
+    long long count = iter_count(n, first, step);
+    if (count == 0 || nlights == 0) return RL_OK;
+    k_direct<<<blocks_for(count, 128), 128, 0, S(stream)>>>(s->dev, lm->dev, T, first, step, count, s->d_status);
+    CK_LAUNCH("k_direct");
+    return RL_OK;
+}
+
+// ------------------------------------------------------------------ AO
+
+// AmbientOcclusion::bakeLumel (baker/AmbientOcclusion.cpp:46-66).
+__global__ void k_ao(DevScene s, DevMap m, int samples, float fraction, float maxd, float exponent, uint2 key,
+                     int first, int step, long long count, int* status) {
+    long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    long long i = first + k * step;
+    if (!(m.flags[i] & 1)) return;
+    V3 pos = ld3(m.position + 3 * i), nrm = ld3(m.normal + 3 * i);
+    int occluded = 0;
+    for (int j = 0; j < samples; j++) {
+        V3 dir = random_hemisphere(nrm, key, (uint32_t)i, (uint32_t)j, kTagAO);
+        if (segment_blocked(s, pos, add3(pos, mul3(dir, maxd)), 0, status)) occluded++;
+    }
+    float value = 1.0f - occluded / (samples * fraction);
+    if (fabsf(1.0f - exponent) > 0.01f) value = powf(value, exponent);
+    float* col = m.color + 3 * i;
+    col[0] = col[0] * value; col[1] = col[1] * value; col[2] = col[2] * value;
+}
+
+extern "C" int rl_bake_ao(const rl_scene* s, rl_map* lm, int samples, float fraction, float maxd, float exponent,
+                          uint64_t seed, int first, int step, void* stream) {
+    if (!s || !lm) return fail(RL_INVALID_CALL, "rl_bake_ao: null argument");
+    if (samples <= 0 || first < 0 || step <= 0) return fail(RL_INVALID_CALL, "rl_bake_ao: bad arguments");
+    long long n = (long long)lm->dev.width * lm->dev.height;
+    long long count = iter_count(n, first, step);
+    if (count == 0) return RL_OK;
+    uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
+    k_ao<<<blocks_for(count, 128), 128, 0, S(stream)>>>(s->dev, lm->dev, samples, fraction, maxd, exponent, key,
+                                                        first, step, count, s->d_status);
+    CK_LAUNCH("k_ao");
+    return RL_OK;
+}
+
+// -------------------------------------------------------------- photons
+
+struct PhotonTables {
+    int nl;                       // lights with an emitter, in scene order
+    int light[kMaxLights];        // light index of emitter slot e
+    unsigned prefix[kMaxLights + 1];  // photon offsets within one pass
+    unsigned per_pass;
+    int nmaps;
+    DevMap maps[kMaxPhotonmaps];
+};
+
+// Photons::emit -> emitPhotons -> trace -> store (baker/Photons.cpp:50-144),
+// one thread per photon; photon p is the p-th iteration of the reference's
+// pass / light / photon loops.
+__global__ void k_photons(DevScene s, const __grid_constant__ LightTable LT, const __grid_constant__ PhotonTables T,
+                          unsigned total, int max_depth, float threshold, float maxd, uint2 key,
+                          unsigned long long* stored, int* status) {
+    unsigned p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= total) return;
+    unsigned r = p % T.per_pass;
+    int e = 0;
+    while (e + 1 < T.nl && T.prefix[e + 1] <= r) e++;
+    const rl_light& L = LT.l[T.light[e]];
+    V3 pos, dir;
+    if (L.emitter == 1) {
+        // PhotonEmitter::emit (scene/Light.cpp:340-344)
+        pos = ld3(L.position);
+        dir = random_direction(key, p, 0, kTagEmit);
+    } else {
+        // DirectionalPhotonEmitter::emit (scene/Light.cpp:355-361)
+        uint4 q = philox(make_uint4(p, 0, 0, kTagEmitPoint), key);
+        float s0 = u01(q.x), s1 = u01(q.y), s2 = u01(q.z);
+        V3 pt = mk3(s.bounds_lo[0] * (1.0f - s0) + s.bounds_hi[0] * s0, s.bounds_lo[1] * (1.0f - s1) + s.bounds_hi[1] * s1,
+                    s.bounds_lo[2] * (1.0f - s2) + s.bounds_hi[2] * s2);
+        V3 pn = ld3(L.emitter_plane);
+        float dist = dot3(pn, pt) + L.emitter_plane[3];
+        V3 onplane = sub3(pt, mul3(pn, dist));
+        dir = ld3(L.direction);
+        pos = sub3(onplane, mul3(dir, 5.0f));
+    }
+    float cut = 1.0f;
+    if (L.cutoff == 2) cut = spot_cutoff(L, dir);
+    if (cut <= 0.0f) return;
+    V3 col = mul3(mul3(ld3(L.color), L.intensity), cut);
+    for (int depth = 0;; depth++) {
+        if (depth > max_depth || (0.2126f * col.x + 0.7152f * col.y + 0.0722f * col.z) < threshold) break;
+        SegHit h;
+        trace_segment(s, pos, add3(pos, mul3(dir, maxd)), kHitPoint | kHitUv | kHitColor | kHitNormal, h, status);
+        if (!h.hit) break;
+        float influence = lambert(neg3(dir), h.normal) * 1.0f;
+        V3 hc = mul3(mk3(col.x * h.rgba.x, col.y * h.rgba.y, col.z * h.rgba.z), influence);
+        int slot = s.mesh_photonmap[h.mesh];
+        if (slot >= 0 && slot < T.nmaps) {
+            const DevMap& P = T.maps[slot];
+            int ti = lumel_at_uv(P.width, P.height, h.uv);
+            if (P.flags[ti] & 1) {
+                atomicAdd(P.color + 3 * ti, hc.x);
+                atomicAdd(P.color + 3 * ti + 1, hc.y);
+                atomicAdd(P.color + 3 * ti + 2, hc.z);
+                atomicAdd(P.photons + ti, 1);
+                if (stored) atomicAdd(stored, 1ull);
+            }
+        }
+        dir = random_hemisphere(h.normal, key, p, (uint32_t)(depth + 1), kTagBounce);
+        pos = h.point;
+        col = hc;
+    }
+}
+
+extern "C" int rl_emit_photons(const rl_scene* s, rl_map* const* maps, int nmaps, const rl_light* lights,
+                               int nlights, int pass_count, int max_depth, float threshold, float maxd, uint64_t seed,
+                               int64_t* stored, void* stream) {
+    if (!s || (nmaps > 0 && !maps)) return fail(RL_INVALID_CALL, "rl_emit_photons: null argument");
+    if (nmaps > kMaxPhotonmaps) return fail(RL_INVALID_CALL, "rl_emit_photons: at most %d photonmaps", kMaxPhotonmaps);
+    cudaStream_t st = S(stream);
+    static thread_local LightTable LT;
+    int rc = make_light_table(lights, nlights, nullptr, 0, LT);
+    if (rc) return rc;
+    static thread_local PhotonTables T;
+    memset(&T, 0, sizeof T);
+    unsigned long long per_pass = 0;
+    for (int l = 0; l < nlights; l++) {
+        if (!lights[l].emitter) continue;
+        // PhotonEmitter::photonCount (scene/Light.cpp:334-337)
+        int cnt = (int)(lights[l].intensity * 25000);
+        T.light[T.nl] = l;
+        T.prefix[T.nl] = (unsigned)per_pass;
+        per_pass += (unsigned long long)std::max(cnt, 0);
+        T.nl++;
+    }
+    T.prefix[T.nl] = (unsigned)per_pass;
+    T.per_pass = (unsigned)per_pass;
+    T.nmaps = nmaps;
+    for (int k = 0; k < nmaps; k++) {
+        if (!maps[k]) return fail(RL_INVALID_CALL, "photonmap %d is null", k);
+        T.maps[k] = maps[k]->dev;
+    }
+    unsigned long long total = per_pass * (unsigned long long)std::max(pass_count, 0);
+    if (total >= (1ull << 32)) return fail(RL_INVALID_CALL, "too many photons (%llu)", total);
+    if (stored) *stored = 0;
+    if (total == 0) return RL_OK;
+    Scratch sc;
+    unsigned long long* dc = nullptr;
+    if (stored) {
+        rc = scratch(sc, &dc, 1, st);
+        if (rc) return rc;
+        CK(cudaMemsetAsync(dc, 0, 8, st));
+    }
+    uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
+    k_photons<<<blocks_for((long long)total, 128), 128, 0, st>>>(s->dev, LT, T, (unsigned)total, max_depth, threshold,
+                                                                maxd, key, dc, s->d_status);
+    CK_LAUNCH("k_photons");
+    if (stored) {
+        unsigned long long h = 0;
+        CK(cudaMemcpyAsync(&h, dc, 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        *stored = (int64_t)h;
+    }
+    return RL_OK;
+}
+
+// Photonmap::gather (Lightmap.cpp:376-413): mean photon colour over the disc
+// of `radius` texels, for y < height and x < height (the loop bound of :379).
+__global__ void k_gather(DevMap m, int radius) {
+    int x = blockIdx.x * blockDim.x + threadIdx.x;
+    int y = blockIdx.y * blockDim.y + threadIdx.y;
+    int W = m.width, H = m.height;
+    if (x >= H || y >= H) return;
+    long long o = (long long)y * W + x;
+    if (o >= (long long)W * H) return;
+    float cr = 0.f, cg = 0.f, cb = 0.f;
+    int photons = 0;
+    for (int j = y - radius; j <= y + radius; j++) {
+        for (int i = x - radius; i <= x + radius; i++) {
+            if (i < 0 || j < 0 || i >= W || j >= H) continue;
+            float distance = sqrtf((float)((x - i) * (x - i) + (y - j) * (y - j)));
+            if (distance > radius) continue;
+            long long li = (long long)j * W + i;
+            cr = cr + m.color[3 * li]; cg = cg + m.color[3 * li + 1]; cb = cb + m.color[3 * li + 2];
+            photons += m.photons[li];
+        }
+    }
+    float* g = m.gathered + 3 * o;
+    if (photons == 0) {
+        g[0] = 0.f; g[1] = 0.f; g[2] = 0.f;
+    } else {
+        float p = (float)photons;
+        g[0] = cr / p; g[1] = cg / p; g[2] = cb / p;
+    }
+}
+
+extern "C" int rl_photonmap_gather(rl_map* pm, int radius, void* stream) {
+    if (!pm) return fail(RL_INVALID_CALL, "null photonmap");
+    if (radius < 0) return fail(RL_INVALID_CALL, "negative radius");
+    dim3 b(32, 8);
+    int H = pm->dev.height;
+    dim3 g((unsigned)((H + 31) / 32), (unsigned)((H + 7) / 8));
+    k_gather<<<g, b, 0, S(stream)>>>(pm->dev, radius);
+    CK_LAUNCH("k_gather");
+    return RL_OK;
+}
+
+// -------------------------------------------------------- final gather
+
+struct GatherMaps {
+    int nmaps;
+    DevMap maps[kMaxPhotonmaps];
+};
+
+// IndirectLight::bakeLumel (baker/IndirectLight.cpp:47-75).
+__global__ void k_indirect(DevScene s, DevMap m, const __grid_constant__ GatherMaps G, int samples, float maxd, V3 sky,
+                           V3 amb, uint2 key, int first, int step, long long count, int* status) {
+    long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    long long i = first + k * step;
+    if (!(m.flags[i] & 1)) return;
+    V3 pos = ld3(m.position + 3 * i), nrm = ld3(m.normal + 3 * i);
+    float gr = 0.f, gg = 0.f, gb = 0.f;
+    for (int j = 0; j < samples; j++) {
+        V3 dir = random_hemisphere(nrm, key, (uint32_t)i, (uint32_t)j, kTagFG);
+        float dp = dot3(nrm, dir);
+        float influence = dp > 0.0f ? dp : 0.0f;
+        SegHit h;
+        trace_segment(s, pos, add3(pos, mul3(dir, maxd)), kHitUv | kHitNormal, h, status);
+        if (!h.hit) {
+            gr = gr + (sky.x * influence + amb.x);
+            gg = gg + (sky.y * influence + amb.y);
+            gb = gb + (sky.z * influence + amb.z);
+            continue;
+        }
+        if (dot3(dir, h.normal) >= 0.0f) continue;
+        int slot = s.mesh_photonmap[h.mesh];
+        if (slot >= 0 && slot < G.nmaps) {
+            const DevMap& P = G.maps[slot];
+            int ti = lumel_at_uv(P.width, P.height, h.uv);
+            const float* g = P.gathered + 3 * (size_t)ti;
+            gr = gr + (g[0] * influence + amb.x);
+            gg = gg + (g[1] * influence + amb.y);
+            gb = gb + (g[2] * influence + amb.z);
+        }
+    }
+    float ns = (float)samples;
+    float* col = m.color + 3 * i;
+    col[0] = col[0] + gr / ns; col[1] = col[1] + gg / ns; col[2] = col[2] + gb / ns;
+}
+
+extern "C" int rl_bake_indirect(const rl_scene* s, rl_map* lm, rl_map* const* maps, int nmaps, int samples,
+                                float maxd, const float sky[3], const float ambient[3], uint64_t seed, int first,
+                                int step, void* stream) {
+    if (!s || !lm || (nmaps > 0 && !maps)) return fail(RL_INVALID_CALL, "rl_bake_indirect: null argument");
+    if (samples <= 0 || first < 0 || step <= 0 || nmaps > kMaxPhotonmaps)
+        return fail(RL_INVALID_CALL, "rl_bake_indirect: bad arguments");
+    cudaStream_t st = S(stream);
+    long long n = (long long)lm->dev.width * lm->dev.height;
+    long long count = iter_count(n, first, step);
+    if (count == 0) return RL_OK;
+    static thread_local GatherMaps G;
+    memset(&G, 0, sizeof G);
+    G.nmaps = nmaps;
+    for (int k = 0; k < nmaps; k++) {
+        if (!maps[k]) return fail(RL_INVALID_CALL, "photonmap %d is null", k);
+        G.maps[k] = maps[k]->dev;
+    }
+    V3 skyv = {sky ? sky[0] : 0.f, sky ? sky[1] : 0.f, sky ? sky[2] : 0.f};
+    V3 ambv = {ambient ? ambient[0] : 0.f, ambient ? ambient[1] : 0.f, ambient ? ambient[2] : 0.f};
+    uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
+    k_indirect<<<blocks_for(count, 128), 128, 0, st>>>(s->dev, lm->dev, G, samples, maxd, skyv, ambv, key, first,
+                                                      step, count, s->d_status);
+    CK_LAUNCH("k_indirect");
+    return RL_OK;
+}
+
+// ------------------------------------------------------------- radiosity
+
+struct FFPair {
+    int i, j;
+    float w;
+};
+
+// RadiosityBuilder::distanceFormFactor (radiosity/RadiosityBuilder.cpp:142-176)
+// for the pair i < j.
+__device__ __forceinline__ void ff_pair(const DevScene& s, int n, const float* pos, const float* nrm, float threshold,
+                                        FFPair* out, unsigned long long cap, unsigned long long* counter, int* status,
+                                        int i, int j) {
+    const float Pi = 3.1415926535897932f;
+    V3 rPos = ld3(pos + 3 * (size_t)i), rN = ld3(nrm + 3 * (size_t)i);
+    V3 sPos = ld3(pos + 3 * (size_t)j), sN = ld3(nrm + 3 * (size_t)j);
+    V3 dir = sub3(sPos, rPos);
+    float r = normalize3(dir);
+    float cosBA = dot3(dir, rN);
+    float cosAB = -(dot3(dir, sN));
+    if (r == 0.0f || cosAB < 0.0f || cosBA < 0.0f) return;
+    float wBA = ((cosBA * cosAB) / (Pi * r * r));
+    if (wBA < threshold) return;
+    if (segment_blocked(s, rPos, sPos, kHitPoint | kHitUv | kHitColor | kHitNormal, status)) return;
+    unsigned long long slot = atomicAdd(counter, 1ull);
+    if (slot < cap) out[slot] = FFPair{i, j, wBA};
+}
+
+// Every pair i < j: rows over blockIdx.y (grid-strided), j over threads.
+__global__ void k_ff_pairs(DevScene s, int n, const float* pos, const float* nrm, float threshold, FFPair* out,
+                           unsigned long long cap, unsigned long long* counter, int* status) {
+    for (int i = blockIdx.y; i < n; i += gridDim.y) {
+        int j = i + 1 + blockIdx.x * blockDim.x + threadIdx.x;
+        if (j < n) ff_pair(s, n, pos, nrm, threshold, out, cap, counter, status, i, j);
+    }
+}
+
+static int assemble_csr(int n, std::vector<FFPair>& pairs, int64_t* row_ptr, int32_t* cols, float* vals,
+                        int64_t capacity, int64_t* nnz_out) {
+    int64_t nnz = 2 * (int64_t)pairs.size();
+    if (nnz_out) *nnz_out = nnz;
+    if (!cols) return RL_OK;
+    if (!row_ptr || !vals) return fail(RL_INVALID_CALL, "form factors: row_ptr/vals missing");
+    if (capacity < nnz) return fail(RL_CAPACITY, "form factors: capacity %lld < nnz %lld", (long long)capacity, (long long)nnz);
+    std::sort(pairs.begin(), pairs.end(), [](const FFPair& a, const FFPair& b) {
+        return a.i != b.i ? a.i < b.i : a.j < b.j;
+    });
+    std::vector<int64_t> fill((size_t)n + 1, 0);
+    for (const FFPair& p : pairs) { fill[p.i + 1]++; fill[p.j + 1]++; }
+    for (int i = 0; i < n; i++) fill[i + 1] += fill[i];
+    std::memcpy(row_ptr, fill.data(), sizeof(int64_t) * ((size_t)n + 1));
+    // pairs in (i, j) order: appending both directions lists each row in
+    // ascending column order, the reference's push_back order
+    for (const FFPair& p : pairs) {
+        int64_t a = fill[p.i]++;
+        cols[a] = p.j; vals[a] = p.w;
+        int64_t b = fill[p.j]++;
+        cols[b] = p.i; vals[b] = p.w;
+    }
+    // RadiosityBuilder::refineFormFactors (:111-120): normalise each row
+    for (int i = 0; i < n; i++) {
+        float sum = 0.0f;
+        for (int64_t k = row_ptr[i]; k < row_ptr[i + 1]; k++) sum += vals[k];
+        for (int64_t k = row_ptr[i]; k < row_ptr[i + 1]; k++) vals[k] /= sum;
+    }
+    return RL_OK;
+}
+
+extern "C" int rl_ff_pairwise(const rl_scene* s, int n, const float* d_pos, const float* d_nrm, float threshold,
+                              int64_t* row_ptr, int32_t* cols, float* vals, int64_t capacity, int64_t* nnz,
+                              void* stream) {
+    if (!s || n < 0 || (n > 0 && (!d_pos || !d_nrm))) return fail(RL_INVALID_CALL, "rl_ff_pairwise: bad arguments");
+    cudaStream_t st = S(stream);
+    std::vector<FFPair> pairs;
+    if (n > 1) {
+        unsigned long long cap = 1ull << 20;
+        for (int attempt = 0; attempt < 2; attempt++) {
+            Scratch sp, sc;
+            FFPair* dp = nullptr;
+            unsigned long long* dc = nullptr;
+            int rc = scratch(sp, &dp, (size_t)cap, st);
+            if (!rc) rc = scratch(sc, &dc, 1, st);
+            if (rc) return rc;
+            CK(cudaMemsetAsync(dc, 0, 8, st));
+            dim3 grid((unsigned)((n + 255) / 256), (unsigned)std::min(n, 65535));
+            k_ff_pairs<<<grid, 256, 0, st>>>(s->dev, n, d_pos, d_nrm, threshold, dp, cap, dc, s->d_status);
+            CK_LAUNCH("k_ff_pairs");
+            unsigned long long count = 0;
+            CK(cudaMemcpyAsync(&count, dc, 8, cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            if (count <= cap) {
+                pairs.resize(count);
+                if (count) CK(cudaMemcpyAsync(pairs.data(), dp, sizeof(FFPair) * count, cudaMemcpyDeviceToHost, st));
+                CK(cudaStreamSynchronize(st));
+                break;
+            }
+            cap = count;
+        }
+    }
+    int rc = check_status(s, st);
+    if (rc) return rc;
+    return assemble_csr(n, pairs, row_ptr, cols, vals, capacity, nnz);
+}
+
+// Orthonormal basis (Duff et al., JCGT 6(1) 2017) and Malley's cosine
+// direction by disc rejection, matching the oracle's sequence.
+__device__ __forceinline__ V3 cosine_direction(V3 n, uint2 key, uint32_t item, uint32_t sample) {
+    float x = 0.f, y = 0.f;
+    for (uint32_t a = 0; a < kMaxAttempts; a++) {
+        uint4 r = philox(make_uint4(item, sample, a, kTagHemiFF), key);
+        x = u01(r.x) * 2.0f - 1.0f;
+        y = u01(r.y) * 2.0f - 1.0f;
+        if (x * x + y * y <= 1.0f) break;
+    }
+    float zz = 1.0f - x * x - y * y;
+    float z = sqrtf(zz > 0.0f ? zz : 0.0f);
+    float sign = n.z >= 0.0f ? 1.0f : -1.0f;
+    float a = -1.0f / (sign + n.z);
+    float b = n.x * n.y * a;
+    V3 b1 = mk3(1.0f + sign * n.x * n.x * a, sign * b, -sign * n.x);
+    V3 b2 = mk3(b, sign + n.y * n.y * a, -n.y);
+    return mk3(b1.x * x + b2.x * y + n.x * z, b1.y * x + b2.y * y + n.y * z, b1.z * x + b2.z * y + n.z * z);
+}
+
+struct HemiMaps {
+    const int* mesh_map;
+    const int* map_dims;
+    const long long* map_base;
+    const int* patch_of_texel;
+    int nmaps;
+};
+
+__global__ void k_ff_hemi_rays(DevScene s, int n, const float* pos, const float* nrm, int rays, float maxd, uint2 key,
+                               HemiMaps hm, int* hits, int* status) {
+    long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (k >= (long long)n * rays) return;
+    int i = (int)(k / rays), r = (int)(k % rays);
+    V3 p = ld3(pos + 3 * (size_t)i), nn = ld3(nrm + 3 * (size_t)i);
+    V3 dir = cosine_direction(nn, key, (uint32_t)i, (uint32_t)r);
+    SegHit h;
+    trace_segment(s, p, add3(p, mul3(dir, maxd)), kHitUv, h, status);
+    int out = -1;
+    if (h.hit) {
+        int map = hm.mesh_map[h.mesh];
+        if (map >= 0 && map < hm.nmaps) {
+            int ti = lumel_at_uv(hm.map_dims[2 * map], hm.map_dims[2 * map + 1], h.uv);
+            out = hm.patch_of_texel[hm.map_base[map] + ti];
+        }
+    }
+    hits[k] = out;
+}
+
+// Per patch: sort its hit patch ids in shared memory (bitonic), then
+// run-length encode them into (patch, count) pairs.
+__global__ void k_ff_hemi_rle(int rays, int pow2, const int* hits, int2* runs, int* run_count) {
+    extern __shared__ int sh[];
+    int* key = sh;
+    int* start = sh + pow2;
+    int i = blockIdx.x;
+    for (int t = threadIdx.x; t < pow2; t += blockDim.x)
+        key[t] = t < rays ? (hits[(size_t)i * rays + t] < 0 ? 0x7fffffff : hits[(size_t)i * rays + t]) : 0x7fffffff;
+    __syncthreads();
+    for (int k = 2; k <= pow2; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int t = threadIdx.x; t < pow2; t += blockDim.x) {
+                int ixj = t ^ j;
+                if (ixj > t) {
+                    bool up = (t & k) == 0;
+                    int a = key[t], b = key[ixj];
+                    if ((a > b) == up) { key[t] = b; key[ixj] = a; }
+                }
+            }
+            __syncthreads();
+        }
+    // run starts, compacted in order by a single warp-serial pass over the
+    // sorted keys (<= 1024 entries)
+    if (threadIdx.x == 0) {
+        int nr = 0;
+        for (int t = 0; t < pow2; t++) {
+            int v = key[t];
+            if (v == 0x7fffffff) break;
+            if (t == 0 || key[t - 1] != v) start[nr++] = t;
+        }
+        int end = 0;
+        while (end < pow2 && key[end] != 0x7fffffff) end++;
+        for (int q = 0; q < nr; q++) {
+            int b = start[q], e = q + 1 < nr ? start[q + 1] : end;
+            runs[(size_t)i * rays + q] = make_int2(key[b], e - b);
+        }
+        run_count[i] = nr;
+    }
+}
+
+__global__ void k_ff_hemi_compact(int n, int rays, const int2* runs, const long long* row_ptr, int* cols, float* vals) {
+    int i = blockIdx.x;
+    long long b = row_ptr[i], e = row_ptr[i + 1];
+    for (long long q = threadIdx.x; q < e - b; q += blockDim.x) {
+        int2 r = runs[(size_t)i * rays + q];
+        cols[b + q] = r.x;
+        vals[b + q] = (float)r.y / (float)rays;
+    }
+}
+
+extern "C" int rl_ff_hemisphere(const rl_scene* s, int n, const float* d_pos, const float* d_nrm, int rays,
+                                float maxd, uint64_t seed, const int32_t* mesh_map, int nmaps, const int32_t* map_dims,
+                                const int64_t* map_base, const int32_t* patch_of_texel, int64_t ntexels,
+                                int64_t* row_ptr, int32_t* cols, float* vals, int64_t capacity, int64_t* nnz,
+                                void* stream) {
+    if (!s || n < 0 || rays <= 0 || rays > 1024 || !mesh_map || !map_dims || !map_base || !patch_of_texel)
+        return fail(RL_INVALID_CALL, "rl_ff_hemisphere: bad arguments (rays must be 1..1024)");
+    cudaStream_t st = S(stream);
+    if (n == 0) {
+        if (nnz) *nnz = 0;
+        if (row_ptr) row_ptr[0] = 0;
+        return RL_OK;
+    }
+    for (int m = 0; m < nmaps; m++)
+        if (map_base[m] < 0 || map_base[m] + (int64_t)map_dims[2 * m] * map_dims[2 * m + 1] > ntexels)
+            return fail(RL_INVALID_CALL, "rl_ff_hemisphere: map %d outside patch_of_texel", m);
+    Scratch s1, s2, s3, s4, s5, s6, s7, s8;
+    int *dmm = nullptr, *ddims = nullptr, *dpot = nullptr, *dhits = nullptr, *dcnt = nullptr, *dcols = nullptr;
+    long long *dbase = nullptr, *drow = nullptr;
+    int2* druns = nullptr;
+    float* dvals = nullptr;
+    int rc = scratch(s1, &dmm, (size_t)s->nmeshes, st);
+    if (!rc) rc = scratch(s2, &ddims, 2 * (size_t)std::max(nmaps, 1), st);
+    if (!rc) rc = scratch(s3, &dbase, (size_t)std::max(nmaps, 1), st);
+    if (!rc) rc = scratch(s4, &dpot, (size_t)std::max<int64_t>(ntexels, 1), st);
+    if (!rc) rc = scratch(s5, &dhits, (size_t)n * rays, st);
+    if (!rc) rc = scratch(s6, &druns, (size_t)n * rays, st);
+    if (!rc) rc = scratch(s7, &dcnt, (size_t)n, st);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(dmm, mesh_map, 4 * (size_t)s->nmeshes, cudaMemcpyHostToDevice, st));
+    if (nmaps) {
+        CK(cudaMemcpyAsync(ddims, map_dims, 8 * (size_t)nmaps, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(dbase, map_base, 8 * (size_t)nmaps, cudaMemcpyHostToDevice, st));
+    }
+    if (ntexels) CK(cudaMemcpyAsync(dpot, patch_of_texel, 4 * (size_t)ntexels, cudaMemcpyHostToDevice, st));
+    HemiMaps hm{dmm, ddims, dbase, dpot, nmaps};
+    uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
+    long long total = (long long)n * rays;
+    k_ff_hemi_rays<<<blocks_for(total, 128), 128, 0, st>>>(s->dev, n, d_pos, d_nrm, rays, maxd, key, hm, dhits,
+                                                          s->d_status);
+    CK_LAUNCH("k_ff_hemi_rays");
+    int pow2 = 1;
+    while (pow2 < rays) pow2 <<= 1;
+    k_ff_hemi_rle<<<n, 256, 2 * pow2 * sizeof(int), st>>>(rays, pow2, dhits, druns, dcnt);
+    CK_LAUNCH("k_ff_hemi_rle");
+    std::vector<int> cnt(n);
+    CK(cudaMemcpyAsync(cnt.data(), dcnt, 4 * (size_t)n, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    std::vector<long long> rp((size_t)n + 1, 0);
+    for (int i = 0; i < n; i++) rp[i + 1] = rp[i] + cnt[i];
+    int64_t total_nnz = rp[n];
+    if (nnz) *nnz = total_nnz;
+    rc = check_status(s, st);
+    if (rc) return rc;
+    if (!cols) return RL_OK;
+    if (!row_ptr || !vals) return fail(RL_INVALID_CALL, "rl_ff_hemisphere: row_ptr/vals missing");
+    if (capacity < total_nnz) return fail(RL_CAPACITY, "rl_ff_hemisphere: capacity %lld < nnz %lld",
+                                          (long long)capacity, (long long)total_nnz);
+    std::memcpy(row_ptr, rp.data(), sizeof(int64_t) * ((size_t)n + 1));
+    rc = scratch(s8, &drow, (size_t)n + 1, st);
+    if (rc) return rc;
+    Scratch s9, s10;
+    rc = scratch(s9, &dcols, (size_t)std::max<int64_t>(total_nnz, 1), st);
+    if (!rc) rc = scratch(s10, &dvals, (size_t)std::max<int64_t>(total_nnz, 1), st);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(drow, rp.data(), 8 * ((size_t)n + 1), cudaMemcpyHostToDevice, st));
+    k_ff_hemi_compact<<<n, 128, 0, st>>>(n, rays, druns, drow, dcols, dvals);
+    CK_LAUNCH("k_ff_hemi_compact");
+    if (total_nnz) {
+        CK(cudaMemcpyAsync(cols, dcols, 4 * (size_t)total_nnz, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(vals, dvals, 4 * (size_t)total_nnz, cudaMemcpyDeviceToHost, st));
+    }
+    CK(cudaStreamSynchronize(st));
+    return RL_OK;
+}
+
+// One warp per patch row: B'_i = E_i + rho_i * sum_k F_ik B_k (RGB).
+__global__ void k_jacobi(int n, const int64_t* row_ptr, const int32_t* cols, const float* vals, const float* E,
+                         const float* rho, const float* B, float* Bn) {
+    int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    if (warp >= n) return;
+    int64_t b = row_ptr[warp], e = row_ptr[warp + 1];
+    float s0 = 0.f, s1 = 0.f, s2 = 0.f;
+    for (int64_t k = b + lane; k < e; k += 32) {
+        float w = vals[k];
+        const float* x = B + 3 * (size_t)cols[k];
+        s0 = __fmaf_rn(w, x[0], s0);
+        s1 = __fmaf_rn(w, x[1], s1);
+        s2 = __fmaf_rn(w, x[2], s2);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+        s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+        s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+    }
+    if (lane == 0) {
+        size_t i = 3 * (size_t)warp;
+        Bn[i] = __fmaf_rn(rho[i], s0, E[i]);
+        Bn[i + 1] = __fmaf_rn(rho[i + 1], s1, E[i + 1]);
+        Bn[i + 2] = __fmaf_rn(rho[i + 2], s2, E[i + 2]);
+    }
+}
+
+extern "C" int rl_radiosity_solve(int n, const int64_t* d_row_ptr, const int32_t* d_cols, const float* d_vals,
+                                  const float* d_E, const float* d_rho, int iters, float* d_B, void* stream) {
+    if (n < 0 || iters < 0 || (n > 0 && (!d_row_ptr || !d_E || !d_rho || !d_B)))
+        return fail(RL_INVALID_CALL, "rl_radiosity_solve: bad arguments");
+    cudaStream_t st = S(stream);
+    if (n == 0) return RL_OK;
+    CK(cudaMemcpyAsync(d_B, d_E, 12 * (size_t)n, cudaMemcpyDeviceToDevice, st));
+    if (iters == 0) return RL_OK;
+    Scratch sb;
+    float* tmp = nullptr;
+    int rc = scratch(sb, &tmp, 3 * (size_t)n, st);
+    if (rc) return rc;
+    float* src = d_B;
+    float* dst = tmp;
+    unsigned grid = blocks_for((long long)n * 32, 256);
+    for (int it = 0; it < iters; it++) {
+        k_jacobi<<<grid, 256, 0, st>>>(n, d_row_ptr, d_cols, d_vals, d_E, d_rho, src, dst);
+        CK_LAUNCH("k_jacobi");
+        std::swap(src, dst);
+    }
+    if (src != d_B) CK(cudaMemcpyAsync(d_B, src, 12 * (size_t)n, cudaMemcpyDeviceToDevice, st));
+    return RL_OK;
+}

@@ -1,0 +1,351 @@
+// Device-side building blocks of the B200 baker: scene view, vector math in
+// the reference's evaluation order, Philox4x32-10, material lookup and BVH
+// traversal.
+//
+// Floating point: this library is compiled with --fmad=false, so an
+// expression written `a * b + c` rounds twice exactly as the reference's C++
+// does (Types.h vector operators, evaluated left to right).  Fused
+// multiply-adds appear only where they are written out as __fmaf_rn(): in
+// the BVH slab test (conservative by construction) and in the triangle test,
+// whose fixed fmaf sequence defines this tracer's arithmetic.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace rl {
+
+// ------------------------------------------------------------------ scene
+
+// BVH node, 64 bytes, both children's boxes in the parent (four float4):
+//   n0 = c0.lo.x c0.hi.x c0.lo.y c0.hi.y
+//   n1 = c1.lo.x c1.hi.x c1.lo.y c1.hi.y
+//   n2 = c0.lo.z c0.hi.z c1.lo.z c1.hi.z
+//   n3 = child0, child1 (int bits), 0, 0
+// child >= 0: inner node index; child < 0: leaf, ~child = first_tri << 3 | (count - 1).
+// Triangles, 48 bytes in leaf order: t0 = v0.xyz | gid bits, t1 = e1.xyz, t2 = e2.xyz.
+struct DevScene {
+    const float4* nodes;
+    const float4* tris;
+    const int4* tri_vidx;       // per global triangle id: a, b, c, mesh
+    const float* pos;
+    const float* nrm;
+    const float* uv0;
+    const float* uv1;
+    const int* vmat;
+    const int* mesh_first_tri;
+    const int* mesh_photonmap;
+    const float* mat_rgb;
+    const int* mat_tex;
+    const int* tex_dims;
+    const long long* tex_offset;
+    const unsigned char* tex_pixels;
+    float bounds_lo[3];
+    float bounds_hi[3];
+    int ntris;
+    int nmeshes;
+    int has_alpha;              // some material can have alpha <= 0.1 (RGBA texture)
+};
+
+// SoA lumel arrays of one map (Lightmap.h:35-55).
+struct DevMap {
+    int width, height;
+    int* flags;
+    int* face;
+    float* position;
+    float* normal;
+    float* color;
+    int* photons;
+    float* gathered;
+};
+
+constexpr int kHitPoint = 1, kHitUv = 2, kHitColor = 4, kHitNormal = 8, kHitUseAlpha = 16;
+constexpr int kStackSize = 64;
+
+// ------------------------------------------------------------------ vectors
+
+struct V3 {
+    float x, y, z;
+};
+__device__ __forceinline__ V3 mk3(float x, float y, float z) { return V3{x, y, z}; }
+__device__ __forceinline__ V3 ld3(const float* p) { return V3{p[0], p[1], p[2]}; }
+__device__ __forceinline__ void st3(float* p, V3 v) { p[0] = v.x; p[1] = v.y; p[2] = v.z; }
+__device__ __forceinline__ V3 add3(V3 a, V3 b) { return V3{a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ V3 sub3(V3 a, V3 b) { return V3{a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ V3 mul3(V3 a, float s) { return V3{a.x * s, a.y * s, a.z * s}; }
+__device__ __forceinline__ V3 neg3(V3 a) { return V3{-a.x, -a.y, -a.z}; }
+// Vec3::operator*(Vec3) (Types.h:794-796)
+__device__ __forceinline__ float dot3(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+// Vec3::length / normalize (Types.h:841-859)
+__device__ __forceinline__ float len3(V3 a) { return sqrtf(a.x * a.x + a.y * a.y + a.z * a.z); }
+__device__ __forceinline__ float normalize3(V3& a) {
+    float len = len3(a);
+    if (len != 0.0f) {
+        a.x = a.x / len; a.y = a.y / len; a.z = a.z / len;
+    }
+    return len;
+}
+
+// ------------------------------------------------------------------ Philox
+
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as
+// easy as 1, 2, 3", SC'11).
+__device__ __forceinline__ uint4 philox(uint4 c, uint2 k) {
+#pragma unroll
+    for (int r = 0; r < 10; r++) {
+        uint32_t hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
+        uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
+        c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+        k.x += 0x9E3779B9u;
+        k.y += 0xBB67AE85u;
+    }
+    return c;
+}
+
+// Purpose tags (counter word 3) keep the streams of different draws apart.
+enum : uint32_t { kTagAO = 1, kTagFG = 2, kTagEmit = 3, kTagEmitPoint = 4, kTagBounce = 5, kTagHemiFF = 6 };
+constexpr int kMaxAttempts = 64;
+
+__device__ __forceinline__ float u01(uint32_t x) { return (float)(x >> 8) * 0x1p-24f; }
+
+// Vec3::randomDirection (Types.h:924-937): uniform cube rejection, dir / len.
+__device__ __forceinline__ V3 random_direction(uint2 key, uint32_t item, uint32_t sample, uint32_t tag) {
+    V3 dir = mk3(0.f, 0.f, 0.f);
+    float len = 0.0f;
+    for (uint32_t a = 0; a < kMaxAttempts; a++) {
+        uint4 r = philox(make_uint4(item, sample, a, tag), key);
+        dir.x = (u01(r.x) * 2.0f - 1.0f);
+        dir.y = (u01(r.y) * 2.0f - 1.0f);
+        dir.z = (u01(r.z) * 2.0f - 1.0f);
+        len = len3(dir);
+        if (!(len > 1.0f)) break;
+    }
+    return mk3(dir.x / len, dir.y / len, dir.z / len);
+}
+
+// Vec3::randomHemisphereDirection (Types.h:940-949).
+__device__ __forceinline__ V3 random_hemisphere(V3 n, uint2 key, uint32_t item, uint32_t sample, uint32_t tag) {
+    V3 d = random_direction(key, item, sample, tag);
+    if (dot3(d, n) < 0.0f) d = neg3(d);
+    return d;
+}
+
+// ---------------------------------------------------------- face attributes
+
+// Face::normalAt / positionAt (scene/Mesh.cpp:454-475): a + (b-a)*y + (c-a)*x.
+__device__ __forceinline__ V3 interp3(const float* arr, int4 f, float bx, float by) {
+    V3 a = ld3(arr + 3 * f.x), b = ld3(arr + 3 * f.y), c = ld3(arr + 3 * f.z);
+    return mk3(a.x + (b.x - a.x) * by + (c.x - a.x) * bx, a.y + (b.y - a.y) * by + (c.y - a.y) * bx,
+               a.z + (b.z - a.z) * by + (c.z - a.z) * bx);
+}
+
+// Face::uvAt (scene/Mesh.cpp:488-495).
+__device__ __forceinline__ float2 interp2(const float* arr, int4 f, float bx, float by) {
+    const float* a = arr + 2 * f.x;
+    const float* b = arr + 2 * f.y;
+    const float* c = arr + 2 * f.z;
+    return make_float2(a[0] + (b[0] - a[0]) * by + (c[0] - a[0]) * bx, a[1] + (b[1] - a[1]) * by + (c[1] - a[1]) * bx);
+}
+
+// Face::colorAt -> Material / TexturedMaterial / Texture::colorAt
+// (scene/Mesh.cpp:478-485, scene/Material.cpp:41-98).
+__device__ __forceinline__ float4 face_color(const DevScene& s, int4 f, float bx, float by) {
+    int m = s.vmat[f.x];
+    if (m < 0) return make_float4(1.f, 1.f, 1.f, 1.f);
+    float4 base = make_float4(s.mat_rgb[3 * m], s.mat_rgb[3 * m + 1], s.mat_rgb[3 * m + 2], 1.0f);
+    int tex = s.mat_tex[m];
+    if (tex < 0) return base;
+    float2 uv = interp2(s.uv0, f, bx, by);
+    int w = s.tex_dims[3 * tex], h = s.tex_dims[3 * tex + 1], ch = s.tex_dims[3 * tex + 2];
+    int x = ((int)(uv.x * (float)w)) % w;
+    int y = ((int)(uv.y * (float)h)) % h;
+    float4 t = make_float4(1.f, 0.f, 1.f, 1.f);
+    if (x >= 0 && x < w && y >= 0 && y < h) {
+        const unsigned char* p = s.tex_pixels + s.tex_offset[tex] + ((long long)y * w * ch + (long long)x * ch);
+        t = make_float4(p[0] / 255.0f, p[1] / 255.0f, p[2] / 255.0f, ch == 4 ? p[3] / 255.0f : 1.0f);
+    }
+    return make_float4(base.x * t.x, base.y * t.y, base.z * t.z, base.w * t.w);
+}
+
+// Lightmap::lumel(const Uv&) (Lightmap.cpp:61-67): x = int(u * (W - 1)).
+// Out-of-range uvs (undefined behaviour in the reference) are clamped.
+__device__ __forceinline__ int lumel_at_uv(int w, int h, float2 uv) {
+    int x = (int)(uv.x * (float)(w - 1));
+    int y = (int)(uv.y * (float)(h - 1));
+    x = x < 0 ? 0 : (x > w - 1 ? w - 1 : x);
+    y = y < 0 ? 0 : (y > h - 1 ? h - 1 : y);
+    return y * w + x;
+}
+
+// ---------------------------------------------------------------- traversal
+
+// Moeller-Trumbore over v0, e1, e2 with the oracle tracer's exact fmaf
+// sequence (hit on the open interval tnear < t < tfar).
+__device__ __forceinline__ bool tri_test(float4 t0, float4 t1, float4 t2, V3 o, V3 d, float tnear, float tfar,
+                                         float& t_out, float& u_out, float& v_out) {
+    float px = __fmaf_rn(d.y, t2.z, -(d.z * t2.y));
+    float py = __fmaf_rn(d.z, t2.x, -(d.x * t2.z));
+    float pz = __fmaf_rn(d.x, t2.y, -(d.y * t2.x));
+    float det = __fmaf_rn(t1.x, px, __fmaf_rn(t1.y, py, t1.z * pz));
+    if (det == 0.0f) return false;
+    float inv = 1.0f / det;
+    float tx = o.x - t0.x, ty = o.y - t0.y, tz = o.z - t0.z;
+    float u = __fmaf_rn(tx, px, __fmaf_rn(ty, py, tz * pz)) * inv;
+    if (!(u >= 0.0f && u <= 1.0f)) return false;
+    float qx = __fmaf_rn(ty, t1.z, -(tz * t1.y));
+    float qy = __fmaf_rn(tz, t1.x, -(tx * t1.z));
+    float qz = __fmaf_rn(tx, t1.y, -(ty * t1.x));
+    float v = __fmaf_rn(d.x, qx, __fmaf_rn(d.y, qy, d.z * qz)) * inv;
+    if (!(v >= 0.0f && u + v <= 1.0f)) return false;
+    float t = __fmaf_rn(t2.x, qx, __fmaf_rn(t2.y, qy, t2.z * qz)) * inv;
+    if (!(t > tnear && t < tfar)) return false;
+    t_out = t; u_out = u; v_out = v;
+    return true;
+}
+
+struct RayHit {
+    float t, u, v;
+    int gid;  // global triangle id, -1 = miss
+};
+
+__device__ __forceinline__ float safe_inv(float d) {
+    // keep the slab test finite: |d| below 1e-20 is treated as +-1e-20
+    float a = fabsf(d) < 1e-20f ? copysignf(1e-20f, d) : d;
+    return 1.0f / a;
+}
+
+// Slab test of both children of a node against [tnear, tmax]; returns the
+// entry distances.  Conservative: boxes were padded at build and the exit
+// bound is widened by a few ulps.
+__device__ __forceinline__ void slab2(float4 n0, float4 n1, float4 n2, V3 idir, V3 ood, float tnear, float tmax,
+                                      bool& h0, bool& h1, float& e0, float& e1) {
+    float a0 = __fmaf_rn(n0.x, idir.x, -ood.x), a1 = __fmaf_rn(n0.y, idir.x, -ood.x);
+    float b0 = __fmaf_rn(n0.z, idir.y, -ood.y), b1 = __fmaf_rn(n0.w, idir.y, -ood.y);
+    float c0 = __fmaf_rn(n2.x, idir.z, -ood.z), c1 = __fmaf_rn(n2.y, idir.z, -ood.z);
+    float lo0 = fmaxf(fmaxf(fminf(a0, a1), fminf(b0, b1)), fmaxf(fminf(c0, c1), tnear));
+    float hi0 = fminf(fminf(fmaxf(a0, a1), fmaxf(b0, b1)), fminf(fmaxf(c0, c1), tmax));
+    float d0 = __fmaf_rn(n1.x, idir.x, -ood.x), d1 = __fmaf_rn(n1.y, idir.x, -ood.x);
+    float f0 = __fmaf_rn(n1.z, idir.y, -ood.y), f1 = __fmaf_rn(n1.w, idir.y, -ood.y);
+    float g0 = __fmaf_rn(n2.z, idir.z, -ood.z), g1 = __fmaf_rn(n2.w, idir.z, -ood.z);
+    float lo1 = fmaxf(fmaxf(fminf(d0, d1), fminf(f0, f1)), fmaxf(fminf(g0, g1), tnear));
+    float hi1 = fminf(fminf(fmaxf(d0, d1), fmaxf(f0, f1)), fminf(fmaxf(g0, g1), tmax));
+    h0 = lo0 <= hi0 * 1.0000003f;
+    h1 = lo1 <= hi1 * 1.0000003f;
+    e0 = lo0;
+    e1 = lo1;
+}
+
+// Closest hit (any = false) or first hit (any = true) on (tnear, tfar).
+// Ties in t go to the smaller global triangle id, so the answer does not
+// depend on the BVH's shape.
+template <bool kAny>
+__device__ __forceinline__ bool traverse(const DevScene& s, V3 o, V3 d, float tnear, float tfar, RayHit& hit,
+                                         int* overflow) {
+    hit.gid = -1;
+    if (s.ntris == 0) return false;
+    V3 idir = mk3(safe_inv(d.x), safe_inv(d.y), safe_inv(d.z));
+    V3 ood = mk3(o.x * idir.x, o.y * idir.y, o.z * idir.z);
+    int stack[kStackSize];
+    int sp = 0;
+    int node = 0;
+    float best = tfar;
+    int best_gid = 0x7fffffff;
+    for (;;) {
+        while (node >= 0) {
+            const float4* np = s.nodes + 4 * (size_t)node;
+            float4 n0 = __ldg(np), n1 = __ldg(np + 1), n2 = __ldg(np + 2), n3 = __ldg(np + 3);
+            bool h0, h1;
+            float e0, e1;
+            slab2(n0, n1, n2, idir, ood, tnear, best, h0, h1, e0, e1);
+            int c0 = __float_as_int(n3.x), c1 = __float_as_int(n3.y);
+            if (h0 && h1) {
+                int nearc = c0, farc = c1;
+                if (e1 < e0) { nearc = c1; farc = c0; }
+                if (sp < kStackSize) stack[sp++] = farc;
+                else if (overflow) *overflow = 1;
+                node = nearc;
+            } else if (h0) {
+                node = c0;
+            } else if (h1) {
+                node = c1;
+            } else {
+                if (sp == 0) return hit.gid >= 0;
+                node = stack[--sp];
+            }
+        }
+        // leaf
+        int code = ~node;
+        int first = code >> 3, count = (code & 7) + 1;
+        for (int i = first; i < first + count; i++) {
+            const float4* tp = s.tris + 3 * (size_t)i;
+            float4 t0 = __ldg(tp), t1 = __ldg(tp + 1), t2 = __ldg(tp + 2);
+            float t, u, v;
+            if (tri_test(t0, t1, t2, o, d, tnear, tfar, t, u, v)) {
+                int gid = __float_as_int(t0.w);
+                if (t < best || (t == best && gid < best_gid)) {
+                    best = t; best_gid = gid;
+                    hit.t = t; hit.u = u; hit.v = v; hit.gid = gid;
+                    if (kAny) return true;
+                }
+            }
+        }
+        if (sp == 0) return hit.gid >= 0;
+        node = stack[--sp];
+    }
+}
+
+// Result of the reference's traceSegment post-processing.
+struct SegHit {
+    bool hit;
+    V3 point;
+    V3 normal;
+    float4 rgba;
+    float2 uv;
+    int mesh, face;
+    float t, u, v;
+};
+
+// rt::Embree::traceSegment + initializeRay (rt/Embree.cpp:107-177).
+__device__ __forceinline__ void trace_segment(const DevScene& s, V3 start, V3 end, int flags, SegHit& r,
+                                              int* overflow) {
+    r.hit = false;
+    for (int step = 0;; step++) {
+        V3 dir = sub3(end, start);
+        float len = normalize3(dir);
+        RayHit h;
+        if (!traverse<false>(s, start, dir, 0.01f, len, h, overflow)) return;
+        V3 point = add3(start, mul3(dir, h.t));
+        int4 f = __ldg(s.tri_vidx + h.gid);
+        float4 rgba = make_float4(1.f, 1.f, 1.f, 1.f);
+        if ((flags & (kHitColor | kHitUseAlpha)) != 0) rgba = face_color(s, f, h.u, h.v);
+        if ((flags & kHitUseAlpha) && rgba.w <= 0.1f && step < 25) {
+            start = add3(point, dir);
+            continue;
+        }
+        r.hit = true;
+        r.point = point;
+        r.mesh = f.w;
+        r.face = h.gid - s.mesh_first_tri[f.w];
+        r.t = h.t; r.u = h.u; r.v = h.v;
+        if (flags & kHitNormal) r.normal = interp3(s.nrm, f, h.u, h.v);
+        if (flags & kHitColor) r.rgba = rgba;
+        if (flags & kHitUv) r.uv = interp2(s.uv1, f, h.u, h.v);
+        return;
+    }
+}
+
+// Hit / miss of a segment as the reference sees it (traceSegment's bool).
+// Without alpha in play a first-hit walk gives the same answer.
+__device__ __forceinline__ bool segment_blocked(const DevScene& s, V3 start, V3 end, int flags, int* overflow) {
+    if (!(flags & kHitUseAlpha) || !s.has_alpha) {
+        V3 dir = sub3(end, start);
+        float len = normalize3(dir);
+        RayHit h;
+        return traverse<true>(s, start, dir, 0.01f, len, h, overflow);
+    }
+    SegHit r;
+    trace_segment(s, start, end, flags, r, overflow);
+    return r.hit;
+}
+
+}  // namespace rl

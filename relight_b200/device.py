@@ -1,0 +1,254 @@
+"""The baking front end: relight::Relight over the CUDA C ABI.
+
+`Relight` mirrors Relight.h:155-189.  A scene's BVH and every lightmap /
+photonmap live on the device once the first bake call sees the scene; the
+bake calls enqueue kernels on `stream` (a cudaStream_t as an int, None = the
+legacy default stream) and return at once, as the C ABI does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from typing import Optional
+
+import numpy as np
+
+from . import _abi
+from ._abi import check, lib
+from .api import (AmbientOcclusionSettings, IndirectLightSettings, Lightmap, Mesh, Photonmap, RelightStatus, Scene)
+
+
+@dataclass
+class LumelBakeIterator:
+    """bake::LumelBakeIterator (baker/Baker.h:138-148): lumels first, first+step, ..."""
+    first: int = 0
+    step: int = 1
+
+
+class DeviceScene:
+    """An rl_scene: the flat scene uploaded and its BVH built (Scene::end)."""
+
+    def __init__(self, flat, stream=None, builder: int = 0):
+        self.flat = flat
+        self.desc, self.keep = _abi.make_scene_desc(flat)
+        self.handle = C.c_void_p()
+        self.stream = stream
+        check(lib().rl_scene_create(C.byref(self.desc), builder, stream, C.byref(self.handle)))
+
+    def bvh_stats(self):
+        nodes, leaves, depth, sah = C.c_int64(), C.c_int64(), C.c_int32(), C.c_double()
+        check(lib().rl_scene_bvh_stats(self.handle, C.byref(nodes), C.byref(leaves), C.byref(depth), C.byref(sah)))
+        return {"nodes": nodes.value, "leaves": leaves.value, "depth": depth.value, "sah": sah.value}
+
+    def close(self):
+        if self.handle:
+            check(lib().rl_scene_destroy(self.handle))
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class DeviceMap:
+    """An rl_map: lumel arrays of one lightmap / photonmap on the device."""
+
+    def __init__(self, kind: int, width: int, height: int):
+        self.kind, self.width, self.height = kind, width, height
+        self.handle = C.c_void_p()
+        check(lib().rl_map_create(kind, width, height, C.byref(self.handle)))
+
+    def add_mesh(self, scene: DeviceScene, mesh_index: int, stream=None):
+        check(lib().rl_map_add_mesh(self.handle, scene.handle, mesh_index, stream))
+
+    def download(self, stream=None, fields=("flags", "face", "position", "normal", "color", "photons", "gathered")):
+        n = self.width * self.height
+        shapes = {"flags": (n,), "face": (n,), "photons": (n,), "position": (n, 3), "normal": (n, 3),
+                  "color": (n, 3), "gathered": (n, 3)}
+        out = {}
+        args = []
+        for f in ("flags", "face", "position", "normal", "color", "photons", "gathered"):
+            if f in fields:
+                dt = np.int32 if f in ("flags", "face", "photons") else np.float32
+                out[f] = np.zeros(shapes[f], dt)
+                args.append(C.c_void_p(out[f].ctypes.data))
+            else:
+                args.append(None)
+        check(lib().rl_map_download(self.handle, *args, stream))
+        return out
+
+    def upload(self, stream=None, **arrays):
+        args = []
+        for f in ("flags", "face", "position", "normal", "color", "photons", "gathered"):
+            a = arrays.get(f)
+            if a is not None:
+                dt = np.int32 if f in ("flags", "face", "photons") else np.float32
+                a = np.ascontiguousarray(a, dt)
+                arrays[f] = a
+                args.append(C.c_void_p(a.ctypes.data))
+            else:
+                args.append(None)
+        check(lib().rl_map_upload(self.handle, *args, stream))
+
+    def clear(self, colors=True, photons=False, stream=None):
+        check(lib().rl_map_clear(self.handle, int(colors), int(photons), stream))
+
+    def device_arrays(self):
+        ptrs = [C.c_void_p() for _ in range(6)]
+        check(lib().rl_map_device_arrays(self.handle, *[C.byref(p) for p in ptrs]))
+        return dict(zip(("flags", "position", "normal", "color", "photons", "gathered"), [p.value for p in ptrs]))
+
+    def valid_count(self):
+        c = C.c_int64()
+        check(lib().rl_map_valid_count(self.handle, C.byref(c)))
+        return c.value
+
+    def close(self):
+        if self.handle:
+            check(lib().rl_map_destroy(self.handle))
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _map_array(maps):
+    arr = (C.c_void_p * max(len(maps), 1))()
+    for i, m in enumerate(maps):
+        arr[i] = m.handle.value
+    return arr
+
+
+class Relight:
+    """relight::Relight (Relight.h:155-189)."""
+
+    def __init__(self, stream=None, seed: int = 0x5EED):
+        self.stream = stream
+        self._seed = seed
+        self._calls = 0
+
+    @staticmethod
+    def create(stream=None):
+        return Relight(stream)
+
+    def create_scene(self) -> Scene:
+        s = Scene()
+        s.begin()
+        return s
+
+    def create_lightmap(self, width, height) -> Lightmap:
+        return Lightmap(width, height)
+
+    def create_photonmap(self, width, height) -> Photonmap:
+        return Photonmap(width, height)
+
+    # ------------------------------------------------------------ helpers
+    def next_seed(self):
+        """Each stochastic call draws from its own Philox key."""
+        self._calls += 1
+        return (self._seed * 0x9E3779B97F4A7C15 + self._calls) & 0xFFFFFFFFFFFFFFFF
+
+    def device_scene(self, scene: Scene) -> DeviceScene:
+        """Upload the scene and rasterise every map's lumels (Scene::end +
+        Lightmap/Photonmap::addMesh, in the reference's addMesh order)."""
+        if scene.flat is None:
+            raise RuntimeError("Scene::end has not been called")
+        if scene._device is None:
+            ds = DeviceScene(scene.flat, self.stream)
+            for maps in (scene.flat.lightmaps, scene.flat.photonmaps):
+                for m in maps:
+                    if m._device is None:
+                        m._device = DeviceMap(m.KIND, m.width, m.height)
+                        for mesh in m.meshes:
+                            m._device.add_mesh(ds, scene.meshes.index(mesh), self.stream)
+            scene._device = ds
+        return scene._device
+
+    @staticmethod
+    def _iter(iterator):
+        if iterator is None:
+            return 0, 1
+        if isinstance(iterator, LumelBakeIterator):
+            return iterator.first, iterator.step
+        raise NotImplementedError("only LumelBakeIterator is supported on the device")
+
+    def _check_mesh(self, scene: Scene, mesh: Mesh):
+        if mesh.face_count() == 0 or mesh.lightmap is None:
+            return RelightStatus.RelightInvalidCall
+        return RelightStatus.RelightSuccess
+
+    # -------------------------------------------------------------- bakes
+    def bake_direct_light(self, scene: Scene, mesh: Mesh, progress=None, iterator=None) -> RelightStatus:
+        """Relight::bakeDirectLight (Relight.cpp:216-227)."""
+        st = self._check_mesh(scene, mesh)
+        if st:
+            return st
+        ds = self.device_scene(scene)
+        first, step = self._iter(iterator)
+        f = scene.flat
+        check(lib().rl_bake_direct(ds.handle, mesh.lightmap._device.handle, C.c_void_p(f.lights.ctypes.data),
+                                   len(f.lights), C.c_void_p(f.light_vertices.ctypes.data),
+                                   int(sum(int(l["vertex_count"]) for l in f.lights)), first, step, self.stream))
+        return RelightStatus.RelightSuccess
+
+    def bake_ambient_occlusion(self, scene: Scene, mesh: Mesh, progress, settings: AmbientOcclusionSettings,
+                               iterator=None, seed: Optional[int] = None) -> RelightStatus:
+        """Relight::bakeAmbientOcclusion (Relight.cpp:260-271)."""
+        st = self._check_mesh(scene, mesh)
+        if st:
+            return st
+        ds = self.device_scene(scene)
+        first, step = self._iter(iterator)
+        seed = self.next_seed() if seed is None else seed
+        check(lib().rl_bake_ao(ds.handle, mesh.lightmap._device.handle, settings.samples, settings.occluded_fraction,
+                               settings.max_distance, settings.exponent, seed, first, step, self.stream))
+        return RelightStatus.RelightSuccess
+
+    def emit_photons(self, scene: Scene, settings: IndirectLightSettings, seed: Optional[int] = None) -> RelightStatus:
+        """Relight::emitPhotons (Relight.cpp:244-257): trace, then gather every photonmap."""
+        ds = self.device_scene(scene)
+        f = scene.flat
+        maps = [m._device for m in f.photonmaps]
+        seed = self.next_seed() if seed is None else seed
+        check(lib().rl_emit_photons(ds.handle, _map_array(maps), len(maps), C.c_void_p(f.lights.ctypes.data),
+                                    len(f.lights), settings.photon_pass_count, settings.photon_bounce_count,
+                                    settings.photon_energy_threshold, settings.photon_max_distance, seed, None,
+                                    self.stream))
+        for m in maps:
+            check(lib().rl_photonmap_gather(m.handle, settings.final_gather_radius, self.stream))
+        return RelightStatus.RelightSuccess
+
+    def bake_indirect_light(self, scene: Scene, mesh: Mesh, progress, settings: IndirectLightSettings,
+                            iterator=None, seed: Optional[int] = None) -> RelightStatus:
+        """Relight::bakeIndirectLight (Relight.cpp:230-241)."""
+        st = self._check_mesh(scene, mesh)
+        if st:
+            return st
+        ds = self.device_scene(scene)
+        first, step = self._iter(iterator)
+        maps = [m._device for m in scene.flat.photonmaps]
+        sky = (C.c_float * 3)(*[float(x) for x in settings.sky_color])
+        amb = (C.c_float * 3)(*[float(x) for x in settings.ambient_color])
+        seed = self.next_seed() if seed is None else seed
+        check(lib().rl_bake_indirect(ds.handle, mesh.lightmap._device.handle, _map_array(maps), len(maps),
+                                     settings.final_gather_samples, settings.final_gather_distance, sky, amb, seed,
+                                     first, step, self.stream))
+        return RelightStatus.RelightSuccess
+
+
+def lumels(lightmap: Lightmap, stream=None):
+    """Lightmap::lumels(): the map's lumel arrays copied to the host."""
+    if lightmap._device is None:
+        raise RuntimeError("the lightmap has not been baked yet")
+    return lightmap._device.download(stream)
+
+
+def to_hdr(lightmap: Lightmap, stream=None):
+    """Lightmap::toHdr (Lightmap.cpp:332-349): float RGB, row-major."""
+    c = lightmap._device.download(stream, fields=("color",))["color"]
+    return c.reshape(lightmap.height, lightmap.width, 3)

@@ -1,0 +1,263 @@
+"""Parity of the CUDA passes with the oracle (the C restatement), through the
+C ABI, on seeded synthetic scenes.
+
+Tolerances:
+  - ray tracing, texel rasterisation, direct light, AO, final gather from a
+    fixed photonmap, pairwise and hemisphere form factors: bit-exact (the
+    kernels follow the oracle's float operation order with --fmad=false and
+    draw the same Philox numbers);
+  - photon deposit: integer counts exact, colour sums within 1e-5 relative
+    (atomic float adds in arbitrary order);
+  - radiosity Jacobi (fp32, 50 iterations): within 1e-4 relative of an FP64
+    Jacobi on the same form factors.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from oracle_bind import LumelMap, Oracle, jacobi_f64
+from relight_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+
+def _dev(a, torch):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def _relight():
+    from relight_b200.device import Relight
+    return Relight()
+
+
+def _lumels(m):
+    from relight_b200.device import lumels
+    return lumels(m)
+
+
+def _segments(rng, lo, hi, n):
+    a = rng.uniform(lo, hi, (n, 3))
+    b = rng.uniform(lo, hi, (n, 3))
+    return np.concatenate([a, b], 1).astype(np.float32)
+
+
+@pytest.mark.parametrize("which", ["room", "terrain"])
+def test_trace_segments_match_oracle(cuda, which):
+    import torch
+    from relight_b200 import _abi
+    if which == "room":
+        w = scenes.room_scene(size=64)
+        scene = w.scene
+    else:
+        w = scenes.terrain_scene(verts=48, n_boxes=60, size=128, tiles=2)
+        scene = w.scene
+    flat = scene.flat
+    rl = _relight()
+    ds = rl.device_scene(scene)
+    orc = Oracle(flat).bind_scene(scene)
+    rng = np.random.default_rng(11)
+    seg = _segments(rng, flat.bounds_lo - 1, flat.bounds_hi + 1, 20000)
+    for flags in (_abi.HIT_ALL, _abi.HIT_UV | _abi.HIT_NORMAL, _abi.HIT_ALL | _abi.HIT_USE_ALPHA):
+        ref = orc.trace_segments(seg, flags)
+        n = seg.shape[0]
+        d_seg = _dev(seg, torch)
+        hit = torch.zeros(n, dtype=torch.int32, device="cuda")
+        mf = torch.zeros((n, 2), dtype=torch.int32, device="cuda")
+        pt = torch.zeros((n, 3), dtype=torch.float32, device="cuda")
+        nm = torch.zeros((n, 3), dtype=torch.float32, device="cuda")
+        rgba = torch.zeros((n, 4), dtype=torch.float32, device="cuda")
+        uv = torch.zeros((n, 2), dtype=torch.float32, device="cuda")
+        _abi.check(_abi.lib().rl_trace_segments(ds.handle, n, d_seg.data_ptr(), flags, hit.data_ptr(), None,
+                                                mf.data_ptr(), pt.data_ptr(), nm.data_ptr(), rgba.data_ptr(),
+                                                uv.data_ptr(), None))
+        torch.cuda.synchronize()
+        assert np.array_equal(hit.cpu().numpy(), ref["hit"])
+        m = ref["hit"] > 0
+        assert m.sum() > 1000
+        assert np.array_equal(mf.cpu().numpy()[:, 0], ref["mesh"])
+        assert np.array_equal(mf.cpu().numpy()[:, 1], ref["face"])
+        assert np.array_equal(pt.cpu().numpy()[m], ref["point"][m])
+        assert np.array_equal(nm.cpu().numpy()[m], ref["normal"][m])
+        assert np.array_equal(uv.cpu().numpy()[m], ref["uv"][m])
+        assert np.array_equal(rgba.cpu().numpy()[m], ref["rgba"][m])
+
+
+def test_texel_rasterisation_matches_oracle(cuda):
+    for scene, maps in ((scenes.room_scene(size=96).scene, "lightmap"),
+                        (scenes.radiosity_room(size=48).scene, "lightmap")):
+        rl = _relight()
+        rl.device_scene(scene)
+        orc = Oracle(scene.flat).bind_scene(scene)
+        for m, lm in zip(scene.flat.lightmaps, orc.maps(maps)):
+            g = _lumels(m)
+            for f in ("flags", "face", "position", "normal"):
+                assert np.array_equal(g[f], getattr(lm, f)), f
+
+
+def test_direct_light_bit_exact(cuda):
+    w = scenes.room_scene(size=128)
+    rl = _relight()
+    rl.bake_direct_light(w.scene, w.mesh, None)
+    g = _lumels(w.lightmap)
+    orc = Oracle(w.scene.flat).bind_scene(w.scene)
+    lm = orc.maps()[0]
+    orc.bake_direct(lm)
+    assert (g["color"].sum(1) > 0).sum() > 1000
+    assert np.array_equal(g["color"], lm.color)
+
+
+def test_direct_light_iterator_subset(cuda):
+    from relight_b200.device import LumelBakeIterator
+    w = scenes.room_scene(size=64)
+    rl = _relight()
+    rl.bake_direct_light(w.scene, w.mesh, None, LumelBakeIterator(3, 7))
+    g = _lumels(w.lightmap)
+    orc = Oracle(w.scene.flat).bind_scene(w.scene)
+    lm = orc.maps()[0]
+    orc.bake_direct(lm, 3, 7)
+    assert np.array_equal(g["color"], lm.color)
+
+
+def test_ambient_occlusion_bit_exact(cuda):
+    w = scenes.room_scene(size=96)
+    rl = _relight()
+    rl.bake_direct_light(w.scene, w.mesh, None)
+    rl.bake_ambient_occlusion(w.scene, w.mesh, None, w.ao, seed=77)
+    g = _lumels(w.lightmap)
+    orc = Oracle(w.scene.flat).bind_scene(w.scene)
+    lm = orc.maps()[0]
+    orc.bake_direct(lm)
+    orc.bake_ao(lm, w.ao.samples, w.ao.occluded_fraction, w.ao.max_distance, w.ao.exponent, 77)
+    assert np.array_equal(g["color"], lm.color)
+
+
+def _small_terrain():
+    return scenes.terrain_scene(verts=64, n_boxes=80, size=128, tiles=2, fg_samples=16, passes=1, bounces=3)
+
+
+def test_photons_and_gather(cuda):
+    w = _small_terrain()
+    st = w.settings
+    rl = _relight()
+    rl.emit_photons(w.scene, st, seed=5)
+    g = _lumels(w.photonmap)
+    orc = Oracle(w.scene.flat).bind_scene(w.scene)
+    pm = orc.maps("photonmap")[0]
+    stored = orc.emit_photons([pm], st.photon_pass_count, st.photon_bounce_count, st.photon_energy_threshold,
+                              st.photon_max_distance, 5)
+    assert stored > 1000
+    assert np.array_equal(g["photons"], pm.photons)
+    np.testing.assert_allclose(g["color"], pm.color, rtol=1e-5, atol=1e-6)
+    orc.gather(pm, st.final_gather_radius)
+    np.testing.assert_allclose(g["gathered"], pm.gathered, rtol=1e-4, atol=1e-6)
+
+
+def test_final_gather_bit_exact_on_fixed_photonmap(cuda):
+    w = _small_terrain()
+    st = w.settings
+    rl = _relight()
+    rl.emit_photons(w.scene, st, seed=9)
+    g = _lumels(w.photonmap)
+    # pin the photonmap: the oracle gathers from the GPU's deposits
+    orc = Oracle(w.scene.flat).bind_scene(w.scene)
+    pm = orc.maps("photonmap")[0]
+    pm.gathered[:] = g["gathered"]
+    lm = orc.maps("lightmap")[0]
+    rl.bake_indirect_light(w.scene, w.meshes[0], None, st, seed=21)
+    gl = _lumels(w.lightmap)
+    orc.bake_indirect(lm, [pm], st.final_gather_samples, st.final_gather_distance, st.sky_color, st.ambient_color, 21)
+    assert (lm.color.sum(1) > 0).sum() > 1000
+    assert np.array_equal(gl["color"], lm.color)
+
+
+def _radiosity_inputs(size=32):
+    w = scenes.radiosity_room(size=size)
+    rl = _relight()
+    rl.device_scene(w.scene)
+    g = _lumels(w.radiancemap)
+    valid = np.nonzero(g["flags"] & 1)[0]
+    return w, rl, valid, g["position"][valid], g["normal"][valid]
+
+
+def _ff_pairwise_gpu(ds, pos, nrm, threshold):
+    import torch
+    from relight_b200 import _abi
+    n = pos.shape[0]
+    dp, dn = _dev(pos, torch), _dev(nrm, torch)
+    nnz = C.c_int64()
+    _abi.check(_abi.lib().rl_ff_pairwise(ds.handle, n, dp.data_ptr(), dn.data_ptr(), threshold, None, None, None, 0,
+                                         C.byref(nnz), None))
+    row = np.zeros(n + 1, np.int64); cols = np.zeros(max(nnz.value, 1), np.int32)
+    vals = np.zeros(max(nnz.value, 1), np.float32)
+    _abi.check(_abi.lib().rl_ff_pairwise(ds.handle, n, dp.data_ptr(), dn.data_ptr(), threshold,
+                                         row.ctypes.data, cols.ctypes.data, vals.ctypes.data, nnz.value,
+                                         C.byref(nnz), None))
+    return row, cols[:nnz.value], vals[:nnz.value]
+
+
+def test_pairwise_form_factors_bit_exact(cuda):
+    w, rl, valid, pos, nrm = _radiosity_inputs(32)
+    ds = rl.device_scene(w.scene)
+    row, cols, vals = _ff_pairwise_gpu(ds, pos, nrm, 0.1)
+    orc = Oracle(w.scene.flat).bind_scene(w.scene)
+    r2, c2, v2 = orc.ff_pairwise(pos, nrm, 0.1)
+    assert len(c2) > 100
+    assert np.array_equal(row, r2) and np.array_equal(cols, c2) and np.array_equal(vals, v2)
+
+
+def _patch_tables(w, valid):
+    W, H = w.radiancemap.width, w.radiancemap.height
+    pot = np.full(W * H, -1, np.int32)
+    pot[valid] = np.arange(len(valid), dtype=np.int32)
+    return (np.array([0], np.int32), np.array([[W, H]], np.int32), np.array([0], np.int64), pot)
+
+
+def _ff_hemi_gpu(ds, pos, nrm, rays, maxd, seed, tabs):
+    import torch
+    from relight_b200 import _abi
+    mesh_map, dims, base, pot = tabs
+    n = pos.shape[0]
+    dp, dn = _dev(pos, torch), _dev(nrm, torch)
+    nnz = C.c_int64()
+    args = (mesh_map.ctypes.data, len(dims), dims.ctypes.data, base.ctypes.data, pot.ctypes.data, pot.size)
+    _abi.check(_abi.lib().rl_ff_hemisphere(ds.handle, n, dp.data_ptr(), dn.data_ptr(), rays, maxd, seed, *args,
+                                           None, None, None, 0, C.byref(nnz), None))
+    row = np.zeros(n + 1, np.int64); cols = np.zeros(max(nnz.value, 1), np.int32)
+    vals = np.zeros(max(nnz.value, 1), np.float32)
+    _abi.check(_abi.lib().rl_ff_hemisphere(ds.handle, n, dp.data_ptr(), dn.data_ptr(), rays, maxd, seed, *args,
+                                           row.ctypes.data, cols.ctypes.data, vals.ctypes.data, nnz.value,
+                                           C.byref(nnz), None))
+    return row, cols[:nnz.value], vals[:nnz.value]
+
+
+def test_hemisphere_form_factors_bit_exact(cuda):
+    w, rl, valid, pos, nrm = _radiosity_inputs(32)
+    ds = rl.device_scene(w.scene)
+    tabs = _patch_tables(w, valid)
+    row, cols, vals = _ff_hemi_gpu(ds, pos, nrm, 128, 100.0, 3, tabs)
+    orc = Oracle(w.scene.flat).bind_scene(w.scene)
+    r2, c2, v2 = orc.ff_hemisphere(pos, nrm, 128, 100.0, 3, *tabs)
+    assert len(c2) > 1000
+    assert np.array_equal(row, r2) and np.array_equal(cols, c2) and np.array_equal(vals, v2)
+
+
+def test_radiosity_jacobi_vs_fp64(cuda):
+    import torch
+    from relight_b200 import _abi
+    w, rl, valid, pos, nrm = _radiosity_inputs(32)
+    ds = rl.device_scene(w.scene)
+    tabs = _patch_tables(w, valid)
+    row, cols, vals = _ff_hemi_gpu(ds, pos, nrm, 256, 100.0, 4, tabs)
+    n = len(row) - 1
+    rng = np.random.default_rng(5)
+    rho = rng.uniform(0.3, 0.9, (n, 3)).astype(np.float32)
+    E = np.zeros((n, 3), np.float32)
+    E[rng.choice(n, 16, replace=False)] = 1.0
+    B = torch.zeros((n, 3), dtype=torch.float32, device="cuda")
+    dr, dc, dv, dE, drho = (_dev(x, torch) for x in (row, cols, vals, E, rho))
+    _abi.check(_abi.lib().rl_radiosity_solve(n, dr.data_ptr(), dc.data_ptr(), dv.data_ptr(), dE.data_ptr(),
+                                             drho.data_ptr(), 50, B.data_ptr(), None))
+    torch.cuda.synchronize()
+    ref = jacobi_f64(row, cols, vals, E, rho, 50)
+    np.testing.assert_allclose(B.cpu().numpy(), ref, rtol=1e-4, atol=1e-6)

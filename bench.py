@@ -1,0 +1,372 @@
+"""Benchmark: Relight's photon-mapping + final-gather bake on one B200.
+
+Workload (a "step"): the 256x256-vertex fBm terrain (amplitude 5, 2x2 tiles)
+plus 2,000 boxes, 154,050 triangles, one sun + 4 point lights; one shared
+1024x1024 lightmap and photonmap.  A step runs Relight::emitPhotons
+(8 passes x 5 lights x 25,000 = 1,000,000 photons, up to 3 bounces, then
+Photonmap::gather with radius 7) and Relight::bakeIndirectLight (256 final-
+gather rays per valid lumel) — the reference's own call sequence.
+
+  value  lightmap texels baked per second, device time, all inputs resident
+         (the scene's BVH and lumels live in HBM; photonmap and lightmap
+         colours are cleared at the start of each step).
+  e2e    the same step through the C ABI with host buffers: lumel inputs
+         uploaded from pinned memory and the baked colours read back, inside
+         the timed region.
+Between timed steps L2 is flushed (a 256 MiB write, outside the step's
+events).  Multi-GPU (torchrun): every rank bakes its own copy of the job with
+its own seed (weak scaling, no collective on the data path); the time is the
+max over ranks.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+# Per-ray algorithmic bytes of a final-gather ray on this scene, measured on
+# the canonical binary SAH BVH by oracle/ray_bytes.py:
+# 48 B ray I/O + 32 B x 43.78 box tests + 48 B x 2.80 triangle tests.
+RAY_MODEL = {"n_box": 43.78, "n_tri": 2.80, "bytes_per_ray": 1583.6}
+METRIC = "lightmap texels/s (photons + gather + final gather 256 spp, 1024^2)"
+UNIT = "texels/s"
+WORKLOAD = "terrain 256^2 verts + 2000 boxes (154,050 tris), 1M photons x3 bounces, gather r7, FG 256 spp, 1024^2"
+# DRAM bytes (read + write) of one k_indirect launch, from the ncu capture in
+# profiles/ (None until captured).
+FG_DRAM_TRAFFIC = None
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks + throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        mhz, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            parts = [p.strip() for p in l.split(",")]
+            try:
+                mhz.append(float(parts[1]))
+                mx = float(parts[2])
+            except (ValueError, IndexError):
+                continue
+            for name, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(mhz) if mhz else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(mhz)}
+
+
+SMALL = False
+
+
+def build_workload(seed):
+    from relight_b200 import scenes
+    if SMALL:  # profiling case: same scene, 512^2 map, 64 spp, 2 photon passes
+        return scenes.terrain_scene(seed=2, size=512, fg_samples=64, passes=2)
+    return scenes.terrain_scene(seed=2)
+
+
+def gpu_arm(args, rank, world, local_rank):
+    import torch
+    from relight_b200 import _abi
+    from relight_b200.device import Relight, _map_array
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    stream = torch.cuda.current_stream(dev)
+    sh = stream.cuda_stream
+    w = build_workload(rank)
+    st = w.settings
+    rl = Relight(stream=sh, seed=1000 + rank)
+    ds = rl.device_scene(w.scene)
+    torch.cuda.synchronize()
+    lmap, pmap = w.lightmap._device, w.photonmap._device
+    L = _abi.lib()
+    flat = w.scene.flat
+    lights = C.c_void_p(flat.lights.ctypes.data)
+    maps = _map_array([pmap])
+    sky = (C.c_float * 3)(*[float(x) for x in st.sky_color])
+    amb = (C.c_float * 3)(*[float(x) for x in st.ambient_color])
+    valid = lmap.valid_count()
+    rays_per_step = valid * st.final_gather_samples
+    launches_per_step = 3  # k_photons, k_gather, k_indirect
+
+    ev = lambda: torch.cuda.Event(enable_timing=True)
+
+    def step(seed, fg_events=None):
+        _abi.check(L.rl_map_clear(pmap.handle, 1, 1, sh))
+        _abi.check(L.rl_map_clear(lmap.handle, 1, 0, sh))
+        _abi.check(L.rl_emit_photons(ds.handle, maps, 1, lights, len(flat.lights), st.photon_pass_count,
+                                     st.photon_bounce_count, st.photon_energy_threshold, st.photon_max_distance,
+                                     seed, None, sh))
+        _abi.check(L.rl_photonmap_gather(pmap.handle, st.final_gather_radius, sh))
+        if fg_events:
+            fg_events[0].record(stream)
+        _abi.check(L.rl_bake_indirect(ds.handle, lmap.handle, maps, 1, st.final_gather_samples,
+                                      st.final_gather_distance, sky, amb, seed + 1, 0, 1, sh))
+        if fg_events:
+            fg_events[1].record(stream)
+
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    for i in range(args.warmup):
+        step(7 + 2 * i)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    step_ms, fg_ms = [], []
+    with ClockSampler(local_rank) as clocks:
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        for i in range(args.steps):
+            flush.zero_()
+            e0, e1, f0, f1 = ev(), ev(), ev(), ev()
+            e0.record(stream)
+            step(1001 + 2 * i, (f0, f1))
+            e1.record(stream)
+            torch.cuda.synchronize()
+            step_ms.append(e0.elapsed_time(e1))
+            fg_ms.append(f0.elapsed_time(f1))
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+    total_ms = sum(step_ms)
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    value = valid * args.steps * world / (total_ms / 1e3)
+
+    # e2e: host buffers through the C ABI (lumel inputs up, baked colours down)
+    host = lmap.download(sh, fields=("flags", "position", "normal"))
+    phost = pmap.download(sh, fields=("flags", "position", "normal"))
+    pin = {}
+    for tag, src in (("l", host), ("p", phost)):
+        for k, a in src.items():
+            t = torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+            pin[tag + k] = t
+    out_color = torch.empty((lmap.width * lmap.height, 3), dtype=torch.float32).pin_memory()
+    h2d = sum(t.numel() * t.element_size() for t in pin.values())
+    d2h = out_color.numel() * 4
+
+    def e2e_step(seed):
+        _abi.check(L.rl_map_upload(lmap.handle, C.c_void_p(pin["lflags"].data_ptr()), None,
+                                   C.c_void_p(pin["lposition"].data_ptr()), C.c_void_p(pin["lnormal"].data_ptr()),
+                                   None, None, None, sh))
+        _abi.check(L.rl_map_upload(pmap.handle, C.c_void_p(pin["pflags"].data_ptr()), None,
+                                   C.c_void_p(pin["pposition"].data_ptr()), C.c_void_p(pin["pnormal"].data_ptr()),
+                                   None, None, None, sh))
+        step(seed)
+        _abi.check(L.rl_map_download(lmap.handle, None, None, None, None, C.c_void_p(out_color.data_ptr()), None,
+                                     None, sh))
+
+    e2e_step(5)
+    torch.cuda.synchronize()
+    e2e_ms = []
+    for i in range(args.steps):
+        flush.zero_()
+        e0, e1 = ev(), ev()
+        e0.record(stream)
+        e2e_step(3001 + 2 * i)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms.append(e0.elapsed_time(e1))
+    e2e_total = sum(e2e_ms)
+    if world > 1:
+        t = torch.tensor([e2e_total], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_total = float(t.item())
+    e2e_value = valid * args.steps * world / (e2e_total / 1e3)
+
+    peak, peak_kind = load_peaks()
+    fg_avg_s = (sum(fg_ms) / len(fg_ms)) / 1e3
+    alg_bytes = rays_per_step * RAY_MODEL["bytes_per_ray"]
+    achieved = alg_bytes / fg_avg_s / 1e9
+    result = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded fBm terrain + boxes)",
+        "config": {"workload": WORKLOAD, "lightmap": [lmap.width, lmap.height], "valid_texels": valid,
+                   "photons": int(st.photon_pass_count * 125000), "fg_samples": st.final_gather_samples, "triangles": flat.ntris,
+                   "parallelism": f"replicas x{world}", "l2": "flushed between steps (256 MiB write)"},
+        "grays_per_s": rays_per_step * args.steps * world / (total_ms / 1e3) / 1e9,
+        "fg_ms": sum(fg_ms) / len(fg_ms),
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "ms_per_step": e2e_total / args.steps},
+        "roofline": {"kernel": "k_indirect (final gather)", "bound": "hbm", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                     "traffic": FG_DRAM_TRAFFIC,
+                     "algorithmic_bytes_per_launch": alg_bytes, "bytes_per_ray": RAY_MODEL["bytes_per_ray"]},
+        "gpu_launches": launches_per_step * args.steps,
+        "clocks": clocks.summary(),
+        "bvh": ds.bvh_stats(),
+    }
+    return result, w
+
+
+def cpu_baseline(w, budget_s=20.0, nthreads=None):
+    """The reference baker (oracle/_ref/librelight_ref_fast.so, compiled
+    from the reference's sources, project CPU BVH in place of Embree) timed
+    on this host's cores over a bounded sample of the same step: one photon
+    pass of eight (x8), the full gather, and the final gather on every k-th
+    lumel via LumelBakeIterator fan-out (x k)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_bind as ob
+    if not os.path.exists(ob.REF_FAST_LIB):
+        return None, "reference build missing"
+    nthreads = nthreads or os.cpu_count() or 1
+    st = w.settings
+    ref = ob.RefScene(w.scene, fast=True)
+    L = ref.lib
+    L.ref_set_rand(0, 1)
+    t0 = time.perf_counter()
+    L.ref_emit_photons(ref.h, 1, st.photon_bounce_count, st.photon_energy_threshold, st.photon_max_distance,
+                       st.final_gather_radius)
+    t_photons_gather = time.perf_counter() - t0
+    # gather alone, to split the photon time from the gather time
+    pm = ref.maps[id(w.photonmap)]
+    t0 = time.perf_counter()
+    L.ref_photonmap_gather(ref.h, pm, st.final_gather_radius)
+    t_gather = time.perf_counter() - t0
+    t_photon_pass = max(t_photons_gather - t_gather, 0.0)
+    sky = np.asarray(st.sky_color, np.float32); amb = np.asarray(st.ambient_color, np.float32)
+    lm = ref.lumels(w.lightmap)
+    valid = int((lm.flags & 1).sum())
+    npix = w.lightmap.width * w.lightmap.height
+    # size the final-gather sample to the budget: probe with a sparse sample first
+    div = 4096
+    t0 = time.perf_counter()
+    L.ref_bake_sampled(ref.h, 2, ref.mesh(w.meshes[0]), nthreads, div, 0, 0.8, 1.0, 1.0, st.final_gather_samples,
+                       st.final_gather_distance, st.final_gather_radius, ob.ptr(sky), ob.ptr(amb))
+    t_probe = time.perf_counter() - t0
+    per_lumel = t_probe / max(npix / div, 1)
+    target = max(budget_s - t_photons_gather, 2.0)
+    div2 = int(max(16, min(4096, per_lumel * npix / target)))
+    t0 = time.perf_counter()
+    L.ref_bake_sampled(ref.h, 2, ref.mesh(w.meshes[0]), nthreads, div2, 0, 0.8, 1.0, 1.0, st.final_gather_samples,
+                       st.final_gather_distance, st.final_gather_radius, ob.ptr(sky), ob.ptr(amb))
+    t_fg = (time.perf_counter() - t0) * div2
+    step_s = st.photon_pass_count * t_photon_pass + t_gather + t_fg
+    return {"value": valid / step_s, "unit": UNIT, "cores": nthreads, "kind": "reference",
+            "sample": (f"reference C++ (Embree unavailable: project CPU BVH): 1 of {st.photon_pass_count} photon "
+                       f"passes (x{st.photon_pass_count}, single-threaded as in Relight::emitPhotons), full "
+                       f"gather, final gather on every {div2}th lumel over {nthreads} threads (x{div2})"),
+            "est_step_s": step_s, "photon_pass_s": t_photon_pass, "gather_s": t_gather, "fg_s": t_fg}, None
+
+
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return None
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_bind as ob
+    if not os.path.exists(ob.REF_FAST_LIB):
+        return {"impl": "reference", "unavailable": "oracle/_ref/librelight_ref_fast.so was not built"}
+    w = build_workload(0)
+    for _ in range(args.warmup):
+        cpu_baseline(w, budget_s=3.0)
+    vals = []
+    details = None
+    for _ in range(args.steps):
+        details, _err = cpu_baseline(w, budget_s=10.0)
+        vals.append(details["est_step_s"])
+    valid = int(details["value"] * details["est_step_s"])
+    total = sum(vals)
+    value = valid * args.steps / total
+    cb = dict(details)
+    cb["value"] = value
+    return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded fBm terrain + boxes)",
+            "config": {"workload": WORKLOAD, "parallelism": f"{cb['cores']} host threads"},
+            "impl": "reference", "cpu_baseline": cb,
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--small", action="store_true", help="512^2 / 64 spp / 2 passes case for ncu captures")
+    args = ap.parse_args()
+    global SMALL
+    SMALL = args.small
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        out = reference_arm(args, rank, world)
+        if out is not None:
+            print(json.dumps(out), flush=True)
+        return
+    import torch
+    if world > 1:
+        import datetime
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                             device_id=torch.device("cuda", local_rank))
+    result, w = gpu_arm(args, rank, world, local_rank)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb, err = cpu_baseline(w)
+        result["cpu_baseline"] = cb if cb else {"unavailable": err}
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,7 +1,8 @@
 """ctypes bindings of the oracle (oracle/liboracle.so, the C restatement) and
 of the reference baker compiled from its own sources
 (oracle/_ref/librelight_ref.so).  Test infrastructure: the checkers of the
-CUDA library, never the thing measured.
+CUDA library, and the CPU baseline that bench.py times beside it — never the
+thing the GPU arm measures.
 """
 from __future__ import annotations
 
@@ -14,12 +15,11 @@ import numpy as np
 from relight_b200 import _abi
 from relight_b200.api import FlatScene, Scene
 
-ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-ORACLE_DIR = os.path.join(ROOT, "oracle")
+ORACLE_DIR = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(ORACLE_DIR)
 ORACLE_LIB = os.path.join(ORACLE_DIR, "liboracle.so")
 REF_LIB = os.path.join(ORACLE_DIR, "_ref", "librelight_ref.so")
 REF_FAST_LIB = os.path.join(ORACLE_DIR, "_ref", "librelight_ref_fast.so")
-REFERENCE_SRC = "/root/reference/src/relight"
 
 _P = C.c_void_p
 

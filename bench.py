@@ -229,6 +229,8 @@ def gpu_arm(args, rank, world, local_rank):
     e2e_value = valid * args.steps * world / (e2e_total / 1e3)
 
     peak, peak_kind = load_peaks()
+    l2 = C.c_double()
+    _abi.check(L.rl_measure_read_bandwidth(48 << 20, 50, C.byref(l2)))
     fg_avg_s = (sum(fg_ms) / len(fg_ms)) / 1e3
     alg_bytes = rays_per_step * RAY_MODEL["bytes_per_ray"]
     achieved = alg_bytes / fg_avg_s / 1e9
@@ -246,7 +248,8 @@ def gpu_arm(args, rank, world, local_rank):
         "roofline": {"kernel": "k_indirect (final gather)", "bound": "hbm", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
                      "traffic": FG_DRAM_TRAFFIC,
-                     "algorithmic_bytes_per_launch": alg_bytes, "bytes_per_ray": RAY_MODEL["bytes_per_ray"]},
+                     "algorithmic_bytes_per_launch": alg_bytes, "bytes_per_ray": RAY_MODEL["bytes_per_ray"],
+                     "l2_read_gbs_measured": l2.value, "frac_of_l2": achieved / l2.value},
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clocks.summary(),
         "bvh": ds.bvh_stats(),

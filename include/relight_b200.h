@@ -226,6 +226,25 @@ int rl_ff_hemisphere(const rl_scene* scene, int n, const float* d_pos, const flo
 int rl_radiosity_solve(int n, const int64_t* d_row_ptr, const int32_t* d_cols, const float* d_vals,
                        const float* d_E, const float* d_rho, int iters, float* d_B, void* stream);
 
+/* ---------------------------------------------------------------- tuning */
+
+/* Launch parameters of the ray-stream kernels (final gather, AO), chosen by
+   the autotuner (relight_b200/autotune.py); process-wide.  They change
+   scheduling only, never results.  No counterpart in the reference.
+     *_REFILL: a warp restarts finished lanes' rays once this many of its
+               live lanes (1..32) have finished;
+     *_BLOCK:  threads per block (64, 128 or 256). */
+enum { RL_TUNE_FG_REFILL = 0, RL_TUNE_FG_BLOCK = 1, RL_TUNE_AO_REFILL = 2, RL_TUNE_AO_BLOCK = 3 };
+int rl_tune_set(int param, int value);
+int rl_tune_get(int param, int* value);
+
+/* ------------------------------------------------------------ measurement */
+
+/* Device read bandwidth (GB/s) of `bytes` streamed `iters` times with 16-byte
+   loads; below the L2 size this is the L2 bandwidth the traversal kernels
+   draw on.  A measurement utility with no counterpart in the reference. */
+int rl_measure_read_bandwidth(size_t bytes, int iters, double* gbs);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,60 @@
+"""Autotuner for the ray-stream kernels' launch parameters (rl_tune_set):
+the warp refill threshold and the block size.  It times one kernel call per
+candidate on the caller's own scene and map (device events on the given
+stream) and keeps the fastest.  The parameters change only scheduling, so
+every candidate produces bit-identical lightmaps; the test suite checks
+that.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import itertools
+
+from . import _abi
+
+REFILLS = (1, 4, 8, 12, 16, 20, 24, 28, 32)
+BLOCKS = (64, 128, 256)
+
+
+KERNELS = {"indirect": (_abi.TUNE_FG_REFILL, _abi.TUNE_FG_BLOCK), "ao": (_abi.TUNE_AO_REFILL, _abi.TUNE_AO_BLOCK)}
+
+
+def get(kernel="indirect"):
+    v = C.c_int()
+    out = {}
+    for name, p in zip(("refill", "block"), KERNELS[kernel]):
+        _abi.check(_abi.lib().rl_tune_get(p, C.byref(v)))
+        out[name] = v.value
+    return out
+
+
+def set(refill=None, block=None, kernel="indirect"):
+    pr, pb = KERNELS[kernel]
+    if refill is not None:
+        _abi.check(_abi.lib().rl_tune_set(pr, int(refill)))
+    if block is not None:
+        _abi.check(_abi.lib().rl_tune_set(pb, int(block)))
+
+
+def tune(run, kernel="indirect", refills=REFILLS, blocks=BLOCKS, reps=2, stream=None):
+    """`run()` enqueues one call of `kernel` ("indirect" or "ao") on `stream`
+    (a torch stream, None = the current one).  Returns (best, table), table
+    mapping (refill, block) -> milliseconds; the best setting is left applied."""
+    import torch
+    st = stream or torch.cuda.current_stream()
+    table = {}
+    for refill, block in itertools.product(refills, blocks):
+        set(refill, block, kernel)
+        run()
+        ms = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            run()
+            e1.record(st)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        table[(refill, block)] = min(ms)
+    best = min(table, key=table.get)
+    set(best[0], best[1], kernel)
+    return {"refill": best[0], "block": best[1], "ms": table[best]}, table

@@ -60,6 +60,11 @@ int fail(int code, const char* fmt, ...) {
 
 inline cudaStream_t S(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
+// Launch tuning (rl_tune_set): per ray-stream kernel, the number of lanes a
+// warp waits for before refilling rays and the threads per block.  Defaults
+// are the autotuner's picks on the terrain final-gather / room AO workloads.
+int g_tune[4] = {24, 64, 32, 128};
+
 inline unsigned blocks_for(long long n, int threads) { return (unsigned)((n + threads - 1) / threads); }
 
 template <typename T>
@@ -135,6 +140,22 @@ extern "C" int rl_last_error(char* buf, size_t len) {
 }
 
 extern "C" const char* rl_version(void) { return "relight_b200 0.1 (sm_100a)"; }
+
+extern "C" int rl_tune_set(int param, int value) {
+    bool refill = param == RL_TUNE_FG_REFILL || param == RL_TUNE_AO_REFILL;
+    bool block = param == RL_TUNE_FG_BLOCK || param == RL_TUNE_AO_BLOCK;
+    if ((refill && value >= 1 && value <= 32) || (block && (value == 64 || value == 128 || value == 256)))
+        g_tune[param] = value;
+    else
+        return fail(RL_INVALID_CALL, "rl_tune_set: bad parameter %d or value %d", param, value);
+    return RL_OK;
+}
+
+extern "C" int rl_tune_get(int param, int* value) {
+    if (!value || param < 0 || param > 3) return fail(RL_INVALID_CALL, "rl_tune_get: bad parameter");
+    *value = g_tune[param];
+    return RL_OK;
+}
 
 // ------------------------------------------------------------- scene
 
@@ -655,20 +676,44 @@ extern "C" int rl_bake_direct(const rl_scene* s, rl_map* lm, const rl_light* lig
 
 // ------------------------------------------------------------------ AO
 
-// AmbientOcclusion::bakeLumel (baker/AmbientOcclusion.cpp:46-66).
-__global__ void k_ao(DevScene s, DevMap m, int samples, float fraction, float maxd, float exponent, uint2 key,
-                     int first, int step, long long count, int* status) {
+// AmbientOcclusion::bakeLumel (baker/AmbientOcclusion.cpp:46-66): the
+// lumel's samples as one lane's ray stream (first-hit rays).
+struct AoGen {
+    V3 pos, nrm;
+    uint2 key;
+    uint32_t item;
+    int j, samples, occluded;
+    float maxd;
+    __device__ bool next(V3& o, V3& d, float& tnear, float& tfar) {
+        if (j >= samples) return false;
+        V3 dir = random_hemisphere(nrm, key, item, (uint32_t)j, kTagAO);
+        segment_ray(pos, dir, maxd, o, d, tnear, tfar);
+        j++;
+        return true;
+    }
+    __device__ void finish(const RayHit& h) {
+        if (h.gid >= 0) occluded++;
+    }
+};
+
+__global__ void __launch_bounds__(256) k_ao(DevScene s, DevMap m, int samples, float fraction, float maxd,
+                                            float exponent, uint2 key, int first, int step, long long count,
+                                            int refill, int* status) {
     long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (k >= count) return;
     long long i = first + k * step;
+    AoGen g;
+    g.pos = ld3(m.position + 3 * i);
+    g.nrm = ld3(m.normal + 3 * i);
+    g.key = key;
+    g.item = (uint32_t)i;
+    g.j = 0;
+    g.samples = (m.flags[i] & 1) ? samples : 0;
+    g.occluded = 0;
+    g.maxd = maxd;
+    ray_loop<true>(s, g, refill, status);
     if (!(m.flags[i] & 1)) return;
-    V3 pos = ld3(m.position + 3 * i), nrm = ld3(m.normal + 3 * i);
-    int occluded = 0;
-    for (int j = 0; j < samples; j++) {
-        V3 dir = random_hemisphere(nrm, key, (uint32_t)i, (uint32_t)j, kTagAO);
-        if (segment_blocked(s, pos, add3(pos, mul3(dir, maxd)), 0, status)) occluded++;
-    }
-    float value = 1.0f - occluded / (samples * fraction);
+    float value = 1.0f - g.occluded / (samples * fraction);
     if (fabsf(1.0f - exponent) > 0.01f) value = powf(value, exponent);
     float* col = m.color + 3 * i;
     col[0] = col[0] * value; col[1] = col[1] * value; col[2] = col[2] * value;
@@ -682,8 +727,9 @@ extern "C" int rl_bake_ao(const rl_scene* s, rl_map* lm, int samples, float frac
     long long count = iter_count(n, first, step);
     if (count == 0) return RL_OK;
     uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
-    k_ao<<<blocks_for(count, 128), 128, 0, S(stream)>>>(s->dev, lm->dev, samples, fraction, maxd, exponent, key,
-                                                        first, step, count, s->d_status);
+    int bs = g_tune[RL_TUNE_AO_BLOCK];
+    k_ao<<<blocks_for(count, bs), bs, 0, S(stream)>>>(s->dev, lm->dev, samples, fraction, maxd, exponent, key,
+                                                      first, step, count, g_tune[RL_TUNE_AO_REFILL], s->d_status);
     CK_LAUNCH("k_ao");
     return RL_OK;
 }
@@ -857,41 +903,77 @@ struct GatherMaps {
     DevMap maps[kMaxPhotonmaps];
 };
 
-// IndirectLight::bakeLumel (baker/IndirectLight.cpp:47-75).
-__global__ void k_indirect(DevScene s, DevMap m, const __grid_constant__ GatherMaps G, int samples, float maxd, V3 sky,
-                           V3 amb, uint2 key, int first, int step, long long count, int* status) {
-    long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (k >= count) return;
-    long long i = first + k * step;
-    if (!(m.flags[i] & 1)) return;
-    V3 pos = ld3(m.position + 3 * i), nrm = ld3(m.normal + 3 * i);
-    float gr = 0.f, gg = 0.f, gb = 0.f;
-    for (int j = 0; j < samples; j++) {
-        V3 dir = random_hemisphere(nrm, key, (uint32_t)i, (uint32_t)j, kTagFG);
+// IndirectLight::bakeLumel (baker/IndirectLight.cpp:47-75): the lumel's
+// final-gather samples as one lane's ray stream; each closest hit is shaded
+// (hit normal and lightmap uv by Barycentric(u, v), photonmap lookup) as soon
+// as its ray ends, in sample order.
+struct FgGen {
+    const DevScene* s;
+    const GatherMaps* G;
+    V3 pos, nrm, dir, sky, amb;
+    uint2 key;
+    uint32_t item;
+    int j, samples;
+    float maxd, influence, gr, gg, gb;
+    __device__ bool next(V3& o, V3& d, float& tnear, float& tfar) {
+        if (j >= samples) return false;
+        dir = random_hemisphere(nrm, key, item, (uint32_t)j, kTagFG);
         float dp = dot3(nrm, dir);
-        float influence = dp > 0.0f ? dp : 0.0f;
-        SegHit h;
-        trace_segment(s, pos, add3(pos, mul3(dir, maxd)), kHitUv | kHitNormal, h, status);
-        if (!h.hit) {
+        influence = dp > 0.0f ? dp : 0.0f;
+        segment_ray(pos, dir, maxd, o, d, tnear, tfar);
+        j++;
+        return true;
+    }
+    __device__ void finish(const RayHit& h) {
+        if (h.gid < 0) {
             gr = gr + (sky.x * influence + amb.x);
             gg = gg + (sky.y * influence + amb.y);
             gb = gb + (sky.z * influence + amb.z);
-            continue;
+            return;
         }
-        if (dot3(dir, h.normal) >= 0.0f) continue;
-        int slot = s.mesh_photonmap[h.mesh];
-        if (slot >= 0 && slot < G.nmaps) {
-            const DevMap& P = G.maps[slot];
-            int ti = lumel_at_uv(P.width, P.height, h.uv);
+        int4 f = __ldg(s->tri_vidx + h.gid);
+        V3 hn = interp3(s->nrm, f, h.u, h.v);
+        if (dot3(dir, hn) >= 0.0f) return;
+        int slot = s->mesh_photonmap[f.w];
+        if (slot >= 0 && slot < G->nmaps) {
+            const DevMap& P = G->maps[slot];
+            float2 uv = interp2(s->uv1, f, h.u, h.v);
+            int ti = lumel_at_uv(P.width, P.height, uv);
             const float* g = P.gathered + 3 * (size_t)ti;
             gr = gr + (g[0] * influence + amb.x);
             gg = gg + (g[1] * influence + amb.y);
             gb = gb + (g[2] * influence + amb.z);
         }
     }
+};
+
+__global__ void __launch_bounds__(256) k_indirect(DevScene s, DevMap m, const __grid_constant__ GatherMaps G,
+                                                  int samples, float maxd, V3 sky, V3 amb, uint2 key, int first,
+                                                  int step, long long count, int refill, int* status) {
+    long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    long long i = first + k * step;
+    bool valid = (m.flags[i] & 1) != 0;
+    FgGen g;
+    g.s = &s;
+    g.G = &G;
+    g.pos = ld3(m.position + 3 * i);
+    g.nrm = ld3(m.normal + 3 * i);
+    g.sky = sky;
+    g.amb = amb;
+    g.key = key;
+    g.item = (uint32_t)i;
+    g.j = 0;
+    g.samples = valid ? samples : 0;
+    g.maxd = maxd;
+    g.gr = g.gg = g.gb = 0.f;
+    g.influence = 0.f;
+    g.dir = mk3(0.f, 0.f, 0.f);
+    ray_loop<false>(s, g, refill, status);
+    if (!valid) return;
     float ns = (float)samples;
     float* col = m.color + 3 * i;
-    col[0] = col[0] + gr / ns; col[1] = col[1] + gg / ns; col[2] = col[2] + gb / ns;
+    col[0] = col[0] + g.gr / ns; col[1] = col[1] + g.gg / ns; col[2] = col[2] + g.gb / ns;
 }
 
 extern "C" int rl_bake_indirect(const rl_scene* s, rl_map* lm, rl_map* const* maps, int nmaps, int samples,
@@ -914,8 +996,9 @@ extern "C" int rl_bake_indirect(const rl_scene* s, rl_map* lm, rl_map* const* ma
     V3 skyv = {sky ? sky[0] : 0.f, sky ? sky[1] : 0.f, sky ? sky[2] : 0.f};
     V3 ambv = {ambient ? ambient[0] : 0.f, ambient ? ambient[1] : 0.f, ambient ? ambient[2] : 0.f};
     uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
-    k_indirect<<<blocks_for(count, 128), 128, 0, st>>>(s->dev, lm->dev, G, samples, maxd, skyv, ambv, key, first,
-                                                      step, count, s->d_status);
+    int bs = g_tune[RL_TUNE_FG_BLOCK];
+    k_indirect<<<blocks_for(count, bs), bs, 0, st>>>(s->dev, lm->dev, G, samples, maxd, skyv, ambv, key, first,
+                                                    step, count, g_tune[RL_TUNE_FG_REFILL], s->d_status);
     CK_LAUNCH("k_indirect");
     return RL_OK;
 }
@@ -1248,5 +1331,47 @@ extern "C" int rl_radiosity_solve(int n, const int64_t* d_row_ptr, const int32_t
         std::swap(src, dst);
     }
     if (src != d_B) CK(cudaMemcpyAsync(d_B, src, 12 * (size_t)n, cudaMemcpyDeviceToDevice, st));
+    return RL_OK;
+}
+
+// ------------------------------------------------------------ bandwidth probe
+
+// Streams `bytes` of device memory `iters` times with 16-byte loads (a
+// grid of 4 x 148 x 8 blocks of 256 threads); with bytes well under the
+// 126 MB L2 the loads are served from L2 after the first pass.
+__global__ void k_read_probe(const float4* __restrict__ buf, size_t n4, int iters, float* sink) {
+    float acc = 0.f;
+    size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (int it = 0; it < iters; it++)
+        for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n4; i += stride) {
+            float4 v = __ldcg(buf + i);
+            acc += v.x + v.y + v.z + v.w;
+        }
+    if (acc == 1234.5f) *sink = acc;
+}
+
+extern "C" int rl_measure_read_bandwidth(size_t bytes, int iters, double* gbs) {
+    if (!gbs || bytes < 4096 || iters <= 0) return fail(RL_INVALID_CALL, "rl_measure_read_bandwidth: bad arguments");
+    float4* buf = nullptr;
+    float* sink = nullptr;
+    CK(cudaMalloc(&buf, bytes));
+    CK(cudaMalloc(&sink, sizeof(float)));
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaMemset(buf, 0, bytes));
+    size_t n4 = bytes / 16;
+    k_read_probe<<<4 * 148 * 8, 256>>>(buf, n4, 1, sink);  // warm
+    CK(cudaEventRecord(e0));
+    k_read_probe<<<4 * 148 * 8, 256>>>(buf, n4, iters, sink);
+    CK(cudaEventRecord(e1));
+    CK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, e0, e1));
+    *gbs = (double)bytes * iters / (ms * 1e-3) / 1e9;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(buf);
+    cudaFree(sink);
     return RL_OK;
 }

@@ -261,3 +261,23 @@ def test_radiosity_jacobi_vs_fp64(cuda):
     torch.cuda.synchronize()
     ref = jacobi_f64(row, cols, vals, E, rho, 50)
     np.testing.assert_allclose(B.cpu().numpy(), ref, rtol=1e-4, atol=1e-6)
+
+
+def test_launch_tuning_changes_no_result(cuda):
+    """The autotuner's knobs (refill threshold, block size) reschedule rays
+    only: every setting bakes the same bits."""
+    from relight_b200 import autotune
+    w = scenes.room_scene(size=64)
+    saved = autotune.get("ao"), autotune.get("indirect")
+    colors = []
+    try:
+        for refill, block in ((1, 64), (13, 128), (32, 256)):
+            autotune.set(refill, block, "ao")
+            rl = _relight()
+            ws = scenes.room_scene(size=64)
+            rl.bake_ambient_occlusion(ws.scene, ws.mesh, None, ws.ao, seed=3)
+            colors.append(_lumels(ws.lightmap)["color"])
+    finally:
+        autotune.set(saved[0]["refill"], saved[0]["block"], "ao")
+        autotune.set(saved[1]["refill"], saved[1]["block"], "indirect")
+    assert all(np.array_equal(colors[0], c) for c in colors[1:])

@@ -226,6 +226,22 @@ int rl_ff_hemisphere(const rl_scene* scene, int n, const float* d_pos, const flo
 int rl_radiosity_solve(int n, const int64_t* d_row_ptr, const int32_t* d_cols, const float* d_vals,
                        const float* d_E, const float* d_rho, int iters, float* d_B, void* stream);
 
+/* The same solve for callers that cannot allocate device memory: a plugin
+   inside a host application (a game engine or an editor) that owns every
+   device allocation itself, or a bake server that reserved its HBM when the
+   request was admitted.  This entry point calls no cudaMalloc, cudaFree or
+   allocating routine; its ping-pong buffer is a fixed array of
+   RL_SOLVE_NOALLOC_MAX_PATCHES x 3 floats (768 KiB) that every GPU loading
+   this library holds until the process exits.  Larger `n` is rejected with
+   RL_INVALID_CALL.  The first call on a device looks the array's address up
+   (once per device, with that device current); make that first call before
+   any stream capture.  All calls share the one array, so calls whose work
+   overlaps on the GPU race; run them on one stream or one at a time.  No
+   counterpart in the reference. */
+#define RL_SOLVE_NOALLOC_MAX_PATCHES 65536
+int rl_radiosity_solve_noalloc(int n, const int64_t* d_row_ptr, const int32_t* d_cols, const float* d_vals,
+                               const float* d_E, const float* d_rho, int iters, float* d_B, void* stream);
+
 /* ---------------------------------------------------------------- tuning */
 
 /* Launch parameters of the ray-stream kernels (final gather, AO), chosen by

@@ -17,6 +17,7 @@ RL_OK, RL_INVALID_CALL, RL_NOT_IMPLEMENTED, RL_OUT_OF_MEMORY, RL_CUDA_ERROR, RL_
 HIT_POINT, HIT_UV, HIT_COLOR, HIT_NORMAL, HIT_USE_ALPHA = 1, 2, 4, 8, 16
 HIT_ALL = 15
 TUNE_FG_REFILL, TUNE_FG_BLOCK, TUNE_AO_REFILL, TUNE_AO_BLOCK = 0, 1, 2, 3
+SOLVE_NOALLOC_MAX_PATCHES = 65536
 
 
 class SceneDesc(C.Structure):
@@ -99,6 +100,7 @@ SIGNATURES = {
     "rl_ff_pairwise": (_I, [_P, _I, _P, _P, _F, _P, _P, _P, _I64, _P, _P]),
     "rl_ff_hemisphere": (_I, [_P, _I, _P, _P, _I, _F, _U64, _P, _I, _P, _P, _P, _I64, _P, _P, _P, _I64, _P, _P]),
     "rl_radiosity_solve": (_I, [_I, _P, _P, _P, _P, _P, _I, _P, _P]),
+    "rl_radiosity_solve_noalloc": (_I, [_I, _P, _P, _P, _P, _P, _I, _P, _P]),
     "rl_measure_read_bandwidth": (_I, [C.c_size_t, _I, _P]),
     "rl_tune_set": (_I, [_I, _I]),
     "rl_tune_get": (_I, [_I, _P]),

@@ -15,6 +15,7 @@
 
 #include <algorithm>
 #include <cstdarg>
+#include <mutex>
 #include <cstdio>
 #include <cstring>
 #include <new>
@@ -1322,6 +1323,67 @@ extern "C" int rl_radiosity_solve(int n, const int64_t* d_row_ptr, const int32_t
     float* tmp = nullptr;
     int rc = scratch(sb, &tmp, 3 * (size_t)n, st);
     if (rc) return rc;
+    float* src = d_B;
+    float* dst = tmp;
+    unsigned grid = blocks_for((long long)n * 32, 256);
+    for (int it = 0; it < iters; it++) {
+        k_jacobi<<<grid, 256, 0, st>>>(n, d_row_ptr, d_cols, d_vals, d_E, d_rho, src, dst);
+        CK_LAUNCH("k_jacobi");
+        std::swap(src, dst);
+    }
+    if (src != d_B) CK(cudaMemcpyAsync(d_B, src, 12 * (size_t)n, cudaMemcpyDeviceToDevice, st));
+    return RL_OK;
+}
+
+// ------------------------------------------------- solve without allocation
+
+// Ping-pong buffer of rl_radiosity_solve_noalloc: a fixed array in device
+// memory, reserved when the library is loaded (on every GPU that loads it,
+// until the process exits) so that the solve itself never allocates.
+static __device__ __align__(256) float g_solve_scratch[3 * RL_SOLVE_NOALLOC_MAX_PATCHES];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_scratch_mutex;
+float* g_scratch_ptr[kMaxDevices] = {};  // device address of g_solve_scratch, per device
+}  // namespace
+
+// Host code only sees a host-side stand-in for g_solve_scratch; the device
+// address comes from cudaGetSymbolAddress, looked up once per device with
+// that device current.
+static int solve_scratch(float** out) {
+    int dev = -1;
+    CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) return fail(RL_INVALID_CALL, "device ordinal %d out of range", dev);
+    std::lock_guard<std::mutex> lock(g_scratch_mutex);
+    if (!g_scratch_ptr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_solve_scratch);
+        if (e != cudaSuccess || !p)
+            return fail(RL_CUDA_ERROR, "cudaGetSymbolAddress(g_solve_scratch) failed on device %d: %s", dev,
+                        cudaGetErrorString(e));
+        g_scratch_ptr[dev] = (float*)p;
+    }
+    *out = g_scratch_ptr[dev];
+    return RL_OK;
+}
+
+extern "C" int rl_radiosity_solve_noalloc(int n, const int64_t* d_row_ptr, const int32_t* d_cols,
+                                          const float* d_vals, const float* d_E, const float* d_rho, int iters,
+                                          float* d_B, void* stream) {
+    if (n < 0 || iters < 0 || (n > 0 && (!d_row_ptr || !d_E || !d_rho || !d_B)))
+        return fail(RL_INVALID_CALL, "rl_radiosity_solve_noalloc: bad arguments");
+    if (n > RL_SOLVE_NOALLOC_MAX_PATCHES)
+        return fail(RL_INVALID_CALL, "rl_radiosity_solve_noalloc: %d patches exceed the fixed maximum of %d "
+                                     "(use rl_radiosity_solve)", n, RL_SOLVE_NOALLOC_MAX_PATCHES);
+    float* tmp = nullptr;
+    int rc = solve_scratch(&tmp);
+    if (rc) return rc;
+    cudaStream_t st = S(stream);
+    if (n == 0) return RL_OK;
+    CK(cudaMemcpyAsync(d_B, d_E, 12 * (size_t)n, cudaMemcpyDeviceToDevice, st));
+    // Every iteration writes all 3n values of its destination before the next
+    // one reads them, so the scratch array needs no clearing.
     float* src = d_B;
     float* dst = tmp;
     unsigned grid = blocks_for((long long)n * 32, 256);

@@ -279,6 +279,7 @@ def _load_ref(path):
         "ref_create": (_P, []), "ref_destroy": (None, [_P]), "ref_set_rand": (None, [I, C.c_uint]),
         "ref_add_material": (I, [_P, F, F, F, I, I, I, _P]),
         "ref_add_mesh": (I, [_P, I, _P, _P, _P, _P, _P, I, _P]),
+        "ref_add_mesh_transformed": (I, [_P, I, _P, _P, _P, _P, _P, I, _P, _P]),
         "ref_mesh_vertices": (None, [_P, I, _P, _P]),
         "ref_add_point_light": (I, [_P, _P, F, _P, F, I]),
         "ref_add_spot_light": (I, [_P, _P, _P, F, F, _P, F, I]),
@@ -338,8 +339,8 @@ class RefScene:
         self.mesh_index = {}
         for i, inst in enumerate(scene.meshes):
             src, transform, material = inst.source
-            if transform is not None or material is not None:
-                raise NotImplementedError("the reference driver adds meshes with the identity and no override")
+            if material is not None:
+                raise NotImplementedError("the reference driver adds meshes without a material override")
             vmat = np.full(src.vertex_count(), -1, np.int32)
             for v, m in enumerate(src.materials):
                 if m is None:
@@ -357,7 +358,13 @@ class RefScene:
             arrs = [np.ascontiguousarray(a, np.float32) for a in (src.positions, src.normals, src.uv0, src.uv1)]
             idx = np.ascontiguousarray(src.indices, np.int32)
             self._keep += arrs + [idx, vmat]
-            k = L.ref_add_mesh(self.h, src.vertex_count(), *[ptr(a) for a in arrs], ptr(vmat), idx.size, ptr(idx))
+            if transform is None:
+                k = L.ref_add_mesh(self.h, src.vertex_count(), *[ptr(a) for a in arrs], ptr(vmat), idx.size, ptr(idx))
+            else:
+                mat = np.ascontiguousarray(np.asarray(transform, np.float32).reshape(16))
+                self._keep.append(mat)
+                k = L.ref_add_mesh_transformed(self.h, src.vertex_count(), *[ptr(a) for a in arrs], ptr(vmat),
+                                               idx.size, ptr(idx), ptr(mat))
             self.mesh_index[id(inst)] = k
         f3 = lambda v: (C.c_float * 3)(*[float(x) for x in np.asarray(v).reshape(3)])
         for li, l in enumerate(scene.lights):

@@ -192,6 +192,18 @@ int ref_add_mesh(void* h, int nverts, const float* pos, const float* nrm, const 
     return (int)c->meshes.size() - 1;
 }
 
+/* Scene::addMesh(mesh, M, NULL) with a caller-supplied Matrix4 (16 floats,
+   Types.h:1177-1185 member order). */
+int ref_add_mesh_transformed(void* h, int nverts, const float* pos, const float* nrm, const float* uv0,
+                             const float* uv1, const int* vmat, int nidx, const int* idx, const float* m) {
+    RefCtx* c = (RefCtx*)h;
+    Mesh* src = build_mesh(c, nverts, pos, nrm, uv0, uv1, vmat, nidx, idx);
+    Matrix4 M(m[0], m[1], m[2], m[3], m[4], m[5], m[6], m[7], m[8], m[9], m[10], m[11], m[12], m[13], m[14], m[15]);
+    Mesh* inst = c->scene->addMesh(src, M, NULL);
+    c->meshes.push_back(inst);
+    return (int)c->meshes.size() - 1;
+}
+
 /* Read back a scene mesh's (transformed) vertex positions and normals. */
 void ref_mesh_vertices(void* h, int mesh, float* pos, float* nrm) {
     RefCtx* c = (RefCtx*)h;

@@ -36,14 +36,26 @@ def set(refill=None, block=None, kernel="indirect"):
         _abi.check(_abi.lib().rl_tune_set(pb, int(block)))
 
 
-def tune(run, kernel="indirect", refills=REFILLS, blocks=BLOCKS, reps=2, stream=None):
+def get_width():
+    v = C.c_int()
+    _abi.check(_abi.lib().rl_tune_get(_abi.TUNE_BVH_WIDTH, C.byref(v)))
+    return v.value
+
+
+def set_width(width):
+    _abi.check(_abi.lib().rl_tune_set(_abi.TUNE_BVH_WIDTH, int(width)))
+
+
+def tune(run, kernel="indirect", refills=REFILLS, blocks=BLOCKS, widths=(4,), reps=2, stream=None):
     """`run()` enqueues one call of `kernel` ("indirect" or "ao") on `stream`
     (a torch stream, None = the current one).  Returns (best, table), table
-    mapping (refill, block) -> milliseconds; the best setting is left applied."""
+    mapping (refill, block, width) -> milliseconds; the best setting is left
+    applied.  The BVH width is shared by both kernels."""
     import torch
     st = stream or torch.cuda.current_stream()
     table = {}
-    for refill, block in itertools.product(refills, blocks):
+    for width, refill, block in itertools.product(widths, refills, blocks):
+        set_width(width)
         set(refill, block, kernel)
         run()
         ms = []
@@ -54,7 +66,8 @@ def tune(run, kernel="indirect", refills=REFILLS, blocks=BLOCKS, reps=2, stream=
             e1.record(st)
             e1.synchronize()
             ms.append(e0.elapsed_time(e1))
-        table[(refill, block)] = min(ms)
+        table[(refill, block, width)] = min(ms)
     best = min(table, key=table.get)
     set(best[0], best[1], kernel)
-    return {"refill": best[0], "block": best[1], "ms": table[best]}, table
+    set_width(best[2])
+    return {"refill": best[0], "block": best[1], "width": best[2], "ms": table[best]}, table

@@ -157,6 +157,18 @@ struct Builder {
     }
 };
 
+// 4-wide node: f4[0..5] = lo.x, hi.x, lo.y, hi.y, lo.z, hi.z of the four
+// children; f4[6] = child codes; f4[7] unused.  Empty slots get a far point
+// box and the code kEmpty4.
+constexpr int kEmpty4 = (int)0x80000000;
+
+void put_child_box4(float* dst, int slot, const Box& b) {
+    for (int k = 0; k < 3; k++) {
+        dst[(2 * k) * 4 + slot] = b.lo[k];
+        dst[(2 * k + 1) * 4 + slot] = b.hi[k];
+    }
+}
+
 void put_child_box(float* dst, int slot, const Box& b) {
     // n0 / n1: lo.x hi.x lo.y hi.y for child 0 / 1; n2: c0 lo.z hi.z, c1 lo.z hi.z
     float* xy = dst + 4 * slot;
@@ -251,6 +263,15 @@ bool build_bvh_sah(const float* pos, int nverts, const int32_t* tris, int ntris,
         std::memcpy(&out.nodes[13], &c, 4);
         out.leaves = 1;
         out.sah = 1.0 + B.nodes[0].count;
+        out.nodes4.assign(32, 0.0f);
+        Box far;
+        for (int a = 0; a < 3; a++) { far.lo[a] = 1e30f; far.hi[a] = 1e30f; }
+        int codes4[4] = {c, kEmpty4, kEmpty4, kEmpty4};
+        for (int k = 0; k < 4; k++) {
+            put_child_box4(out.nodes4.data(), k, k == 0 ? B.nodes[0].box : far);
+            std::memcpy(&out.nodes4[24 + k], &codes4[k], 4);
+        }
+        out.nodes4_count = 1;
         return true;
     }
     out.nodes.assign(16 * order.size(), 0.0f);
@@ -271,6 +292,62 @@ bool build_bvh_sah(const float* pos, int nverts, const int32_t* tris, int ntris,
         }
     }
     out.sah = sah;
+
+    // Collapse into a 4-wide tree: each 4-wide node takes a binary inner node
+    // and repeatedly opens its largest-area inner child until it has four.
+    struct Collapse {
+        const std::vector<Node>& bn;
+        std::vector<float>& n4;
+        int (*leaf_code)(const Node&);
+        int emit(int id) {
+            int me = (int)(n4.size() / 32);
+            n4.resize(n4.size() + 32, 0.0f);
+            int kids[4] = {bn[id].child[0], bn[id].child[1], -1, -1};
+            int nk = 2;
+            while (nk < 4) {
+                int pick = -1;
+                float best = -1.0f;
+                for (int k = 0; k < nk; k++) {
+                    const Node& c = bn[kids[k]];
+                    if (c.count == 0 && c.box.area() > best) { best = c.box.area(); pick = k; }
+                }
+                if (pick < 0) break;
+                int opened = kids[pick];
+                kids[pick] = bn[opened].child[0];
+                kids[nk++] = bn[opened].child[1];
+            }
+            int codes[4];
+            for (int k = 0; k < 4; k++) {
+                if (k >= nk) { codes[k] = kEmpty4; continue; }
+                const Node& c = bn[kids[k]];
+                codes[k] = c.count > 0 ? leaf_code(c) : emit(kids[k]);
+            }
+            float* dst = &n4[32 * (size_t)me];
+            Box far;
+            for (int a = 0; a < 3; a++) { far.lo[a] = 1e30f; far.hi[a] = 1e30f; }
+            for (int k = 0; k < 4; k++) {
+                put_child_box4(dst, k, k < nk ? bn[kids[k]].box : far);
+                std::memcpy(&dst[24 + k], &codes[k], 4);
+            }
+            return me;
+        }
+    };
+    auto lc = [](const Node& n) -> int { return ~((n.first << 3) | (n.count - 1)); };
+    Collapse col{B.nodes, out.nodes4, +lc};
+    if (B.nodes[0].count > 0) {
+        // single leaf: one 4-wide node holding it
+        out.nodes4.assign(32, 0.0f);
+        Box far;
+        for (int a = 0; a < 3; a++) { far.lo[a] = 1e30f; far.hi[a] = 1e30f; }
+        int codes[4] = {lc(B.nodes[0]), kEmpty4, kEmpty4, kEmpty4};
+        for (int k = 0; k < 4; k++) {
+            put_child_box4(out.nodes4.data(), k, k == 0 ? B.nodes[0].box : far);
+            std::memcpy(&out.nodes4[24 + k], &codes[k], 4);
+        }
+    } else {
+        col.emit(0);
+    }
+    out.nodes4_count = (int64_t)(out.nodes4.size() / 32);
     return true;
 }
 

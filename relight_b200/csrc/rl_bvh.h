@@ -9,6 +9,8 @@ namespace rl {
 struct BvhBuild {
     std::vector<float> nodes;  // 16 floats per node (four float4, see rl_device.cuh)
     std::vector<float> tris;   // 12 floats per triangle in leaf order (three float4)
+    std::vector<float> nodes4; // 32 floats per 4-wide node (eight float4, see rl_device.cuh)
+    int64_t nodes4_count = 0;
     int64_t leaves = 0;
     int depth = 0;
     double sah = 0.0;

@@ -64,7 +64,7 @@ inline cudaStream_t S(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 // Launch tuning (rl_tune_set): per ray-stream kernel, the number of lanes a
 // warp waits for before refilling rays and the threads per block.  Defaults
 // are the autotuner's picks on the terrain final-gather / room AO workloads.
-int g_tune[4] = {24, 64, 32, 128};
+int g_tune[5] = {24, 64, 32, 128, 2};  // + BVH width of the ray-stream kernels
 
 inline unsigned blocks_for(long long n, int threads) { return (unsigned)((n + threads - 1) / threads); }
 
@@ -145,7 +145,9 @@ extern "C" const char* rl_version(void) { return "relight_b200 0.1 (sm_100a)"; }
 extern "C" int rl_tune_set(int param, int value) {
     bool refill = param == RL_TUNE_FG_REFILL || param == RL_TUNE_AO_REFILL;
     bool block = param == RL_TUNE_FG_BLOCK || param == RL_TUNE_AO_BLOCK;
-    if ((refill && value >= 1 && value <= 32) || (block && (value == 64 || value == 128 || value == 256)))
+    bool width = param == RL_TUNE_BVH_WIDTH;
+    if ((refill && value >= 1 && value <= 32) || (block && (value == 64 || value == 128 || value == 256)) ||
+        (width && (value == 2 || value == 4)))
         g_tune[param] = value;
     else
         return fail(RL_INVALID_CALL, "rl_tune_set: bad parameter %d or value %d", param, value);
@@ -153,7 +155,7 @@ extern "C" int rl_tune_set(int param, int value) {
 }
 
 extern "C" int rl_tune_get(int param, int* value) {
-    if (!value || param < 0 || param > 3) return fail(RL_INVALID_CALL, "rl_tune_get: bad parameter");
+    if (!value || param < 0 || param > 4) return fail(RL_INVALID_CALL, "rl_tune_get: bad parameter");
     *value = g_tune[param];
     return RL_OK;
 }
@@ -220,7 +222,9 @@ extern "C" int rl_scene_create(const rl_scene_desc* d, int builder, void* stream
     int *dvmat = nullptr, *first = nullptr, *dpmap = nullptr, *dmat_tex = nullptr, *tex_dims = nullptr;
     long long* tex_off = nullptr;
     unsigned char* tex_px = nullptr;
+    float4* nodes4 = nullptr;
     up(&nodes, (const float4*)b.nodes.data(), b.nodes.size() / 4);
+    up(&nodes4, (const float4*)b.nodes4.data(), b.nodes4.size() / 4);
     up(&tris, (const float4*)b.tris.data(), b.tris.size() / 4);
     up(&dvidx, vidx.data(), vidx.size());
     up(&pos, d->pos, 3 * (size_t)d->nverts);
@@ -255,7 +259,7 @@ extern "C" int rl_scene_create(const rl_scene_desc* d, int builder, void* stream
         return rc;
     }
     DevScene& v = s->dev;
-    v.nodes = nodes; v.tris = tris; v.tri_vidx = dvidx;
+    v.nodes = nodes; v.nodes4 = nodes4; v.tris = tris; v.tri_vidx = dvidx;
     v.pos = pos; v.nrm = nrm; v.uv0 = uv0; v.uv1 = uv1; v.vmat = dvmat;
     v.mesh_first_tri = first; v.mesh_photonmap = dpmap;
     v.mat_rgb = mat_rgb; v.mat_tex = dmat_tex; v.tex_dims = tex_dims; v.tex_offset = tex_off; v.tex_pixels = tex_px;
@@ -697,6 +701,7 @@ struct AoGen {
     }
 };
 
+template <int kWidth>
 __global__ void __launch_bounds__(256) k_ao(DevScene s, DevMap m, int samples, float fraction, float maxd,
                                             float exponent, uint2 key, int first, int step, long long count,
                                             int refill, int* status) {
@@ -712,7 +717,8 @@ __global__ void __launch_bounds__(256) k_ao(DevScene s, DevMap m, int samples, f
     g.samples = (m.flags[i] & 1) ? samples : 0;
     g.occluded = 0;
     g.maxd = maxd;
-    ray_loop<true>(s, g, refill, status);
+    if (kWidth == 4) ray_loop4<true>(s, g, refill, status);
+    else ray_loop<true>(s, g, refill, status);
     if (!(m.flags[i] & 1)) return;
     float value = 1.0f - g.occluded / (samples * fraction);
     if (fabsf(1.0f - exponent) > 0.01f) value = powf(value, exponent);
@@ -729,7 +735,8 @@ extern "C" int rl_bake_ao(const rl_scene* s, rl_map* lm, int samples, float frac
     if (count == 0) return RL_OK;
     uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
     int bs = g_tune[RL_TUNE_AO_BLOCK];
-    k_ao<<<blocks_for(count, bs), bs, 0, S(stream)>>>(s->dev, lm->dev, samples, fraction, maxd, exponent, key,
+    auto kern = g_tune[RL_TUNE_BVH_WIDTH] == 4 ? k_ao<4> : k_ao<2>;
+    kern<<<blocks_for(count, bs), bs, 0, S(stream)>>>(s->dev, lm->dev, samples, fraction, maxd, exponent, key,
                                                       first, step, count, g_tune[RL_TUNE_AO_REFILL], s->d_status);
     CK_LAUNCH("k_ao");
     return RL_OK;
@@ -948,6 +955,7 @@ struct FgGen {
     }
 };
 
+template <int kWidth>
 __global__ void __launch_bounds__(256) k_indirect(DevScene s, DevMap m, const __grid_constant__ GatherMaps G,
                                                   int samples, float maxd, V3 sky, V3 amb, uint2 key, int first,
                                                   int step, long long count, int refill, int* status) {
@@ -970,7 +978,8 @@ __global__ void __launch_bounds__(256) k_indirect(DevScene s, DevMap m, const __
     g.gr = g.gg = g.gb = 0.f;
     g.influence = 0.f;
     g.dir = mk3(0.f, 0.f, 0.f);
-    ray_loop<false>(s, g, refill, status);
+    if (kWidth == 4) ray_loop4<false>(s, g, refill, status);
+    else ray_loop<false>(s, g, refill, status);
     if (!valid) return;
     float ns = (float)samples;
     float* col = m.color + 3 * i;
@@ -998,8 +1007,9 @@ extern "C" int rl_bake_indirect(const rl_scene* s, rl_map* lm, rl_map* const* ma
     V3 ambv = {ambient ? ambient[0] : 0.f, ambient ? ambient[1] : 0.f, ambient ? ambient[2] : 0.f};
     uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
     int bs = g_tune[RL_TUNE_FG_BLOCK];
-    k_indirect<<<blocks_for(count, bs), bs, 0, st>>>(s->dev, lm->dev, G, samples, maxd, skyv, ambv, key, first,
-                                                    step, count, g_tune[RL_TUNE_FG_REFILL], s->d_status);
+    auto kern = g_tune[RL_TUNE_BVH_WIDTH] == 4 ? k_indirect<4> : k_indirect<2>;
+    kern<<<blocks_for(count, bs), bs, 0, st>>>(s->dev, lm->dev, G, samples, maxd, skyv, ambv, key, first, step,
+                                              count, g_tune[RL_TUNE_FG_REFILL], s->d_status);
     CK_LAUNCH("k_indirect");
     return RL_OK;
 }

@@ -26,6 +26,7 @@ namespace rl {
 // Triangles, 48 bytes in leaf order: t0 = v0.xyz | gid bits, t1 = e1.xyz, t2 = e2.xyz.
 struct DevScene {
     const float4* nodes;
+    const float4* nodes4;       // 4-wide nodes, 128 B: lo.x hi.x lo.y hi.y lo.z hi.z (4 children each), codes, pad
     const float4* tris;
     const int4* tri_vidx;       // per global triangle id: a, b, c, mesh
     const float* pos;
@@ -365,6 +366,123 @@ __device__ __forceinline__ void ray_loop(const DevScene& s, Gen& g, int refill, 
             } else {
                 node = sp > 0 ? stack[--sp] : kNodeDone;
             }
+        }
+        if (node == kNodeDone) continue;
+        // one leaf
+        int code = ~node;
+        int first = code >> 3, count = (code & 7) + 1;
+        bool stop = false;
+        for (int i = first; i < first + count; i++) {
+            const float4* tp = s.tris + 3 * (size_t)i;
+            float4 t0 = __ldg(tp), t1 = __ldg(tp + 1), t2 = __ldg(tp + 2);
+            float t, u, v;
+            if (tri_test(t0, t1, t2, o, d, tnear, tfar, t, u, v)) {
+                int gid = __float_as_int(t0.w);
+                if (t < best || (t == best && gid < best_gid)) {
+                    best = t; best_gid = gid;
+                    hit.t = t; hit.u = u; hit.v = v; hit.gid = gid;
+                    if (kAny) { stop = true; break; }
+                }
+            }
+        }
+        node = (!stop && sp > 0) ? stack[--sp] : kNodeDone;
+    }
+}
+
+// Entry distance of one child of a 4-wide node, or kMissKey when the ray
+// misses its box (or the slot is empty).  Same conservative slab test as slab2.
+constexpr float kMissKey = 3.0e38f;
+
+__device__ __forceinline__ float child_entry(float lx, float hx, float ly, float hy, float lz, float hz, V3 idir,
+                                             V3 ood, float tnear, float tmax, int code) {
+    float a0 = __fmaf_rn(lx, idir.x, -ood.x), a1 = __fmaf_rn(hx, idir.x, -ood.x);
+    float b0 = __fmaf_rn(ly, idir.y, -ood.y), b1 = __fmaf_rn(hy, idir.y, -ood.y);
+    float c0 = __fmaf_rn(lz, idir.z, -ood.z), c1 = __fmaf_rn(hz, idir.z, -ood.z);
+    float lo = fmaxf(fmaxf(fminf(a0, a1), fminf(b0, b1)), fmaxf(fminf(c0, c1), tnear));
+    float hi = fminf(fminf(fmaxf(a0, a1), fmaxf(b0, b1)), fminf(fmaxf(c0, c1), tmax));
+    return (lo <= hi * 1.0000003f && code != kNodeDone) ? lo : kMissKey;
+}
+
+__device__ __forceinline__ void cswap(float& ka, int& ca, float& kb, int& cb) {
+    bool sw = kb < ka;
+    float tk = sw ? kb : ka;
+    int tc = sw ? cb : ca;
+    kb = sw ? ka : kb;
+    cb = sw ? ca : cb;
+    ka = tk;
+    ca = tc;
+}
+
+template <bool kAny, typename Gen>
+__device__ __forceinline__ void ray_loop4(const DevScene& s, Gen& g, int refill, int* overflow) {
+    V3 o = mk3(0.f, 0.f, 0.f), d = o, idir = o, ood = o;
+    float tnear = 0.f, tfar = 0.f, best = 0.f;
+    int best_gid = 0x7fffffff;
+    RayHit hit;
+    hit.gid = -1; hit.t = hit.u = hit.v = 0.f;
+    int stack[kStackSize];
+    int sp = 0;
+    int node = kNodeDone;
+    bool have = false, exhausted = false;
+    const unsigned mask = __activemask();
+    for (;;) {
+        // Lanes whose ray ended wait until `refill` of the warp's live lanes
+        // (or all of them) have ended, then start their next rays together,
+        // so ray generation and hit shading run on many lanes at once.
+        bool need = node == kNodeDone && !exhausted;
+        unsigned alive = __ballot_sync(mask, !exhausted);
+        if (alive == 0) break;
+        unsigned needm = __ballot_sync(mask, need);
+        if (need && (__popc(needm) >= refill || needm == alive)) {
+            if (have) {
+                g.finish(hit);
+                have = false;
+            }
+            if (g.next(o, d, tnear, tfar)) {
+                have = true;
+                idir = mk3(safe_inv(d.x), safe_inv(d.y), safe_inv(d.z));
+                ood = mk3(o.x * idir.x, o.y * idir.y, o.z * idir.z);
+                best = tfar;
+                best_gid = 0x7fffffff;
+                hit.gid = -1;
+                sp = 0;
+                node = s.ntris > 0 ? 0 : kNodeDone;
+            } else {
+                exhausted = true;
+            }
+        }
+        if (node == kNodeDone) continue;
+        // 4-wide inner nodes until a leaf (or the end of the walk)
+        while (node >= 0) {
+            const float4* np = s.nodes4 + 8 * (size_t)node;
+            float4 lx = __ldg(np), hx = __ldg(np + 1), ly = __ldg(np + 2), hy = __ldg(np + 3);
+            float4 lz = __ldg(np + 4), hz = __ldg(np + 5);
+            int4 cc = __ldg(reinterpret_cast<const int4*>(np + 6));
+            float k0 = child_entry(lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, idir, ood, tnear, best, cc.x);
+            float k1 = child_entry(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, idir, ood, tnear, best, cc.y);
+            float k2 = child_entry(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, idir, ood, tnear, best, cc.z);
+            float k3 = child_entry(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, idir, ood, tnear, best, cc.w);
+            int c0 = cc.x, c1 = cc.y, c2 = cc.z, c3 = cc.w;
+            // sort (entry, child) ascending: 5 compare-exchanges
+            cswap(k0, c0, k1, c1);
+            cswap(k2, c2, k3, c3);
+            cswap(k0, c0, k2, c2);
+            cswap(k1, c1, k3, c3);
+            cswap(k1, c1, k2, c2);
+            int nh = (k0 < kMissKey) + (k1 < kMissKey) + (k2 < kMissKey) + (k3 < kMissKey);
+            if (nh == 0) {
+                node = sp > 0 ? stack[--sp] : kNodeDone;
+                continue;
+            }
+            if (sp + nh - 1 > kStackSize) {
+                if (overflow) *overflow = 1;
+                nh = 1 + (kStackSize - sp > 0 ? kStackSize - sp : 0);
+                if (nh > 4) nh = 4;
+            }
+            if (nh > 3) stack[sp++] = c3;
+            if (nh > 2) stack[sp++] = c2;
+            if (nh > 1) stack[sp++] = c1;
+            node = c0;
         }
         if (node == kNodeDone) continue;
         // one leaf

@@ -267,17 +267,27 @@ def test_launch_tuning_changes_no_result(cuda):
     """The autotuner's knobs (refill threshold, block size) reschedule rays
     only: every setting bakes the same bits."""
     from relight_b200 import autotune
-    w = scenes.room_scene(size=64)
-    saved = autotune.get("ao"), autotune.get("indirect")
-    colors = []
+    saved = autotune.get("ao"), autotune.get("indirect"), autotune.get_width()
+    colors, fg = [], []
     try:
-        for refill, block in ((1, 64), (13, 128), (32, 256)):
+        for refill, block, width in ((1, 64, 2), (13, 128, 4), (32, 256, 2), (24, 64, 4)):
+            autotune.set_width(width)
             autotune.set(refill, block, "ao")
+            autotune.set(refill, block, "indirect")
             rl = _relight()
             ws = scenes.room_scene(size=64)
             rl.bake_ambient_occlusion(ws.scene, ws.mesh, None, ws.ao, seed=3)
             colors.append(_lumels(ws.lightmap)["color"])
+            wt = _small_terrain()
+            rl.emit_photons(wt.scene, wt.settings, seed=2)
+            rl.bake_indirect_light(wt.scene, wt.meshes[0], None, wt.settings, seed=4)
+            fg.append(_lumels(wt.lightmap)["color"])
     finally:
         autotune.set(saved[0]["refill"], saved[0]["block"], "ao")
         autotune.set(saved[1]["refill"], saved[1]["block"], "indirect")
+        autotune.set_width(saved[2])
     assert all(np.array_equal(colors[0], c) for c in colors[1:])
+    # photon deposits are atomic float sums, so the final gather is compared
+    # through the photonmap's tolerance
+    for c in fg[1:]:
+        np.testing.assert_allclose(c, fg[0], rtol=1e-4, atol=1e-6)

@@ -183,6 +183,19 @@ int rl_emit_photons(const rl_scene* scene, rl_map* const* photonmaps, int nmaps,
                     int nlights, int pass_count, int max_depth, float energy_threshold, float max_distance,
                     uint64_t seed, int64_t* stored, void* stream);
 
+/* The same photons, restricted to the global photon indices
+   [first_photon, first_photon + photon_count) of the reference's
+   pass / light / photon loop order: a GPU's share when one bake's photons
+   are split across GPUs.  The shares' photonmap accumulators (colour, count)
+   summed over GPUs equal the unsplit emission's. */
+int rl_emit_photons_range(const rl_scene* scene, rl_map* const* photonmaps, int nmaps, const rl_light* lights,
+                          int nlights, int pass_count, int max_depth, float energy_threshold, float max_distance,
+                          uint64_t seed, int64_t first_photon, int64_t photon_count, int64_t* stored, void* stream);
+/* Number of photons one emission traces: pass_count x sum over emitting
+   lights of int(intensity * 25000) (PhotonEmitter::photonCount,
+   scene/Light.cpp:334-337). */
+int rl_photon_count(const rl_light* lights, int nlights, int pass_count, int64_t* total);
+
 /* Photonmap::gather(radius) (Lightmap.cpp:376-413), the loop-bound quirk
    of :379 included. */
 int rl_photonmap_gather(rl_map* photonmap, int radius, void* stream);
@@ -225,6 +238,14 @@ int rl_ff_hemisphere(const rl_scene* scene, int n, const float* d_pos, const flo
    vectors are device arrays; d_B [n][3] receives the result. */
 int rl_radiosity_solve(int n, const int64_t* d_row_ptr, const int32_t* d_cols, const float* d_vals,
                        const float* d_E, const float* d_rho, int iters, float* d_B, void* stream);
+
+/* One Jacobi step restricted to rows [row_begin, row_end):
+   d_B_next[row] = E[row] + rho[row] * sum_k F[row][k] d_B[k].  The unit of a
+   row-sharded solve across GPUs (each GPU steps its rows, then the rows are
+   all-gathered into d_B). */
+int rl_radiosity_step(int row_begin, int row_end, const int64_t* d_row_ptr, const int32_t* d_cols,
+                      const float* d_vals, const float* d_E, const float* d_rho, const float* d_B, float* d_B_next,
+                      void* stream);
 
 /* The same solve for callers that cannot allocate device memory: a plugin
    inside a host application (a game engine or an editor) that owns every

@@ -18,7 +18,7 @@ from relight_b200.api import FlatScene, Scene
 ORACLE_DIR = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(ORACLE_DIR)
 ORACLE_LIB = os.path.join(ORACLE_DIR, "liboracle.so")
-REF_LIB = os.path.join(ORACLE_DIR, "_ref", "librelight_ref.so")
+REF_LIB = os.environ.get("RELIGHT_REF_LIB") or os.path.join(ORACLE_DIR, "_ref", "librelight_ref.so")
 REF_FAST_LIB = os.path.join(ORACLE_DIR, "_ref", "librelight_ref_fast.so")
 
 _P = C.c_void_p
@@ -85,6 +85,8 @@ def _load_oracle():
         "oro_bake_ao": (None, [_P, _P, C.c_int, C.c_float, C.c_float, C.c_float, C.c_uint64, C.c_int, C.c_int]),
         "oro_emit_photons": (C.c_longlong, [_P, _P, C.c_int, _P, C.c_int, C.c_int, C.c_float, C.c_float,
                                             C.c_uint64]),
+        "oro_emit_photons_range": (C.c_longlong, [_P, _P, C.c_int, _P, C.c_int, C.c_int, C.c_float, C.c_float,
+                                                  C.c_uint64, C.c_longlong, C.c_longlong]),
         "oro_photonmap_gather": (None, [_P, C.c_int]),
         "oro_bake_indirect": (None, [_P, _P, _P, C.c_int, C.c_float, _P, _P, C.c_uint64, C.c_int, C.c_int]),
         "oro_ff_pairwise": (C.c_longlong, [_P, C.c_int, _P, _P, C.c_float, _P, _P, _P]),
@@ -115,7 +117,9 @@ def oracle_lib():
 
 
 def ptr(a):
-    return None if a is None else C.c_void_p(a.ctypes.data)
+    """A c_void_p to `a`'s data that keeps `a` alive as long as the pointer
+    (numpy's data_as holds a reference), so temporaries survive the call."""
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
 
 
 def philox(ctr, key):
@@ -189,6 +193,12 @@ class Oracle:
         f = self.flat
         return self.lib.oro_emit_photons(self.ctx, ptr(f.lights), len(f.lights), arr, passes, depth, threshold, maxd,
                                          seed)
+
+    def emit_photons_range(self, pms, passes, depth, threshold, maxd, seed, first, count):
+        arr = (Lumels * max(len(pms), 1))(*[p.struct() for p in pms])
+        f = self.flat
+        return self.lib.oro_emit_photons_range(self.ctx, ptr(f.lights), len(f.lights), arr, passes, depth, threshold,
+                                               maxd, seed, first, count)
 
     def gather(self, pm: LumelMap, radius):
         s = pm.struct()

@@ -57,9 +57,11 @@ int ort_triangle_count(const ort_scene* s) { return s->ntri; }
 
 int ort_add_mesh(ort_scene* s, const float* verts, int vstride, int nverts, const int* tris, int ntris) {
     int base = s->npos;
+    if (nverts < 0 || ntris < 0) return -1;
     if (s->npos + nverts > s->cap_pos) {
-        s->cap_pos = (s->npos + nverts) * 2 + 16;
-        s->pos = (float*)realloc(s->pos, sizeof(float) * 3 * (size_t)s->cap_pos);
+        size_t cap = ((size_t)s->npos + (size_t)nverts) * 2 + 16;
+        s->pos = (float*)realloc(s->pos, sizeof(float) * 3 * cap);
+        s->cap_pos = (int)cap;
     }
     for (int i = 0; i < nverts; i++) {
         s->pos[3 * (base + i) + 0] = verts[(size_t)i * vstride + 0];
@@ -68,10 +70,11 @@ int ort_add_mesh(ort_scene* s, const float* verts, int vstride, int nverts, cons
     }
     s->npos += nverts;
     if (s->ntri + ntris > s->cap_tri) {
-        s->cap_tri = (s->ntri + ntris) * 2 + 16;
-        s->idx = (int*)realloc(s->idx, sizeof(int) * 3 * (size_t)s->cap_tri);
-        s->tgeom = (int*)realloc(s->tgeom, sizeof(int) * (size_t)s->cap_tri);
-        s->tprim = (int*)realloc(s->tprim, sizeof(int) * (size_t)s->cap_tri);
+        size_t cap = ((size_t)s->ntri + (size_t)ntris) * 2 + 16;
+        s->idx = (int*)realloc(s->idx, sizeof(int) * 3 * cap);
+        s->tgeom = (int*)realloc(s->tgeom, sizeof(int) * cap);
+        s->tprim = (int*)realloc(s->tprim, sizeof(int) * cap);
+        s->cap_tri = (int)cap;
     }
     for (int t = 0; t < ntris; t++) {
         for (int k = 0; k < 3; k++) s->idx[3 * (s->ntri + t) + k] = base + tris[3 * t + k];
@@ -199,12 +202,12 @@ static void build_rec(builder* b, int ni, int first, int count) {
 }
 
 void ort_commit(ort_scene* s) {
-    int n = s->ntri;
+    int n = s->ntri > 0 ? s->ntri : 0;
     builder b;
     memset(&b, 0, sizeof(b));
-    b.tbox = (box3*)malloc(sizeof(box3) * (size_t)(n ? n : 1));
-    b.cent = (float*)malloc(sizeof(float) * 3 * (size_t)(n ? n : 1));
-    b.order = (int*)malloc(sizeof(int) * (size_t)(n ? n : 1));
+    b.tbox = (box3*)malloc(sizeof(box3) * (size_t)(n > 0 ? n : 1));
+    b.cent = (float*)malloc(sizeof(float) * 3 * (size_t)(n > 0 ? n : 1));
+    b.order = (int*)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
     for (int t = 0; t < n; t++) {
         box3* bx = &b.tbox[t];
         box_empty(bx);
@@ -224,8 +227,8 @@ void ort_commit(ort_scene* s) {
     if (n > 0) build_rec(&b, root, 0, n);
     else { box3 e; box_empty(&e); memcpy(b.nodes[0].lo, e.lo, sizeof e.lo); memcpy(b.nodes[0].hi, e.hi, sizeof e.hi); b.nodes[0].left = 0; b.nodes[0].count = 0; }
     s->nodes = b.nodes; s->nnodes = b.nnodes;
-    s->tris = (ort_tri*)malloc(sizeof(ort_tri) * (size_t)(n ? n : 1));
-    s->tri64 = (double*)malloc(sizeof(double) * 9 * (size_t)(n ? n : 1));
+    s->tris = (ort_tri*)malloc(sizeof(ort_tri) * (size_t)(n > 0 ? n : 1));
+    s->tri64 = (double*)malloc(sizeof(double) * 9 * (size_t)(n > 0 ? n : 1));
     for (int i = 0; i < n; i++) {
         int t = b.order[i];
         const float* p0 = &s->pos[3 * s->idx[3 * t + 0]];

@@ -454,6 +454,13 @@ static inline float luminance(v3 c) { return 0.2126f * c.x + 0.7152f * c.y + 0.0
 long long oro_emit_photons(const oro_ctx* c, const rl_light* lights, int nlights, rl_lumels* photonmaps,
                            int pass_count, int max_depth, float energy_threshold, float max_distance,
                            uint64_t seed) {
+    return oro_emit_photons_range(c, lights, nlights, photonmaps, pass_count, max_depth, energy_threshold,
+                                  max_distance, seed, 0, -1);
+}
+
+long long oro_emit_photons_range(const oro_ctx* c, const rl_light* lights, int nlights, rl_lumels* photonmaps,
+                                 int pass_count, int max_depth, float energy_threshold, float max_distance,
+                                 uint64_t seed, long long first_photon, long long photon_count) {
     const rl_scene_desc* d = c->d;
     long long stored = 0;
     uint32_t photon = 0;
@@ -468,6 +475,9 @@ long long oro_emit_photons(const oro_ctx* c, const rl_light* lights, int nlights
             int count = (int)(L->intensity * 25000);
             /* Photons::emitPhotons (baker/Photons.cpp:68-92) */
             for (int k = 0; k < count; k++, photon++) {
+                if ((long long)photon < first_photon ||
+                    (photon_count >= 0 && (long long)photon >= first_photon + photon_count))
+                    continue;
                 v3 pos, dir;
                 if (L->emitter == 1) {
                     /* PhotonEmitter::emit (scene/Light.cpp:340-344) */

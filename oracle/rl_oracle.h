@@ -116,6 +116,12 @@ long long oro_emit_photons(const oro_ctx* c, const rl_light* lights, int nlights
                            int pass_count, int max_depth, float energy_threshold, float max_distance,
                            uint64_t seed);
 
+/* The photons with global index in [first_photon, first_photon + count)
+   (count < 0: to the end), in the pass / light / photon loop order above. */
+long long oro_emit_photons_range(const oro_ctx* c, const rl_light* lights, int nlights, rl_lumels* photonmaps,
+                                 int pass_count, int max_depth, float energy_threshold, float max_distance,
+                                 uint64_t seed, long long first_photon, long long photon_count);
+
 /* Photonmap::gather(radius) (Lightmap.cpp:376-413). */
 void oro_photonmap_gather(rl_lumels* pm, int radius);
 
@@ -130,8 +136,8 @@ void oro_bake_indirect(const oro_ctx* c, rl_lumels* lm, const rl_lumels* photonm
 long long oro_ff_pairwise(const oro_ctx* c, int n, const float* pos, const float* nrm, float threshold,
                           int64_t* row_ptr, int32_t* cols, float* vals);
 
-/* Hemisphere-cast form factors (no reference counterpart: BASELINE's
-   cosine-weighted variant): `rays` cosine-weighted rays per patch, F_ij = hits/rays. */
+/* Hemisphere-cast form factors (no reference counterpart: the
+   cosine-weighted hemisphere variant): `rays` cosine-weighted rays per patch, F_ij = hits/rays. */
 long long oro_ff_hemisphere(const oro_ctx* c, int n, const float* pos, const float* nrm, int rays,
                             float max_distance, uint64_t seed, const int32_t* mesh_map, const int32_t* map_dims,
                             const int64_t* map_base, const int32_t* patch_of_texel, int64_t* row_ptr,

@@ -35,7 +35,9 @@ class SceneDesc(C.Structure):
 
 
 def _ptr(a):
-    return None if a is None else C.c_void_p(a.ctypes.data)
+    """A c_void_p to `a`'s data that holds a reference to `a` (numpy's
+    data_as), so the array outlives the pointer."""
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
 
 
 def make_scene_desc(flat):
@@ -95,12 +97,15 @@ SIGNATURES = {
     "rl_bake_direct": (_I, [_P, _P, _P, _I, _P, _I, _I, _I, _P]),
     "rl_bake_ao": (_I, [_P, _P, _I, _F, _F, _F, _U64, _I, _I, _P]),
     "rl_emit_photons": (_I, [_P, _P, _I, _P, _I, _I, _I, _F, _F, _U64, _P, _P]),
+    "rl_emit_photons_range": (_I, [_P, _P, _I, _P, _I, _I, _I, _F, _F, _U64, _I64, _I64, _P, _P]),
+    "rl_photon_count": (_I, [_P, _I, _I, _P]),
     "rl_photonmap_gather": (_I, [_P, _I, _P]),
     "rl_bake_indirect": (_I, [_P, _P, _P, _I, _I, _F, _P, _P, _U64, _I, _I, _P]),
     "rl_ff_pairwise": (_I, [_P, _I, _P, _P, _F, _P, _P, _P, _I64, _P, _P]),
     "rl_ff_hemisphere": (_I, [_P, _I, _P, _P, _I, _F, _U64, _P, _I, _P, _P, _P, _I64, _P, _P, _P, _I64, _P, _P]),
     "rl_radiosity_solve": (_I, [_I, _P, _P, _P, _P, _P, _I, _P, _P]),
     "rl_radiosity_solve_noalloc": (_I, [_I, _P, _P, _P, _P, _P, _I, _P, _P]),
+    "rl_radiosity_step": (_I, [_I, _I, _P, _P, _P, _P, _P, _P, _P, _P]),
     "rl_measure_read_bandwidth": (_I, [C.c_size_t, _I, _P]),
     "rl_tune_set": (_I, [_I, _I]),
     "rl_tune_get": (_I, [_I, _P]),

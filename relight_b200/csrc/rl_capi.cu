@@ -757,10 +757,11 @@ struct PhotonTables {
 // one thread per photon; photon p is the p-th iteration of the reference's
 // pass / light / photon loops.
 __global__ void k_photons(DevScene s, const __grid_constant__ LightTable LT, const __grid_constant__ PhotonTables T,
-                          unsigned total, int max_depth, float threshold, float maxd, uint2 key,
+                          unsigned first, unsigned total, int max_depth, float threshold, float maxd, uint2 key,
                           unsigned long long* stored, int* status) {
-    unsigned p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= total) return;
+    unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= total) return;
+    unsigned p = first + t;
     unsigned r = p % T.per_pass;
     int e = 0;
     while (e + 1 < T.nl && T.prefix[e + 1] <= r) e++;
@@ -811,9 +812,9 @@ __global__ void k_photons(DevScene s, const __grid_constant__ LightTable LT, con
     }
 }
 
-extern "C" int rl_emit_photons(const rl_scene* s, rl_map* const* maps, int nmaps, const rl_light* lights,
-                               int nlights, int pass_count, int max_depth, float threshold, float maxd, uint64_t seed,
-                               int64_t* stored, void* stream) {
+static int emit_photons(const rl_scene* s, rl_map* const* maps, int nmaps, const rl_light* lights, int nlights,
+                        int pass_count, int max_depth, float threshold, float maxd, uint64_t seed, int64_t first_photon,
+                        int64_t photon_count, int64_t* stored, void* stream) {
     if (!s || (nmaps > 0 && !maps)) return fail(RL_INVALID_CALL, "rl_emit_photons: null argument");
     if (nmaps > kMaxPhotonmaps) return fail(RL_INVALID_CALL, "rl_emit_photons: at most %d photonmaps", kMaxPhotonmaps);
     cudaStream_t st = S(stream);
@@ -839,9 +840,13 @@ extern "C" int rl_emit_photons(const rl_scene* s, rl_map* const* maps, int nmaps
         if (!maps[k]) return fail(RL_INVALID_CALL, "photonmap %d is null", k);
         T.maps[k] = maps[k]->dev;
     }
-    unsigned long long total = per_pass * (unsigned long long)std::max(pass_count, 0);
-    if (total >= (1ull << 32)) return fail(RL_INVALID_CALL, "too many photons (%llu)", total);
+    unsigned long long all = per_pass * (unsigned long long)std::max(pass_count, 0);
+    if (all >= (1ull << 32)) return fail(RL_INVALID_CALL, "too many photons (%llu)", all);
     if (stored) *stored = 0;
+    unsigned long long first = first_photon < 0 ? 0 : (unsigned long long)first_photon;
+    unsigned long long total = photon_count < 0 ? all : (unsigned long long)photon_count;
+    if (first > all) first = all;
+    if (first + total > all) total = all - first;
     if (total == 0) return RL_OK;
     Scratch sc;
     unsigned long long* dc = nullptr;
@@ -851,8 +856,8 @@ extern "C" int rl_emit_photons(const rl_scene* s, rl_map* const* maps, int nmaps
         CK(cudaMemsetAsync(dc, 0, 8, st));
     }
     uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
-    k_photons<<<blocks_for((long long)total, 128), 128, 0, st>>>(s->dev, LT, T, (unsigned)total, max_depth, threshold,
-                                                                maxd, key, dc, s->d_status);
+    k_photons<<<blocks_for((long long)total, 128), 128, 0, st>>>(s->dev, LT, T, (unsigned)first, (unsigned)total,
+                                                                max_depth, threshold, maxd, key, dc, s->d_status);
     CK_LAUNCH("k_photons");
     if (stored) {
         unsigned long long h = 0;
@@ -860,6 +865,31 @@ extern "C" int rl_emit_photons(const rl_scene* s, rl_map* const* maps, int nmaps
         CK(cudaStreamSynchronize(st));
         *stored = (int64_t)h;
     }
+    return RL_OK;
+}
+
+extern "C" int rl_emit_photons(const rl_scene* s, rl_map* const* maps, int nmaps, const rl_light* lights,
+                               int nlights, int pass_count, int max_depth, float threshold, float maxd, uint64_t seed,
+                               int64_t* stored, void* stream) {
+    return emit_photons(s, maps, nmaps, lights, nlights, pass_count, max_depth, threshold, maxd, seed, 0, -1, stored,
+                        stream);
+}
+
+extern "C" int rl_emit_photons_range(const rl_scene* s, rl_map* const* maps, int nmaps, const rl_light* lights,
+                                     int nlights, int pass_count, int max_depth, float threshold, float maxd,
+                                     uint64_t seed, int64_t first_photon, int64_t photon_count, int64_t* stored,
+                                     void* stream) {
+    if (first_photon < 0 || photon_count < 0) return fail(RL_INVALID_CALL, "rl_emit_photons_range: negative range");
+    return emit_photons(s, maps, nmaps, lights, nlights, pass_count, max_depth, threshold, maxd, seed, first_photon,
+                        photon_count, stored, stream);
+}
+
+extern "C" int rl_photon_count(const rl_light* lights, int nlights, int pass_count, int64_t* total) {
+    if (!total || (nlights > 0 && !lights)) return fail(RL_INVALID_CALL, "rl_photon_count: null argument");
+    long long per_pass = 0;
+    for (int l = 0; l < nlights; l++)
+        if (lights[l].emitter) per_pass += std::max((int)(lights[l].intensity * 25000), 0);
+    *total = per_pass * (long long)std::max(pass_count, 0);
     return RL_OK;
 }
 
@@ -1319,6 +1349,48 @@ __global__ void k_jacobi(int n, const int64_t* row_ptr, const int32_t* cols, con
         Bn[i + 1] = __fmaf_rn(rho[i + 1], s1, E[i + 1]);
         Bn[i + 2] = __fmaf_rn(rho[i + 2], s2, E[i + 2]);
     }
+}
+
+// One Jacobi step over rows [row_begin, row_end): Bn[row] from the full B.
+__global__ void k_jacobi_rows(int row_begin, int row_end, const int64_t* row_ptr, const int32_t* cols,
+                              const float* vals, const float* E, const float* rho, const float* B, float* Bn) {
+    int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    int row = row_begin + warp;
+    if (row >= row_end) return;
+    int64_t b = row_ptr[row], e = row_ptr[row + 1];
+    float s0 = 0.f, s1 = 0.f, s2 = 0.f;
+    for (int64_t k = b + lane; k < e; k += 32) {
+        float w = vals[k];
+        const float* x = B + 3 * (size_t)cols[k];
+        s0 = __fmaf_rn(w, x[0], s0);
+        s1 = __fmaf_rn(w, x[1], s1);
+        s2 = __fmaf_rn(w, x[2], s2);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+        s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+        s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+    }
+    if (lane == 0) {
+        size_t i = 3 * (size_t)row;
+        Bn[i] = __fmaf_rn(rho[i], s0, E[i]);
+        Bn[i + 1] = __fmaf_rn(rho[i + 1], s1, E[i + 1]);
+        Bn[i + 2] = __fmaf_rn(rho[i + 2], s2, E[i + 2]);
+    }
+}
+
+extern "C" int rl_radiosity_step(int row_begin, int row_end, const int64_t* d_row_ptr, const int32_t* d_cols,
+                                 const float* d_vals, const float* d_E, const float* d_rho, const float* d_B,
+                                 float* d_B_next, void* stream) {
+    if (row_begin < 0 || row_end < row_begin || !d_row_ptr || !d_E || !d_rho || !d_B || !d_B_next)
+        return fail(RL_INVALID_CALL, "rl_radiosity_step: bad arguments");
+    if (row_end == row_begin) return RL_OK;
+    k_jacobi_rows<<<blocks_for((long long)(row_end - row_begin) * 32, 256), 256, 0, S(stream)>>>(
+        row_begin, row_end, d_row_ptr, d_cols, d_vals, d_E, d_rho, d_B, d_B_next);
+    CK_LAUNCH("k_jacobi_rows");
+    return RL_OK;
 }
 
 extern "C" int rl_radiosity_solve(int n, const int64_t* d_row_ptr, const int32_t* d_cols, const float* d_vals,

@@ -204,9 +204,17 @@ def terrain_scene(seed: int = 2, verts: int = 256, n_boxes: int = 2000, size: in
             inst = scene.add_mesh(src)
             lm.add_mesh(inst); pm.add_mesh(inst)
             meshes.append(inst)
-    # boxes standing on the terrain, 4x4-texel cells below the terrain region
+    # boxes standing on the terrain, in cells below the terrain region: 4x4
+    # texels when they fit, smaller otherwise, and shared (wrapped) beyond
+    # that, so every lightmap uv stays inside [0, 1] (Lightmap::lumel(uv)
+    # does not range-check, Lightmap.cpp:61-67)
     src = Mesh.create()
-    cell, cols = 4, size // 4
+    rows_px = size - terrain_rows
+    cell = 4
+    while cell > 1 and (size // cell) * (rows_px // cell) < 6 * n_boxes:
+        cell //= 2
+    cols = size // cell
+    ncells = cols * (rows_px // cell)
     k = 0
     for _ in range(n_boxes):
         s = rng.uniform(0.5, 2.0, 3).astype(F32)
@@ -216,7 +224,8 @@ def terrain_scene(seed: int = 2, verts: int = 256, n_boxes: int = 2000, size: in
         hi = np.array([cx + s[0] / 2, base + s[1], cz + s[2] / 2], F32)
         mat = palette[int(rng.integers(0, len(palette)))]
         for corners, n in _box_faces(lo, hi):
-            pos, nn, uv, idx = _quad(corners, n, _cell_rect(k, cols, cell, size, size, y0=terrain_rows))
+            pos, nn, uv, idx = _quad(corners, n, _cell_rect(k % ncells, cols, cell, size, size, y0=terrain_rows,
+                                                            gutter=1 if cell >= 3 else 0))
             src.add_faces(pos, nn, None, uv, idx, mat)
             k += 1
     inst = scene.add_mesh(src)

@@ -291,3 +291,58 @@ def test_launch_tuning_changes_no_result(cuda):
     # through the photonmap's tolerance
     for c in fg[1:]:
         np.testing.assert_allclose(c, fg[0], rtol=1e-4, atol=1e-6)
+
+
+def test_photon_shares_sum_to_the_full_emission(cuda):
+    """rl_emit_photons_range: two shares of the photon sequence, deposited into
+    two photonmap replicas, sum to the unsplit emission (the multi-GPU split)."""
+    import ctypes as C
+    from relight_b200 import _abi, parallel
+    from relight_b200.device import DeviceMap, _map_array
+    w = _small_terrain()
+    st, f = w.settings, w.scene.flat
+    rl = _relight()
+    ds = rl.device_scene(w.scene)
+    L = _abi.lib()
+    lights = C.c_void_p(f.lights.ctypes.data)
+    total = C.c_int64()
+    _abi.check(L.rl_photon_count(lights, len(f.lights), st.photon_pass_count, C.byref(total)))
+    assert total.value == st.photon_pass_count * 5 * 25000
+    reps = []
+    for k in range(3):
+        m = DeviceMap(1, w.photonmap.width, w.photonmap.height)
+        for mesh in w.photonmap.meshes:
+            m.add_mesh(ds, w.scene.meshes.index(mesh))
+        reps.append(m)
+    args = (st.photon_pass_count, st.photon_bounce_count, st.photon_energy_threshold, st.photon_max_distance, 8)
+    for k, m in enumerate(reps[:2]):
+        first, count = parallel.photon_share(total.value, k, 2)
+        _abi.check(L.rl_emit_photons_range(ds.handle, _map_array([m]), 1, lights, len(f.lights), *args, first, count,
+                                           None, None))
+    _abi.check(L.rl_emit_photons(ds.handle, _map_array([reps[2]]), 1, lights, len(f.lights), *args, None, None))
+    a, b, full = (m.download() for m in reps)
+    assert full["photons"].sum() > 1000
+    assert np.array_equal(a["photons"] + b["photons"], full["photons"])
+    np.testing.assert_allclose(a["color"] + b["color"], full["color"], rtol=1e-5, atol=1e-6)
+
+
+def test_distributed_emission_on_one_rank_matches(cuda):
+    import os
+    import socket
+    import torch.distributed as dist
+    from relight_b200 import parallel
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    os.environ["MASTER_ADDR"], os.environ["MASTER_PORT"] = "127.0.0.1", str(port)
+    dist.init_process_group("nccl", rank=0, world_size=1)
+    try:
+        w1, w2 = _small_terrain(), _small_terrain()
+        rl = _relight()
+        parallel.emit_photons_distributed(rl, w1.scene, w1.settings, seed=4)
+        rl.emit_photons(w2.scene, w2.settings, seed=4)
+        a, b = _lumels(w1.photonmap), _lumels(w2.photonmap)
+        assert np.array_equal(a["photons"], b["photons"])
+        np.testing.assert_allclose(a["gathered"], b["gathered"], rtol=1e-4, atol=1e-6)
+    finally:
+        dist.destroy_process_group()

@@ -152,7 +152,7 @@ def gpu_arm(args, rank, world, local_rank):
         if fg_events:
             fg_events[0].record(stream)
         _abi.check(L.rl_bake_indirect(ds.handle, lmap.handle, maps, 1, st.final_gather_samples,
-                                      st.final_gather_distance, sky, amb, seed + 1, 0, 1, sh))
+                                      st.final_gather_distance, sky, amb, seed + 1, None, sh))
         if fg_events:
             fg_events[1].record(stream)
 

@@ -160,19 +160,34 @@ int rl_map_valid_count(const rl_map* map, int64_t* count);
 
 /* --------------------------------------------------------------- passes */
 
-/* Relight::bakeDirectLight with LumelBakeIterator(first, step)
+/* bake::LumelBakeIterator / bake::FaceBakeIterator (baker/Baker.h:91-155,
+   baker/Baker.cpp:176-234): which lumels of the map a bake call visits.
+     kind 0  LumelBakeIterator(first, step): lumels first, first + step, ...
+             of the whole map, whichever mesh rasterised them;
+     kind 1  FaceBakeIterator(first, step) on `mesh`: the lumels rasterised
+             from faces first, first + step, ... of that scene mesh.
+   A NULL iterator means LumelBakeIterator(0, 1), the default of the
+   Relight::bake* calls (Relight.cpp:218-220). */
+typedef struct {
+    int32_t kind;
+    int32_t first;
+    int32_t step;
+    int32_t mesh;
+} rl_iterator;
+
+/* Relight::bakeDirectLight with a bake iterator
    (Relight.cpp:216-227; baker/DirectLight.cpp:46-125;
    scene/Light.cpp:372-500).  Adds every light's influence to the lumel
    colours.  `lights` and `light_vertices` ([nverts][3]) are host arrays. */
 int rl_bake_direct(const rl_scene* scene, rl_map* lightmap, const rl_light* lights, int nlights,
-                   const float* light_vertices, int nlight_vertices, int first, int step, void* stream);
+                   const float* light_vertices, int nlight_vertices, const rl_iterator* iterator, void* stream);
 
 /* Relight::bakeAmbientOcclusion (Relight.cpp:260-271;
    baker/AmbientOcclusion.cpp:46-66): colour *= 1 - occluded/(samples*fraction),
    optionally raised to `exponent`.  Directions are Philox-keyed by (seed,
    lumel index, sample). */
 int rl_bake_ao(const rl_scene* scene, rl_map* lightmap, int samples, float occluded_fraction, float max_distance,
-               float exponent, uint64_t seed, int first, int step, void* stream);
+               float exponent, uint64_t seed, const rl_iterator* iterator, void* stream);
 
 /* Relight::emitPhotons minus the gather (Relight.cpp:244-250;
    baker/Photons.cpp:50-144; scene/Light.cpp:334-361): trace
@@ -204,8 +219,8 @@ int rl_photonmap_gather(rl_map* photonmap, int radius, void* stream);
    baker/IndirectLight.cpp:47-75): final gather against the gathered
    photonmaps (maps[] by photonmap slot). */
 int rl_bake_indirect(const rl_scene* scene, rl_map* lightmap, rl_map* const* photonmaps, int nmaps, int samples,
-                     float max_distance, const float sky[3], const float ambient[3], uint64_t seed, int first,
-                     int step, void* stream);
+                     float max_distance, const float sky[3], const float ambient[3], uint64_t seed,
+                     const rl_iterator* iterator, void* stream);
 
 /* ------------------------------------------------------------- radiosity */
 

@@ -36,13 +36,23 @@ def reference_available():
 class Lumels(C.Structure):
     """rl_lumels (oracle/rl_oracle.h)."""
     _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("flags", _P), ("face", _P), ("position", _P),
-                ("normal", _P), ("color", _P), ("photons", _P), ("gathered", _P)]
+                ("normal", _P), ("color", _P), ("photons", _P), ("gathered", _P), ("mesh", _P)]
+
+
+class Iterator(C.Structure):
+    """rl_iterator (oracle/rl_oracle.h)."""
+    _fields_ = [("kind", C.c_int32), ("first", C.c_int32), ("step", C.c_int32), ("mesh", C.c_int32)]
+
+
+def iterator(first=0, step=1, mesh=None):
+    """LumelBakeIterator(first, step) if mesh is None, else FaceBakeIterator."""
+    return C.byref(Iterator(0 if mesh is None else 1, first, step, -1 if mesh is None else mesh))
 
 
 class LumelMap:
     """Numpy-backed lumel arrays (Lightmap.h:35-55) for the oracle."""
 
-    FIELDS = ("flags", "face", "position", "normal", "color", "photons", "gathered")
+    FIELDS = ("flags", "face", "position", "normal", "color", "photons", "gathered", "mesh")
 
     def __init__(self, width, height):
         n = width * height
@@ -54,6 +64,7 @@ class LumelMap:
         self.color = np.zeros((n, 3), np.float32)
         self.photons = np.zeros(n, np.int32)
         self.gathered = np.zeros((n, 3), np.float32)
+        self.mesh = np.full(n, -1, np.int32)
 
     def struct(self):
         s = Lumels()
@@ -81,14 +92,14 @@ def _load_oracle():
         "oro_philox4x32_10": (None, [_P, _P, _P]),
         "oro_init_lumels": (None, [_P, C.c_int, _P]),
         "oro_trace_segments": (None, [_P, C.c_int, _P, C.c_int, _P, _P, _P, _P, _P, _P, _P]),
-        "oro_bake_direct": (None, [_P, _P, C.c_int, _P, _P, C.c_int, C.c_int]),
-        "oro_bake_ao": (None, [_P, _P, C.c_int, C.c_float, C.c_float, C.c_float, C.c_uint64, C.c_int, C.c_int]),
+        "oro_bake_direct": (None, [_P, _P, C.c_int, _P, _P, _P]),
+        "oro_bake_ao": (None, [_P, _P, C.c_int, C.c_float, C.c_float, C.c_float, C.c_uint64, _P]),
         "oro_emit_photons": (C.c_longlong, [_P, _P, C.c_int, _P, C.c_int, C.c_int, C.c_float, C.c_float,
                                             C.c_uint64]),
         "oro_emit_photons_range": (C.c_longlong, [_P, _P, C.c_int, _P, C.c_int, C.c_int, C.c_float, C.c_float,
                                                   C.c_uint64, C.c_longlong, C.c_longlong]),
         "oro_photonmap_gather": (None, [_P, C.c_int]),
-        "oro_bake_indirect": (None, [_P, _P, _P, C.c_int, C.c_float, _P, _P, C.c_uint64, C.c_int, C.c_int]),
+        "oro_bake_indirect": (None, [_P, _P, _P, C.c_int, C.c_float, _P, _P, C.c_uint64, _P]),
         "oro_ff_pairwise": (C.c_longlong, [_P, C.c_int, _P, _P, C.c_float, _P, _P, _P]),
         "oro_ff_hemisphere": (C.c_longlong, [_P, C.c_int, _P, _P, C.c_int, C.c_float, C.c_uint64, _P, _P, _P, _P,
                                              _P, _P, _P]),
@@ -178,15 +189,16 @@ class Oracle:
                                     ptr(out["face"]))
         return out
 
-    def bake_direct(self, lm: LumelMap, first=0, step=1):
+    def bake_direct(self, lm: LumelMap, first=0, step=1, mesh=None):
         f = self.flat
         s = lm.struct()
-        self.lib.oro_bake_direct(self.ctx, ptr(f.lights), len(f.lights), ptr(f.light_vertices), C.byref(s), first,
-                                 step)
+        self.lib.oro_bake_direct(self.ctx, ptr(f.lights), len(f.lights), ptr(f.light_vertices), C.byref(s),
+                                 iterator(first, step, mesh))
 
-    def bake_ao(self, lm: LumelMap, samples, fraction, maxd, exponent, seed, first=0, step=1):
+    def bake_ao(self, lm: LumelMap, samples, fraction, maxd, exponent, seed, first=0, step=1, mesh=None):
         s = lm.struct()
-        self.lib.oro_bake_ao(self.ctx, C.byref(s), samples, fraction, maxd, exponent, seed, first, step)
+        self.lib.oro_bake_ao(self.ctx, C.byref(s), samples, fraction, maxd, exponent, seed,
+                             iterator(first, step, mesh))
 
     def emit_photons(self, pms, passes, depth, threshold, maxd, seed):
         arr = (Lumels * max(len(pms), 1))(*[p.struct() for p in pms])
@@ -204,11 +216,12 @@ class Oracle:
         s = pm.struct()
         self.lib.oro_photonmap_gather(C.byref(s), radius)
 
-    def bake_indirect(self, lm: LumelMap, pms, samples, maxd, sky, ambient, seed, first=0, step=1):
+    def bake_indirect(self, lm: LumelMap, pms, samples, maxd, sky, ambient, seed, first=0, step=1, mesh=None):
         arr = (Lumels * max(len(pms), 1))(*[p.struct() for p in pms])
         s = lm.struct()
         sky = np.asarray(sky, np.float32); amb = np.asarray(ambient, np.float32)
-        self.lib.oro_bake_indirect(self.ctx, C.byref(s), arr, samples, maxd, ptr(sky), ptr(amb), seed, first, step)
+        self.lib.oro_bake_indirect(self.ctx, C.byref(s), arr, samples, maxd, ptr(sky), ptr(amb), seed,
+                                   iterator(first, step, mesh))
 
     def ff_pairwise(self, pos, nrm, threshold):
         pos = np.ascontiguousarray(pos, np.float32); nrm = np.ascontiguousarray(nrm, np.float32)

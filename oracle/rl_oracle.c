@@ -305,6 +305,7 @@ void oro_init_lumels(const rl_scene_desc* d, int mesh, rl_lumels* lm) {
                 if (!uv_inside(a, b, cc, uv, bary)) continue;
                 size_t i = (size_t)W * v + u;
                 lm->face[i] = t - t0;
+                if (lm->mesh) lm->mesh[i] = mesh;
                 st3(lm->position + 3 * i, interp3(d->pos, f, bary[0], bary[1]));
                 st3(lm->normal + 3 * i, interp3(d->nrm, f, bary[0], bary[1]));
                 st3(lm->color + 3 * i, mk3(0, 0, 0));
@@ -312,6 +313,23 @@ void oro_init_lumels(const rl_scene_desc* d, int mesh, rl_lumels* lm) {
             }
         }
     }
+}
+
+/* ------------------------------------------------------------ iterators */
+
+/* Lumel i's turn under `it`: LumelBakeIterator::next visits i = first,
+   first + step, ... (baker/Baker.cpp:176-185); FaceBakeIterator::next visits
+   the lumels of faces first, first + step, ... of its mesh whose m_faceIdx is
+   that face (:202-234). */
+static int iter_visits(const rl_lumels* lm, const rl_iterator* it, int i) {
+    if (!(lm->flags[i] & 1)) return 0;
+    if (!it || it->kind == 0) {
+        int first = it ? it->first : 0, step = it ? it->step : 1;
+        return i >= first && (i - first) % step == 0;
+    }
+    if (!lm->mesh || lm->mesh[i] != it->mesh) return 0;
+    int f = lm->face[i];
+    return f >= it->first && (f - it->first) % it->step == 0;
 }
 
 /* ---------------------------------------------------------- direct light */
@@ -401,12 +419,11 @@ static void direct_lumel(const oro_ctx* c, const rl_light* lights, int nlights, 
 }
 
 void oro_bake_direct(const oro_ctx* c, const rl_light* lights, int nlights, const float* light_vertices,
-                     rl_lumels* lm, int first, int step) {
+                     rl_lumels* lm, const rl_iterator* it) {
     int n = lm->width * lm->height;
     ((oro_ctx*)c)->stats[0] = ((oro_ctx*)c)->stats[1] = ((oro_ctx*)c)->stats[2] = 0;
-    /* LumelBakeIterator::next (baker/Baker.cpp:176-185) */
-    for (int i = first; i < n; i += step) {
-        if (!(lm->flags[i] & 1)) continue;
+    for (int i = 0; i < n; i++) {
+        if (!iter_visits(lm, it, i)) continue;
         direct_lumel(c, lights, nlights, light_vertices, ld3(lm->position + 3 * (size_t)i),
                      ld3(lm->normal + 3 * (size_t)i), lm->color + 3 * (size_t)i);
     }
@@ -415,11 +432,11 @@ void oro_bake_direct(const oro_ctx* c, const rl_light* lights, int nlights, cons
 /* ----------------------------------------------------------- AO */
 
 void oro_bake_ao(const oro_ctx* c, rl_lumels* lm, int samples, float occluded_fraction, float max_distance,
-                 float exponent, uint64_t seed, int first, int step) {
+                 float exponent, uint64_t seed, const rl_iterator* it) {
     int n = lm->width * lm->height;
     ((oro_ctx*)c)->stats[0] = ((oro_ctx*)c)->stats[1] = ((oro_ctx*)c)->stats[2] = 0;
-    for (int i = first; i < n; i += step) {
-        if (!(lm->flags[i] & 1)) continue;
+    for (int i = 0; i < n; i++) {
+        if (!iter_visits(lm, it, i)) continue;
         v3 pos = ld3(lm->position + 3 * (size_t)i), nrm = ld3(lm->normal + 3 * (size_t)i);
         int occluded = 0;
         for (int s = 0; s < samples; s++) {
@@ -567,14 +584,14 @@ void oro_photonmap_gather(rl_lumels* pm, int radius) {
 /* ---------------------------------------------------------- final gather */
 
 void oro_bake_indirect(const oro_ctx* c, rl_lumels* lm, const rl_lumels* photonmaps, int samples,
-                       float max_distance, const float sky[3], const float ambient[3], uint64_t seed, int first,
-                       int step) {
+                       float max_distance, const float sky[3], const float ambient[3], uint64_t seed,
+                       const rl_iterator* it) {
     const rl_scene_desc* d = c->d;
     int n = lm->width * lm->height;
     ((oro_ctx*)c)->stats[0] = ((oro_ctx*)c)->stats[1] = ((oro_ctx*)c)->stats[2] = 0;
     /* IndirectLight::bakeLumel (baker/IndirectLight.cpp:47-75) */
-    for (int i = first; i < n; i += step) {
-        if (!(lm->flags[i] & 1)) continue;
+    for (int i = 0; i < n; i++) {
+        if (!iter_visits(lm, it, i)) continue;
         v3 pos = ld3(lm->position + 3 * (size_t)i), nrm = ld3(lm->normal + 3 * (size_t)i);
         float gr = 0, gg = 0, gb = 0;
         for (int k = 0; k < samples; k++) {

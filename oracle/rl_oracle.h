@@ -81,7 +81,14 @@ typedef struct {
     float* color;      /* [w*h][3] */
     int32_t* photons;  /* [w*h] */
     float* gathered;   /* [w*h][3] */
+    int32_t* mesh;     /* [w*h] scene mesh that rasterised the lumel, -1 none */
 } rl_lumels;
+
+/* bake::LumelBakeIterator (kind 0) / FaceBakeIterator (kind 1, over `mesh`)
+   (baker/Baker.h:91-155, baker/Baker.cpp:176-234); NULL = LumelBakeIterator(0, 1). */
+typedef struct {
+    int32_t kind, first, step, mesh;
+} rl_iterator;
 
 typedef struct oro_ctx oro_ctx;
 
@@ -100,14 +107,14 @@ void oro_init_lumels(const rl_scene_desc* d, int mesh, rl_lumels* lm);
 void oro_trace_segments(const oro_ctx* c, int n, const float* seg, int flags, int32_t* hit, float* point,
                         float* normal, float* rgba, float* uv, int32_t* mesh, int32_t* face);
 
-/* Relight::bakeDirectLight with LumelBakeIterator(first, step)
+/* Relight::bakeDirectLight with a bake iterator
    (Relight.cpp:216-227, baker/DirectLight.cpp:46-125). */
 void oro_bake_direct(const oro_ctx* c, const rl_light* lights, int nlights, const float* light_vertices,
-                     rl_lumels* lm, int first, int step);
+                     rl_lumels* lm, const rl_iterator* it);
 
 /* Relight::bakeAmbientOcclusion (baker/AmbientOcclusion.cpp:46-66). */
 void oro_bake_ao(const oro_ctx* c, rl_lumels* lm, int samples, float occluded_fraction, float max_distance,
-                 float exponent, uint64_t seed, int first, int step);
+                 float exponent, uint64_t seed, const rl_iterator* it);
 
 /* Relight::emitPhotons minus the gather (baker/Photons.cpp:50-144).
    photonmaps[k] is map id k; deposits go to the hit mesh's photonmap.
@@ -127,8 +134,8 @@ void oro_photonmap_gather(rl_lumels* pm, int radius);
 
 /* Relight::bakeIndirectLight (baker/IndirectLight.cpp:47-75). */
 void oro_bake_indirect(const oro_ctx* c, rl_lumels* lm, const rl_lumels* photonmaps, int samples,
-                       float max_distance, const float sky[3], const float ambient[3], uint64_t seed, int first,
-                       int step);
+                       float max_distance, const float sky[3], const float ambient[3], uint64_t seed,
+                       const rl_iterator* it);
 
 /* RadiosityBuilder::computeFormFactors with distanceFormFactor and
    refineFormFactors, maxFormFactors = 0 (radiosity/RadiosityBuilder.cpp:99-176).

@@ -34,6 +34,12 @@ class SceneDesc(C.Structure):
     ]
 
 
+class Iterator(C.Structure):
+    """rl_iterator: kind 0 LumelBakeIterator(first, step), kind 1
+    FaceBakeIterator(first, step) over one scene mesh."""
+    _fields_ = [("kind", C.c_int32), ("first", C.c_int32), ("step", C.c_int32), ("mesh", C.c_int32)]
+
+
 def _ptr(a):
     """A c_void_p to `a`'s data that holds a reference to `a` (numpy's
     data_as), so the array outlives the pointer."""
@@ -94,13 +100,13 @@ SIGNATURES = {
     "rl_map_clear": (_I, [_P, _I, _I, _P]),
     "rl_map_device_arrays": (_I, [_P, _P, _P, _P, _P, _P, _P]),
     "rl_map_valid_count": (_I, [_P, _P]),
-    "rl_bake_direct": (_I, [_P, _P, _P, _I, _P, _I, _I, _I, _P]),
-    "rl_bake_ao": (_I, [_P, _P, _I, _F, _F, _F, _U64, _I, _I, _P]),
+    "rl_bake_direct": (_I, [_P, _P, _P, _I, _P, _I, _P, _P]),
+    "rl_bake_ao": (_I, [_P, _P, _I, _F, _F, _F, _U64, _P, _P]),
     "rl_emit_photons": (_I, [_P, _P, _I, _P, _I, _I, _I, _F, _F, _U64, _P, _P]),
     "rl_emit_photons_range": (_I, [_P, _P, _I, _P, _I, _I, _I, _F, _F, _U64, _I64, _I64, _P, _P]),
     "rl_photon_count": (_I, [_P, _I, _I, _P]),
     "rl_photonmap_gather": (_I, [_P, _I, _P]),
-    "rl_bake_indirect": (_I, [_P, _P, _P, _I, _I, _F, _P, _P, _U64, _I, _I, _P]),
+    "rl_bake_indirect": (_I, [_P, _P, _P, _I, _I, _F, _P, _P, _U64, _P, _P]),
     "rl_ff_pairwise": (_I, [_P, _I, _P, _P, _F, _P, _P, _P, _I64, _P, _P]),
     "rl_ff_hemisphere": (_I, [_P, _I, _P, _P, _I, _F, _U64, _P, _I, _P, _P, _P, _I64, _P, _P, _P, _I64, _P, _P]),
     "rl_radiosity_solve": (_I, [_I, _P, _P, _P, _P, _P, _I, _P, _P]),

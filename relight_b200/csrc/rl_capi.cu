@@ -129,7 +129,7 @@ struct rl_map {
     int* d_owner = nullptr;  // rasterisation scratch: winning face per texel
     ~rl_map() {
         cudaFree(dev.flags); cudaFree(dev.face); cudaFree(dev.position); cudaFree(dev.normal);
-        cudaFree(dev.color); cudaFree(dev.photons); cudaFree(dev.gathered); cudaFree(d_owner);
+        cudaFree(dev.color); cudaFree(dev.photons); cudaFree(dev.gathered); cudaFree(dev.mesh); cudaFree(d_owner);
     }
 };
 
@@ -350,6 +350,7 @@ extern "C" int rl_map_create(int kind, int width, int height, rl_map** out) {
     if (!rc) rc = dalloc(&m->dev.color, 3 * n);
     if (!rc) rc = dalloc(&m->dev.photons, n);
     if (!rc) rc = dalloc(&m->dev.gathered, 3 * n);
+    if (!rc) rc = dalloc(&m->dev.mesh, n);
     if (!rc) rc = dalloc(&m->d_owner, n);
     if (rc) {
         delete m;
@@ -364,6 +365,7 @@ extern "C" int rl_map_create(int kind, int width, int height, rl_map** out) {
     cudaMemset(m->dev.photons, 0, 4 * n);
     cudaMemset(m->dev.gathered, 0, 12 * n);
     cudaMemset(m->d_owner, 0xff, 4 * n);
+    cudaMemset(m->dev.mesh, 0xff, 4 * n);
     std::vector<int> face(n, 0xffff);
     cudaMemcpy(m->dev.face, face.data(), 4 * n, cudaMemcpyHostToDevice);
     cudaError_t e = cudaDeviceSynchronize();
@@ -434,7 +436,7 @@ __global__ void k_raster_owner(DevScene s, int t0, int t1, int W, int H, int* ow
 }
 
 // Pass 2: Lightmap::initializeLumel (Lightmap.cpp:157-164) for the winner.
-__global__ void k_raster_init(DevScene s, int t0, DevMap m, int* owner) {
+__global__ void k_raster_init(DevScene s, int mesh, int t0, DevMap m, int* owner) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int W = m.width, H = m.height;
     if (i >= W * H) return;
@@ -448,6 +450,7 @@ __global__ void k_raster_init(DevScene s, int t0, DevMap m, int* owner) {
     float bu, bv;
     uv_inside(a, b, c, uv, bu, bv);
     m.face[i] = fl & 0xffff;
+    m.mesh[i] = mesh;
     st3(m.position + 3 * (size_t)i, interp3(s.pos, f, bu, bv));
     st3(m.normal + 3 * (size_t)i, interp3(s.nrm, f, bu, bv));
     st3(m.color + 3 * (size_t)i, mk3(0.f, 0.f, 0.f));
@@ -464,7 +467,7 @@ extern "C" int rl_map_add_mesh(rl_map* m, const rl_scene* s, int mesh, void* str
                                                             m->d_owner);
     CK_LAUNCH("k_raster_owner");
     long long n = (long long)m->dev.width * m->dev.height;
-    k_raster_init<<<blocks_for(n, 256), 256, 0, st>>>(s->dev, t0, m->dev, m->d_owner);
+    k_raster_init<<<blocks_for(n, 256), 256, 0, st>>>(s->dev, mesh, t0, m->dev, m->d_owner);
     CK_LAUNCH("k_raster_init");
     return RL_OK;
 }
@@ -628,12 +631,12 @@ __device__ float influence_from_point(const DevScene& s, V3 lpos, V3 lnrm, V3 po
 }
 
 // DirectLight::bakeLumel (baker/DirectLight.cpp:46-98), one thread per lumel.
-__global__ void k_direct(DevScene s, DevMap m, const __grid_constant__ LightTable T, int first, int step,
-                         long long count, int* status) {
+__global__ void k_direct(DevScene s, DevMap m, const __grid_constant__ LightTable T, Iter it, long long count,
+                         int* status) {
     long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (k >= count) return;
-    long long i = first + k * step;
-    if (!(m.flags[i] & 1)) return;
+    long long i;
+    if (!iter_lumel(m, it, k, i)) return;
     V3 pos = ld3(m.position + 3 * i), nrm = ld3(m.normal + 3 * i);
     float* col = m.color + 3 * i;
     float cr = col[0], cg = col[1], cb = col[2];
@@ -659,22 +662,34 @@ __global__ void k_direct(DevScene s, DevMap m, const __grid_constant__ LightTabl
     col[0] = cr; col[1] = cg; col[2] = cb;
 }
 
-static long long iter_count(long long n, int first, int step) {
-    if (first >= n) return 0;
-    return (n - first + step - 1) / step;
+// Validate an rl_iterator (NULL = LumelBakeIterator(0, 1)) and size the
+// launch: one thread per visited lumel (kind 0) or per lumel (kind 1).
+static int make_iter(const rl_iterator* it, const rl_scene* s, long long n, Iter& out, long long& count) {
+    Iter d{0, 0, 1, -1};
+    if (it) d = Iter{it->kind, it->first, it->step, it->mesh};
+    if (d.kind < 0 || d.kind > 1 || d.first < 0 || d.step <= 0)
+        return fail(RL_INVALID_CALL, "bad iterator (kind %d first %d step %d)", d.kind, d.first, d.step);
+    if (d.kind == 1 && (d.mesh < 0 || d.mesh >= s->nmeshes))
+        return fail(RL_INVALID_CALL, "face iterator: mesh %d out of range", d.mesh);
+    out = d;
+    if (d.kind == 1) count = n;
+    else count = d.first >= n ? 0 : (n - d.first + d.step - 1) / d.step;
+    return RL_OK;
 }
 
 extern "C" int rl_bake_direct(const rl_scene* s, rl_map* lm, const rl_light* lights, int nlights,
-                              const float* light_vertices, int nlight_vertices, int first, int step, void* stream) {
+                              const float* light_vertices, int nlight_vertices, const rl_iterator* iterator,
+                              void* stream) {
     if (!s || !lm) return fail(RL_INVALID_CALL, "rl_bake_direct: null argument");
-    if (first < 0 || step <= 0) return fail(RL_INVALID_CALL, "rl_bake_direct: bad iterator (first %d step %d)", first, step);
     static thread_local LightTable T;
     int rc = make_light_table(lights, nlights, light_vertices, nlight_vertices, T);
     if (rc) return rc;
-    long long n = (long long)lm->dev.width * lm->dev.height;
-    long long count = iter_count(n, first, step);
+    long long n = (long long)lm->dev.width * lm->dev.height, count = 0;
+    Iter it;
+    rc = make_iter(iterator, s, n, it, count);
+    if (rc) return rc;
     if (count == 0 || nlights == 0) return RL_OK;
-    k_direct<<<blocks_for(count, 128), 128, 0, S(stream)>>>(s->dev, lm->dev, T, first, step, count, s->d_status);
+    k_direct<<<blocks_for(count, 128), 128, 0, S(stream)>>>(s->dev, lm->dev, T, it, count, s->d_status);
     CK_LAUNCH("k_direct");
     return RL_OK;
 }
@@ -703,23 +718,24 @@ struct AoGen {
 
 template <int kWidth>
 __global__ void __launch_bounds__(256) k_ao(DevScene s, DevMap m, int samples, float fraction, float maxd,
-                                            float exponent, uint2 key, int first, int step, long long count,
-                                            int refill, int* status) {
+                                            float exponent, uint2 key, Iter it, long long count, int refill,
+                                            int* status) {
     long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (k >= count) return;
-    long long i = first + k * step;
+    long long i;
+    bool valid = iter_lumel(m, it, k, i);
     AoGen g;
     g.pos = ld3(m.position + 3 * i);
     g.nrm = ld3(m.normal + 3 * i);
     g.key = key;
     g.item = (uint32_t)i;
     g.j = 0;
-    g.samples = (m.flags[i] & 1) ? samples : 0;
+    g.samples = valid ? samples : 0;
     g.occluded = 0;
     g.maxd = maxd;
     if (kWidth == 4) ray_loop4<true>(s, g, refill, status);
     else ray_loop<true>(s, g, refill, status);
-    if (!(m.flags[i] & 1)) return;
+    if (!valid) return;
     float value = 1.0f - g.occluded / (samples * fraction);
     if (fabsf(1.0f - exponent) > 0.01f) value = powf(value, exponent);
     float* col = m.color + 3 * i;
@@ -727,17 +743,19 @@ __global__ void __launch_bounds__(256) k_ao(DevScene s, DevMap m, int samples, f
 }
 
 extern "C" int rl_bake_ao(const rl_scene* s, rl_map* lm, int samples, float fraction, float maxd, float exponent,
-                          uint64_t seed, int first, int step, void* stream) {
+                          uint64_t seed, const rl_iterator* iterator, void* stream) {
     if (!s || !lm) return fail(RL_INVALID_CALL, "rl_bake_ao: null argument");
-    if (samples <= 0 || first < 0 || step <= 0) return fail(RL_INVALID_CALL, "rl_bake_ao: bad arguments");
-    long long n = (long long)lm->dev.width * lm->dev.height;
-    long long count = iter_count(n, first, step);
+    if (samples <= 0) return fail(RL_INVALID_CALL, "rl_bake_ao: samples must be positive");
+    long long n = (long long)lm->dev.width * lm->dev.height, count = 0;
+    Iter it;
+    int rc = make_iter(iterator, s, n, it, count);
+    if (rc) return rc;
     if (count == 0) return RL_OK;
     uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
     int bs = g_tune[RL_TUNE_AO_BLOCK];
     auto kern = g_tune[RL_TUNE_BVH_WIDTH] == 4 ? k_ao<4> : k_ao<2>;
-    kern<<<blocks_for(count, bs), bs, 0, S(stream)>>>(s->dev, lm->dev, samples, fraction, maxd, exponent, key,
-                                                      first, step, count, g_tune[RL_TUNE_AO_REFILL], s->d_status);
+    kern<<<blocks_for(count, bs), bs, 0, S(stream)>>>(s->dev, lm->dev, samples, fraction, maxd, exponent, key, it,
+                                                      count, g_tune[RL_TUNE_AO_REFILL], s->d_status);
     CK_LAUNCH("k_ao");
     return RL_OK;
 }
@@ -987,12 +1005,12 @@ struct FgGen {
 
 template <int kWidth>
 __global__ void __launch_bounds__(256) k_indirect(DevScene s, DevMap m, const __grid_constant__ GatherMaps G,
-                                                  int samples, float maxd, V3 sky, V3 amb, uint2 key, int first,
-                                                  int step, long long count, int refill, int* status) {
+                                                  int samples, float maxd, V3 sky, V3 amb, uint2 key, Iter it,
+                                                  long long count, int refill, int* status) {
     long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (k >= count) return;
-    long long i = first + k * step;
-    bool valid = (m.flags[i] & 1) != 0;
+    long long i;
+    bool valid = iter_lumel(m, it, k, i);
     FgGen g;
     g.s = &s;
     g.G = &G;
@@ -1017,14 +1035,15 @@ __global__ void __launch_bounds__(256) k_indirect(DevScene s, DevMap m, const __
 }
 
 extern "C" int rl_bake_indirect(const rl_scene* s, rl_map* lm, rl_map* const* maps, int nmaps, int samples,
-                                float maxd, const float sky[3], const float ambient[3], uint64_t seed, int first,
-                                int step, void* stream) {
+                                float maxd, const float sky[3], const float ambient[3], uint64_t seed,
+                                const rl_iterator* iterator, void* stream) {
     if (!s || !lm || (nmaps > 0 && !maps)) return fail(RL_INVALID_CALL, "rl_bake_indirect: null argument");
-    if (samples <= 0 || first < 0 || step <= 0 || nmaps > kMaxPhotonmaps)
-        return fail(RL_INVALID_CALL, "rl_bake_indirect: bad arguments");
+    if (samples <= 0 || nmaps > kMaxPhotonmaps) return fail(RL_INVALID_CALL, "rl_bake_indirect: bad arguments");
     cudaStream_t st = S(stream);
-    long long n = (long long)lm->dev.width * lm->dev.height;
-    long long count = iter_count(n, first, step);
+    long long n = (long long)lm->dev.width * lm->dev.height, count = 0;
+    Iter it;
+    int rc = make_iter(iterator, s, n, it, count);
+    if (rc) return rc;
     if (count == 0) return RL_OK;
     static thread_local GatherMaps G;
     memset(&G, 0, sizeof G);
@@ -1038,8 +1057,8 @@ extern "C" int rl_bake_indirect(const rl_scene* s, rl_map* lm, rl_map* const* ma
     uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
     int bs = g_tune[RL_TUNE_FG_BLOCK];
     auto kern = g_tune[RL_TUNE_BVH_WIDTH] == 4 ? k_indirect<4> : k_indirect<2>;
-    kern<<<blocks_for(count, bs), bs, 0, st>>>(s->dev, lm->dev, G, samples, maxd, skyv, ambv, key, first, step,
-                                              count, g_tune[RL_TUNE_FG_REFILL], s->d_status);
+    kern<<<blocks_for(count, bs), bs, 0, st>>>(s->dev, lm->dev, G, samples, maxd, skyv, ambv, key, it, count,
+                                              g_tune[RL_TUNE_FG_REFILL], s->d_status);
     CK_LAUNCH("k_indirect");
     return RL_OK;
 }

@@ -53,12 +53,32 @@ struct DevMap {
     int width, height;
     int* flags;
     int* face;
+    int* mesh;  // scene mesh whose faces rasterised the lumel, -1 none
     float* position;
     float* normal;
     float* color;
     int* photons;
     float* gathered;
 };
+
+// bake::LumelBakeIterator / FaceBakeIterator (baker/Baker.h:91-155) as a
+// predicate over lumels: kind 0 visits lumels first, first + step, ...; kind 1
+// visits every lumel rasterised from face first, first + step, ... of `mesh`.
+struct Iter {
+    int kind, first, step, mesh;
+};
+
+// Thread k's lumel i under `it`, and whether it is to be baked.
+__device__ __forceinline__ bool iter_lumel(const DevMap& m, const Iter& it, long long k, long long& i) {
+    if (it.kind == 0) {
+        i = it.first + k * it.step;
+        return (m.flags[i] & 1) != 0;
+    }
+    i = k;
+    if (!(m.flags[i] & 1) || m.mesh[i] != it.mesh) return false;
+    int f = m.face[i];
+    return f >= it.first && (f - it.first) % it.step == 0;
+}
 
 constexpr int kHitPoint = 1, kHitUv = 2, kHitColor = 4, kHitNormal = 8, kHitUseAlpha = 16;
 constexpr int kStackSize = 64;

@@ -20,7 +20,16 @@ from .api import (AmbientOcclusionSettings, IndirectLightSettings, Lightmap, Mes
 
 @dataclass
 class LumelBakeIterator:
-    """bake::LumelBakeIterator (baker/Baker.h:138-148): lumels first, first+step, ..."""
+    """bake::LumelBakeIterator (baker/Baker.h:138-148): lumels first, first+step, ...
+    of the mesh's whole lightmap (whichever mesh rasterised them)."""
+    first: int = 0
+    step: int = 1
+
+
+@dataclass
+class FaceBakeIterator:
+    """bake::FaceBakeIterator (baker/Baker.h:151-155): the lumels rasterised
+    from the baked mesh's faces first, first+step, ..."""
     first: int = 0
     step: int = 1
 
@@ -170,12 +179,14 @@ class Relight:
         return scene._device
 
     @staticmethod
-    def _iter(iterator):
+    def _iter(scene, mesh, iterator):
         if iterator is None:
-            return 0, 1
+            return None
         if isinstance(iterator, LumelBakeIterator):
-            return iterator.first, iterator.step
-        raise NotImplementedError("only LumelBakeIterator is supported on the device")
+            return C.byref(_abi.Iterator(0, iterator.first, iterator.step, -1))
+        if isinstance(iterator, FaceBakeIterator):
+            return C.byref(_abi.Iterator(1, iterator.first, iterator.step, scene.meshes.index(mesh)))
+        raise TypeError("iterator must be a LumelBakeIterator or a FaceBakeIterator")
 
     def _check_mesh(self, scene: Scene, mesh: Mesh):
         if mesh.face_count() == 0 or mesh.lightmap is None:
@@ -189,11 +200,11 @@ class Relight:
         if st:
             return st
         ds = self.device_scene(scene)
-        first, step = self._iter(iterator)
+        it = self._iter(scene, mesh, iterator)
         f = scene.flat
         check(lib().rl_bake_direct(ds.handle, mesh.lightmap._device.handle, C.c_void_p(f.lights.ctypes.data),
                                    len(f.lights), C.c_void_p(f.light_vertices.ctypes.data),
-                                   int(sum(int(l["vertex_count"]) for l in f.lights)), first, step, self.stream))
+                                   int(sum(int(l["vertex_count"]) for l in f.lights)), it, self.stream))
         return RelightStatus.RelightSuccess
 
     def bake_ambient_occlusion(self, scene: Scene, mesh: Mesh, progress, settings: AmbientOcclusionSettings,
@@ -203,10 +214,10 @@ class Relight:
         if st:
             return st
         ds = self.device_scene(scene)
-        first, step = self._iter(iterator)
+        it = self._iter(scene, mesh, iterator)
         seed = self.next_seed() if seed is None else seed
         check(lib().rl_bake_ao(ds.handle, mesh.lightmap._device.handle, settings.samples, settings.occluded_fraction,
-                               settings.max_distance, settings.exponent, seed, first, step, self.stream))
+                               settings.max_distance, settings.exponent, seed, it, self.stream))
         return RelightStatus.RelightSuccess
 
     def emit_photons(self, scene: Scene, settings: IndirectLightSettings, seed: Optional[int] = None) -> RelightStatus:
@@ -230,14 +241,14 @@ class Relight:
         if st:
             return st
         ds = self.device_scene(scene)
-        first, step = self._iter(iterator)
+        it = self._iter(scene, mesh, iterator)
         maps = [m._device for m in scene.flat.photonmaps]
         sky = (C.c_float * 3)(*[float(x) for x in settings.sky_color])
         amb = (C.c_float * 3)(*[float(x) for x in settings.ambient_color])
         seed = self.next_seed() if seed is None else seed
         check(lib().rl_bake_indirect(ds.handle, mesh.lightmap._device.handle, _map_array(maps), len(maps),
                                      settings.final_gather_samples, settings.final_gather_distance, sky, amb, seed,
-                                     first, step, self.stream))
+                                     it, self.stream))
         return RelightStatus.RelightSuccess
 
 

@@ -346,3 +346,31 @@ def test_distributed_emission_on_one_rank_matches(cuda):
         np.testing.assert_allclose(a["gathered"], b["gathered"], rtol=1e-4, atol=1e-6)
     finally:
         dist.destroy_process_group()
+
+
+def test_face_iterator_bakes_match_oracle(cuda):
+    """FaceBakeIterator(first, step) per mesh of a shared lightmap, for the
+    direct, AO and final-gather bakes."""
+    from relight_b200.device import FaceBakeIterator
+    w = _small_terrain()
+    st = w.settings
+    rl = _relight()
+    rl.emit_photons(w.scene, st, seed=6)
+    g = _lumels(w.photonmap)
+    orc = Oracle(w.scene.flat).bind_scene(w.scene)
+    pm = orc.maps("photonmap")[0]
+    pm.gathered[:] = g["gathered"]
+    lm = orc.maps()[0]
+    for k, mesh in enumerate(w.meshes):
+        it = FaceBakeIterator(k % 3, 3)
+        mi = w.scene.meshes.index(mesh)
+        rl.bake_direct_light(w.scene, mesh, None, it)
+        orc.bake_direct(lm, k % 3, 3, mesh=mi)
+        rl.bake_ambient_occlusion(w.scene, mesh, None, scenes.AmbientOcclusionSettings(8, 0.8, 2.0, 1.0), it, seed=k)
+        orc.bake_ao(lm, 8, 0.8, 2.0, 1.0, k, k % 3, 3, mesh=mi)
+        rl.bake_indirect_light(w.scene, mesh, None, st, it, seed=100 + k)
+        orc.bake_indirect(lm, [pm], st.final_gather_samples, st.final_gather_distance, st.sky_color,
+                          st.ambient_color, 100 + k, k % 3, 3, mesh=mi)
+    gl = _lumels(w.lightmap)
+    assert (lm.color.sum(1) > 0).sum() > 500
+    assert np.array_equal(gl["color"], lm.color)

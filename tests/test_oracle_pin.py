@@ -213,3 +213,19 @@ def test_final_gather_statistics_match_reference():
     a, b = _rmse(lm.color[tex], ex), _rmse(r.color[tex], ex)
     assert a <= 1.25 * b and b <= 1.25 * a
     del C_float3
+
+
+@needs_ref
+def test_face_iterator_direct_light_matches_reference():
+    """FaceBakeIterator over each mesh of a shared lightmap (the iterator
+    Relight's FullBakeJob hands its workers, Worker.cpp:69-73)."""
+    w = scenes.terrain_scene(verts=40, n_boxes=40, size=96, tiles=2)
+    ref = RefScene(w.scene)
+    orc = Oracle(w.scene.flat).bind_scene(w.scene)
+    lm = orc.maps()[0]
+    for k, mesh in enumerate(w.meshes):
+        ref.lib.ref_bake_direct(ref.h, ref.mesh(mesh), 1, k % 2, 2)
+        orc.bake_direct(lm, k % 2, 2, mesh=w.scene.meshes.index(mesh))
+    r = ref.lumels(w.lightmap)
+    assert (r.color.sum(1) > 0).sum() > 500
+    assert np.array_equal(lm.color, r.color)

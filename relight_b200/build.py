@@ -20,13 +20,14 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "librelight_b200.so")
 
-SOURCES = ["rl_capi.cu", "rl_bvh.cpp"]
-HEADERS = ["rl_device.cuh", "rl_bvh.h", os.path.join("..", "..", "include", "relight_b200.h")]
+SOURCES = ["rl_capi.cu", "rl_bvh.cpp", os.path.join("host", "relight_api.cpp")]
+HEADERS = ["rl_device.cuh", "rl_bvh.h", os.path.join("..", "..", "include", "relight_b200.h"),
+           os.path.join("..", "..", "include", "relight", "Relight.h")]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "--fmad=false", "-lineinfo", "-std=c++17",
-    "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
+    "-Xcompiler", "-fPIC", "-Xcompiler", "-O3", "-Xcompiler", "-ffp-contract=off",
     "-shared", "-cudart", "static",
 ]
 
@@ -57,6 +58,19 @@ def build(force: bool = False, verbose: bool = False) -> str:
         raise RuntimeError("nvcc failed:\n" + r.stdout + r.stderr)
     os.replace(OUT + ".tmp", OUT)
     return OUT
+
+
+def build_cpp_example(out_dir: str) -> str:
+    """Compile tests/cpp/bake_room.cpp, a Relight C++ program, against the
+    C++ API (include/relight/Relight.h) and this library."""
+    src = os.path.join(ROOT, "tests", "cpp", "bake_room.cpp")
+    exe = os.path.join(out_dir, "bake_room")
+    cmd = [os.environ.get("CXX", "g++"), "-std=c++17", "-O2", "-I", os.path.join(ROOT, "include"), src,
+           "-L", HERE, "-lrelight_b200", "-Wl,-rpath," + HERE, "-o", exe]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("C++ example failed to build:\n" + r.stdout + r.stderr)
+    return exe
 
 
 if __name__ == "__main__":

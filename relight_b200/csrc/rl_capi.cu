@@ -555,7 +555,8 @@ struct LightTable {
     float verts[3 * kMaxLightVerts];
 };
 
-static int make_light_table(const rl_light* lights, int nlights, const float* lverts, int nverts, LightTable& T) {
+static int make_light_table(const rl_light* lights, int nlights, const float* lverts, int nverts, LightTable& T,
+                            bool use_vertices = true) {
     if (nlights < 0 || nlights > kMaxLights) return fail(RL_INVALID_CALL, "at most %d lights per call", kMaxLights);
     if (nverts < 0 || nverts > kMaxLightVerts)
         return fail(RL_INVALID_CALL, "at most %d light vertices per call", kMaxLightVerts);
@@ -565,10 +566,16 @@ static int make_light_table(const rl_light* lights, int nlights, const float* lv
     T.n = nlights;
     T.nverts = nverts;
     for (int l = 0; l < nlights; l++) {
+        T.l[l] = lights[l];
+        if (!use_vertices) {
+            // photon emission starts at the light's position only
+            // (PhotonEmitter::emit, scene/Light.cpp:340-344)
+            T.l[l].vertex_first = T.l[l].vertex_count = 0;
+            continue;
+        }
         if (lights[l].vertex_count > 0 &&
             (lights[l].vertex_first < 0 || lights[l].vertex_first + lights[l].vertex_count > nverts))
             return fail(RL_INVALID_CALL, "light %d: vertex range outside the light-vertex pool", l);
-        T.l[l] = lights[l];
     }
     if (nverts) memcpy(T.verts, lverts, 12 * (size_t)nverts);
     return RL_OK;
@@ -837,7 +844,7 @@ static int emit_photons(const rl_scene* s, rl_map* const* maps, int nmaps, const
     if (nmaps > kMaxPhotonmaps) return fail(RL_INVALID_CALL, "rl_emit_photons: at most %d photonmaps", kMaxPhotonmaps);
     cudaStream_t st = S(stream);
     static thread_local LightTable LT;
-    int rc = make_light_table(lights, nlights, nullptr, 0, LT);
+    int rc = make_light_table(lights, nlights, nullptr, 0, LT, false);
     if (rc) return rc;
     static thread_local PhotonTables T;
     memset(&T, 0, sizeof T);

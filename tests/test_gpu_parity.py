@@ -136,6 +136,32 @@ def _small_terrain():
     return scenes.terrain_scene(verts=64, n_boxes=80, size=128, tiles=2, fg_samples=16, passes=1, bounces=3)
 
 
+def test_photons_from_room_lights_with_area_light(cuda):
+    """Point, spot and area lights all emit from their position."""
+    w = scenes.room_scene(size=64)
+    pm_scene = w.scene
+    rl = _relight()
+    # the room has no photonmap: add one over the same mesh through a second scene
+    from relight_b200.api import Photonmap, Scene
+    sc = Scene()
+    sc.begin()
+    inst = sc.add_mesh(w.mesh.source[0])
+    pm = Photonmap(64, 64)
+    pm.add_mesh(inst)
+    for l in pm_scene.lights:
+        sc.add_light(l)
+    sc.end()
+    st = scenes.IndirectLightSettings(1, 2, 0.05, 20.0, 8, 20.0, 7)
+    rl.emit_photons(sc, st, seed=3)
+    g = _lumels(pm)
+    orc = Oracle(sc.flat).bind_scene(sc)
+    opm = orc.maps("photonmap")[0]
+    stored = orc.emit_photons([opm], 1, 2, 0.05, 20.0, 3)
+    assert stored > 1000
+    assert np.array_equal(g["photons"], opm.photons)
+    np.testing.assert_allclose(g["color"], opm.color, rtol=1e-5, atol=1e-6)
+
+
 def test_photons_and_gather(cuda):
     w = _small_terrain()
     st = w.settings

@@ -286,8 +286,17 @@ int rl_radiosity_solve_noalloc(int n, const int64_t* d_row_ptr, const int32_t* d
      *_REFILL: a warp restarts finished lanes' rays once this many of its
                live lanes (1..32) have finished;
      *_BLOCK:  threads per block (64, 128 or 256);
-     RL_TUNE_BVH_WIDTH: 2 (binary nodes) or 4 (4-wide nodes). */
-enum { RL_TUNE_FG_REFILL = 0, RL_TUNE_FG_BLOCK = 1, RL_TUNE_AO_REFILL = 2, RL_TUNE_AO_BLOCK = 3, RL_TUNE_BVH_WIDTH = 4 };
+     RL_TUNE_BVH_WIDTH: 2 (binary nodes) or 4 (4-wide nodes);
+     RL_TUNE_SPECULATIVE: 1 = binary traversal parks leaves until the whole
+                          warp has one (speculative traversal), 0 = off. */
+enum {
+    RL_TUNE_FG_REFILL = 0,
+    RL_TUNE_FG_BLOCK = 1,
+    RL_TUNE_AO_REFILL = 2,
+    RL_TUNE_AO_BLOCK = 3,
+    RL_TUNE_BVH_WIDTH = 4,
+    RL_TUNE_SPECULATIVE = 5
+};
 int rl_tune_set(int param, int value);
 int rl_tune_get(int param, int* value);
 

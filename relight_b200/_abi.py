@@ -16,7 +16,7 @@ LIB_PATH = os.path.join(_HERE, "librelight_b200.so")
 RL_OK, RL_INVALID_CALL, RL_NOT_IMPLEMENTED, RL_OUT_OF_MEMORY, RL_CUDA_ERROR, RL_CAPACITY = range(6)
 HIT_POINT, HIT_UV, HIT_COLOR, HIT_NORMAL, HIT_USE_ALPHA = 1, 2, 4, 8, 16
 HIT_ALL = 15
-TUNE_FG_REFILL, TUNE_FG_BLOCK, TUNE_AO_REFILL, TUNE_AO_BLOCK, TUNE_BVH_WIDTH = 0, 1, 2, 3, 4
+TUNE_FG_REFILL, TUNE_FG_BLOCK, TUNE_AO_REFILL, TUNE_AO_BLOCK, TUNE_BVH_WIDTH, TUNE_SPECULATIVE = 0, 1, 2, 3, 4, 5
 SOLVE_NOALLOC_MAX_PATCHES = 65536
 
 

@@ -46,16 +46,30 @@ def set_width(width):
     _abi.check(_abi.lib().rl_tune_set(_abi.TUNE_BVH_WIDTH, int(width)))
 
 
-def tune(run, kernel="indirect", refills=REFILLS, blocks=BLOCKS, widths=(4,), reps=2, stream=None):
+def get_speculative():
+    v = C.c_int()
+    _abi.check(_abi.lib().rl_tune_get(_abi.TUNE_SPECULATIVE, C.byref(v)))
+    return v.value
+
+
+def set_speculative(on):
+    _abi.check(_abi.lib().rl_tune_set(_abi.TUNE_SPECULATIVE, int(bool(on))))
+
+
+def tune(run, kernel="indirect", refills=REFILLS, blocks=BLOCKS, widths=(2,), speculative=(0, 1), reps=2,
+         stream=None):
     """`run()` enqueues one call of `kernel` ("indirect" or "ao") on `stream`
     (a torch stream, None = the current one).  Returns (best, table), table
-    mapping (refill, block, width) -> milliseconds; the best setting is left
-    applied.  The BVH width is shared by both kernels."""
+    mapping (refill, block, width, speculative) -> milliseconds; the best
+    setting is left applied.  Width and speculation are shared by both kernels."""
     import torch
     st = stream or torch.cuda.current_stream()
     table = {}
-    for width, refill, block in itertools.product(widths, refills, blocks):
+    for width, spec, refill, block in itertools.product(widths, speculative, refills, blocks):
+        if width == 4 and spec:
+            continue
         set_width(width)
+        set_speculative(spec)
         set(refill, block, kernel)
         run()
         ms = []
@@ -66,8 +80,9 @@ def tune(run, kernel="indirect", refills=REFILLS, blocks=BLOCKS, widths=(4,), re
             e1.record(st)
             e1.synchronize()
             ms.append(e0.elapsed_time(e1))
-        table[(refill, block, width)] = min(ms)
+        table[(refill, block, width, spec)] = min(ms)
     best = min(table, key=table.get)
     set(best[0], best[1], kernel)
     set_width(best[2])
-    return {"refill": best[0], "block": best[1], "width": best[2], "ms": table[best]}, table
+    set_speculative(best[3])
+    return {"refill": best[0], "block": best[1], "width": best[2], "speculative": best[3], "ms": table[best]}, table

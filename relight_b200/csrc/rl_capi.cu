@@ -64,7 +64,7 @@ inline cudaStream_t S(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 // Launch tuning (rl_tune_set): per ray-stream kernel, the number of lanes a
 // warp waits for before refilling rays and the threads per block.  Defaults
 // are the autotuner's picks on the terrain final-gather / room AO workloads.
-int g_tune[5] = {24, 64, 32, 128, 2};  // + BVH width of the ray-stream kernels
+int g_tune[6] = {24, 64, 32, 128, 2, 0};  // + BVH width, speculative traversal
 
 inline unsigned blocks_for(long long n, int threads) { return (unsigned)((n + threads - 1) / threads); }
 
@@ -146,8 +146,9 @@ extern "C" int rl_tune_set(int param, int value) {
     bool refill = param == RL_TUNE_FG_REFILL || param == RL_TUNE_AO_REFILL;
     bool block = param == RL_TUNE_FG_BLOCK || param == RL_TUNE_AO_BLOCK;
     bool width = param == RL_TUNE_BVH_WIDTH;
+    bool spec = param == RL_TUNE_SPECULATIVE;
     if ((refill && value >= 1 && value <= 32) || (block && (value == 64 || value == 128 || value == 256)) ||
-        (width && (value == 2 || value == 4)))
+        (width && (value == 2 || value == 4)) || (spec && (value == 0 || value == 1)))
         g_tune[param] = value;
     else
         return fail(RL_INVALID_CALL, "rl_tune_set: bad parameter %d or value %d", param, value);
@@ -155,7 +156,7 @@ extern "C" int rl_tune_set(int param, int value) {
 }
 
 extern "C" int rl_tune_get(int param, int* value) {
-    if (!value || param < 0 || param > 4) return fail(RL_INVALID_CALL, "rl_tune_get: bad parameter");
+    if (!value || param < 0 || param > 5) return fail(RL_INVALID_CALL, "rl_tune_get: bad parameter");
     *value = g_tune[param];
     return RL_OK;
 }
@@ -741,6 +742,7 @@ __global__ void __launch_bounds__(256) k_ao(DevScene s, DevMap m, int samples, f
     g.occluded = 0;
     g.maxd = maxd;
     if (kWidth == 4) ray_loop4<true>(s, g, refill, status);
+    else if (kWidth == 3) ray_loop_spec<true>(s, g, refill, status);
     else ray_loop<true>(s, g, refill, status);
     if (!valid) return;
     float value = 1.0f - g.occluded / (samples * fraction);
@@ -760,7 +762,7 @@ extern "C" int rl_bake_ao(const rl_scene* s, rl_map* lm, int samples, float frac
     if (count == 0) return RL_OK;
     uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
     int bs = g_tune[RL_TUNE_AO_BLOCK];
-    auto kern = g_tune[RL_TUNE_BVH_WIDTH] == 4 ? k_ao<4> : k_ao<2>;
+    auto kern = g_tune[RL_TUNE_BVH_WIDTH] == 4 ? k_ao<4> : (g_tune[RL_TUNE_SPECULATIVE] ? k_ao<3> : k_ao<2>);
     kern<<<blocks_for(count, bs), bs, 0, S(stream)>>>(s->dev, lm->dev, samples, fraction, maxd, exponent, key, it,
                                                       count, g_tune[RL_TUNE_AO_REFILL], s->d_status);
     CK_LAUNCH("k_ao");
@@ -1034,6 +1036,7 @@ __global__ void __launch_bounds__(256) k_indirect(DevScene s, DevMap m, const __
     g.influence = 0.f;
     g.dir = mk3(0.f, 0.f, 0.f);
     if (kWidth == 4) ray_loop4<false>(s, g, refill, status);
+    else if (kWidth == 3) ray_loop_spec<false>(s, g, refill, status);
     else ray_loop<false>(s, g, refill, status);
     if (!valid) return;
     float ns = (float)samples;
@@ -1063,7 +1066,8 @@ extern "C" int rl_bake_indirect(const rl_scene* s, rl_map* lm, rl_map* const* ma
     V3 ambv = {ambient ? ambient[0] : 0.f, ambient ? ambient[1] : 0.f, ambient ? ambient[2] : 0.f};
     uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
     int bs = g_tune[RL_TUNE_FG_BLOCK];
-    auto kern = g_tune[RL_TUNE_BVH_WIDTH] == 4 ? k_indirect<4> : k_indirect<2>;
+    auto kern = g_tune[RL_TUNE_BVH_WIDTH] == 4 ? k_indirect<4>
+                                                : (g_tune[RL_TUNE_SPECULATIVE] ? k_indirect<3> : k_indirect<2>);
     kern<<<blocks_for(count, bs), bs, 0, st>>>(s->dev, lm->dev, G, samples, maxd, skyv, ambv, key, it, count,
                                               g_tune[RL_TUNE_FG_REFILL], s->d_status);
     CK_LAUNCH("k_indirect");

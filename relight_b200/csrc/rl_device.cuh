@@ -409,6 +409,106 @@ __device__ __forceinline__ void ray_loop(const DevScene& s, Gen& g, int refill, 
     }
 }
 
+template <bool kAny, typename Gen>
+__device__ __forceinline__ void ray_loop_spec(const DevScene& s, Gen& g, int refill, int* overflow) {
+    V3 o = mk3(0.f, 0.f, 0.f), d = o, idir = o, ood = o;
+    float tnear = 0.f, tfar = 0.f, best = 0.f;
+    int best_gid = 0x7fffffff;
+    RayHit hit;
+    hit.gid = -1; hit.t = hit.u = hit.v = 0.f;
+    int stack[kStackSize];
+    int sp = 0;
+    int node = kNodeDone;
+    bool have = false, exhausted = false;
+    const unsigned mask = __activemask();
+    for (;;) {
+        // Lanes whose ray ended wait until `refill` of the warp's live lanes
+        // (or all of them) have ended, then start their next rays together,
+        // so ray generation and hit shading run on many lanes at once.
+        bool need = node == kNodeDone && !exhausted;
+        unsigned alive = __ballot_sync(mask, !exhausted);
+        if (alive == 0) break;
+        unsigned needm = __ballot_sync(mask, need);
+        if (need && (__popc(needm) >= refill || needm == alive)) {
+            if (have) {
+                g.finish(hit);
+                have = false;
+            }
+            if (g.next(o, d, tnear, tfar)) {
+                have = true;
+                idir = mk3(safe_inv(d.x), safe_inv(d.y), safe_inv(d.z));
+                ood = mk3(o.x * idir.x, o.y * idir.y, o.z * idir.z);
+                best = tfar;
+                best_gid = 0x7fffffff;
+                hit.gid = -1;
+                sp = 0;
+                node = s.ntris > 0 ? 0 : kNodeDone;
+            } else {
+                exhausted = true;
+            }
+        }
+        if (node == kNodeDone) continue;
+        // Inner nodes with speculative leaf postponing (Aila & Laine, "Understanding
+        // the efficiency of ray traversal on GPUs", HPG 2009): a lane that reaches
+        // a leaf parks it and keeps descending until every lane of the warp has a
+        // leaf, then all lanes test their leaves together.
+        int leaf = 0;  // 0: none parked; otherwise a leaf code
+        while (node >= 0) {
+            const float4* np = s.nodes + 4 * (size_t)node;
+            float4 n0 = __ldg(np), n1 = __ldg(np + 1), n2 = __ldg(np + 2), n3 = __ldg(np + 3);
+            bool h0, h1;
+            float e0, e1;
+            slab2(n0, n1, n2, idir, ood, tnear, best, h0, h1, e0, e1);
+            int c0 = __float_as_int(n3.x), c1 = __float_as_int(n3.y);
+            if (h0 && h1) {
+                int nearc = c0, farc = c1;
+                if (e1 < e0) { nearc = c1; farc = c0; }
+                if (sp < kStackSize) stack[sp++] = farc;
+                else if (overflow) *overflow = 1;
+                node = nearc;
+            } else if (h0) {
+                node = c0;
+            } else if (h1) {
+                node = c1;
+            } else {
+                node = sp > 0 ? stack[--sp] : kNodeDone;
+            }
+            if (node < 0 && node != kNodeDone && leaf == 0) {
+                leaf = node;
+                node = sp > 0 ? stack[--sp] : kNodeDone;
+            }
+            if (!__any_sync(__activemask(), leaf == 0)) break;
+        }
+        // the parked leaf, then a leaf met right after it
+        bool stop = false;
+        while (leaf != 0) {
+            int code = ~leaf;
+            int first = code >> 3, count = (code & 7) + 1;
+            for (int i = first; i < first + count; i++) {
+                const float4* tp = s.tris + 3 * (size_t)i;
+                float4 t0 = __ldg(tp), t1 = __ldg(tp + 1), t2 = __ldg(tp + 2);
+                float t, u, v;
+                if (tri_test(t0, t1, t2, o, d, tnear, tfar, t, u, v)) {
+                    int gid = __float_as_int(t0.w);
+                    if (t < best || (t == best && gid < best_gid)) {
+                        best = t; best_gid = gid;
+                        hit.t = t; hit.u = u; hit.v = v; hit.gid = gid;
+                        if (kAny) { stop = true; break; }
+                    }
+                }
+            }
+            if (stop) break;
+            if (node < 0 && node != kNodeDone) {
+                leaf = node;
+                node = sp > 0 ? stack[--sp] : kNodeDone;
+            } else {
+                leaf = 0;
+            }
+        }
+        if (stop) node = kNodeDone;
+    }
+}
+
 // Entry distance of one child of a 4-wide node, or kMissKey when the ray
 // misses its box (or the slot is empty).  Same conservative slab test as slab2.
 constexpr float kMissKey = 3.0e38f;

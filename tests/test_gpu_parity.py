@@ -293,11 +293,12 @@ def test_launch_tuning_changes_no_result(cuda):
     """The autotuner's knobs (refill threshold, block size) reschedule rays
     only: every setting bakes the same bits."""
     from relight_b200 import autotune
-    saved = autotune.get("ao"), autotune.get("indirect"), autotune.get_width()
+    saved = autotune.get("ao"), autotune.get("indirect"), autotune.get_width(), autotune.get_speculative()
     colors, fg = [], []
     try:
-        for refill, block, width in ((1, 64, 2), (13, 128, 4), (32, 256, 2), (24, 64, 4)):
+        for refill, block, width, spec in ((1, 64, 2, 0), (13, 128, 4, 0), (32, 256, 2, 1), (24, 64, 2, 1)):
             autotune.set_width(width)
+            autotune.set_speculative(spec)
             autotune.set(refill, block, "ao")
             autotune.set(refill, block, "indirect")
             rl = _relight()
@@ -312,6 +313,7 @@ def test_launch_tuning_changes_no_result(cuda):
         autotune.set(saved[0]["refill"], saved[0]["block"], "ao")
         autotune.set(saved[1]["refill"], saved[1]["block"], "indirect")
         autotune.set_width(saved[2])
+        autotune.set_speculative(saved[3])
     assert all(np.array_equal(colors[0], c) for c in colors[1:])
     # photon deposits are atomic float sums, so the final gather is compared
     # through the photonmap's tolerance

@@ -109,7 +109,10 @@ typedef struct rl_scene rl_scene;
 
 /* Scene::end -> new rt::Embree; addMesh...; rtcCommit (scene/Scene.cpp:122-142,
    rt/Embree.cpp:49-58): upload the geometry and build the BVH on the device.
-   `builder`: 0 = binned SAH (host), 1 = LBVH (device). */
+   `builder`: 0 = binned SAH on the host (the better tree: the bake default),
+   1 = LBVH on the device (Karras 2012; the fast build for many or changing
+   scenes).  Hits do not depend on the builder (closest hit, ties to the
+   smaller triangle id). */
 int rl_scene_create(const rl_scene_desc* desc, int builder, void* stream, rl_scene** out);
 int rl_scene_destroy(rl_scene* scene);
 /* BVH statistics: node count, leaf count, max depth, SAH cost. */

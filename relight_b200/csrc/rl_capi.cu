@@ -25,6 +25,7 @@
 #include "../../include/relight_b200.h"
 #include "rl_bvh.h"
 #include "rl_device.cuh"
+#include "rl_lbvh.h"
 
 using namespace rl;
 
@@ -171,13 +172,18 @@ extern "C" int rl_scene_create(const rl_scene_desc* d, int builder, void* stream
         return fail(RL_INVALID_CALL, "rl_scene_create: missing geometry arrays");
     if (d->nmeshes > 0 && d->mesh_first_tri[d->nmeshes] != d->ntris)
         return fail(RL_INVALID_CALL, "mesh_first_tri[nmeshes] must equal ntris");
-    if (builder != 0) return fail(RL_NOT_IMPLEMENTED, "only the binned-SAH builder (0) is available");
+    if (builder != 0 && builder != 1) return fail(RL_INVALID_CALL, "builder must be 0 (SAH) or 1 (LBVH)");
     cudaStream_t st = S(stream);
     rl_scene* s = new (std::nothrow) rl_scene;
     if (!s) return fail(RL_OUT_OF_MEMORY, "host allocation failed");
     BvhBuild b;
     const char* err = "";
-    if (!build_bvh_sah(d->pos, d->nverts, d->tris, d->ntris, b, &err)) {
+    for (int t = 0; t < 3 * d->ntris; t++)
+        if (d->tris[t] < 0 || d->tris[t] >= d->nverts) {
+            delete s;
+            return fail(RL_INVALID_CALL, "triangle vertex index out of range");
+        }
+    if (builder == 0 && !build_bvh_sah(d->pos, d->nverts, d->tris, d->ntris, b, &err)) {
         delete s;
         return fail(RL_INVALID_CALL, "BVH build: %s", err);
     }
@@ -224,9 +230,11 @@ extern "C" int rl_scene_create(const rl_scene_desc* d, int builder, void* stream
     long long* tex_off = nullptr;
     unsigned char* tex_px = nullptr;
     float4* nodes4 = nullptr;
-    up(&nodes, (const float4*)b.nodes.data(), b.nodes.size() / 4);
-    up(&nodes4, (const float4*)b.nodes4.data(), b.nodes4.size() / 4);
-    up(&tris, (const float4*)b.tris.data(), b.tris.size() / 4);
+    if (builder == 0) {
+        up(&nodes, (const float4*)b.nodes.data(), b.nodes.size() / 4);
+        up(&nodes4, (const float4*)b.nodes4.data(), b.nodes4.size() / 4);
+        up(&tris, (const float4*)b.tris.data(), b.tris.size() / 4);
+    }
     up(&dvidx, vidx.data(), vidx.size());
     up(&pos, d->pos, 3 * (size_t)d->nverts);
     up(&nrm, d->nrm ? d->nrm : zeros3.data(), 3 * (size_t)d->nverts);
@@ -245,6 +253,22 @@ extern "C" int rl_scene_create(const rl_scene_desc* d, int builder, void* stream
             bytes = std::max(bytes, (size_t)d->tex_offset[t] + (size_t)d->tex_dims[3 * t] * d->tex_dims[3 * t + 1] *
                                         d->tex_dims[3 * t + 2]);
         up(&tex_px, d->tex_pixels, bytes);
+    }
+    if (!rc && builder == 1 && d->ntris > 0) {
+        int64_t nn = 0;
+        int depth = 0;
+        const char* lerr = "";
+        if (!build_lbvh_device(pos, dvidx, d->ntris, st, &nodes, &tris, &nn, &depth, &lerr)) {
+            rc = fail(RL_CUDA_ERROR, "LBVH build: %s", lerr);
+        } else {
+            s->owned.push_back(nodes);
+            s->owned.push_back(tris);
+            s->nnodes = nn;
+            s->leaves = d->ntris;
+            s->depth = depth;
+            s->sah = 0.0;
+            if (depth >= kStackSize - 1) rc = fail(RL_NOT_IMPLEMENTED, "LBVH depth %d exceeds the traversal stack", depth);
+        }
     }
     if (!rc) {
         cudaError_t e = cudaMalloc(&s->d_status, sizeof(int));
@@ -762,7 +786,8 @@ extern "C" int rl_bake_ao(const rl_scene* s, rl_map* lm, int samples, float frac
     if (count == 0) return RL_OK;
     uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
     int bs = g_tune[RL_TUNE_AO_BLOCK];
-    auto kern = g_tune[RL_TUNE_BVH_WIDTH] == 4 ? k_ao<4> : (g_tune[RL_TUNE_SPECULATIVE] ? k_ao<3> : k_ao<2>);
+    bool wide = g_tune[RL_TUNE_BVH_WIDTH] == 4 && s->dev.nodes4 != nullptr;
+    auto kern = wide ? k_ao<4> : (g_tune[RL_TUNE_SPECULATIVE] ? k_ao<3> : k_ao<2>);
     kern<<<blocks_for(count, bs), bs, 0, S(stream)>>>(s->dev, lm->dev, samples, fraction, maxd, exponent, key, it,
                                                       count, g_tune[RL_TUNE_AO_REFILL], s->d_status);
     CK_LAUNCH("k_ao");
@@ -1066,8 +1091,8 @@ extern "C" int rl_bake_indirect(const rl_scene* s, rl_map* lm, rl_map* const* ma
     V3 ambv = {ambient ? ambient[0] : 0.f, ambient ? ambient[1] : 0.f, ambient ? ambient[2] : 0.f};
     uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
     int bs = g_tune[RL_TUNE_FG_BLOCK];
-    auto kern = g_tune[RL_TUNE_BVH_WIDTH] == 4 ? k_indirect<4>
-                                                : (g_tune[RL_TUNE_SPECULATIVE] ? k_indirect<3> : k_indirect<2>);
+    bool wide = g_tune[RL_TUNE_BVH_WIDTH] == 4 && s->dev.nodes4 != nullptr;
+    auto kern = wide ? k_indirect<4> : (g_tune[RL_TUNE_SPECULATIVE] ? k_indirect<3> : k_indirect<2>);
     kern<<<blocks_for(count, bs), bs, 0, st>>>(s->dev, lm->dev, G, samples, maxd, skyv, ambv, key, it, count,
                                               g_tune[RL_TUNE_FG_REFILL], s->d_status);
     CK_LAUNCH("k_indirect");

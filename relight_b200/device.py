@@ -136,10 +136,11 @@ def _map_array(maps):
 class Relight:
     """relight::Relight (Relight.h:155-189)."""
 
-    def __init__(self, stream=None, seed: int = 0x5EED):
+    def __init__(self, stream=None, seed: int = 0x5EED, builder: int = 0):
         self.stream = stream
         self._seed = seed
         self._calls = 0
+        self.builder = builder  # 0: binned SAH on the host, 1: LBVH on the device
 
     @staticmethod
     def create(stream=None):
@@ -168,7 +169,7 @@ class Relight:
         if scene.flat is None:
             raise RuntimeError("Scene::end has not been called")
         if scene._device is None:
-            ds = DeviceScene(scene.flat, self.stream)
+            ds = DeviceScene(scene.flat, self.stream, self.builder)
             for maps in (scene.flat.lightmaps, scene.flat.photonmaps):
                 for m in maps:
                     if m._device is None:

@@ -26,9 +26,9 @@ def _dev(a, torch):
     return torch.from_numpy(np.ascontiguousarray(a)).cuda()
 
 
-def _relight():
+def _relight(builder=0):
     from relight_b200.device import Relight
-    return Relight()
+    return Relight(builder=builder)
 
 
 def _lumels(m):
@@ -42,8 +42,9 @@ def _segments(rng, lo, hi, n):
     return np.concatenate([a, b], 1).astype(np.float32)
 
 
+@pytest.mark.parametrize("builder", [0, 1])
 @pytest.mark.parametrize("which", ["room", "terrain"])
-def test_trace_segments_match_oracle(cuda, which):
+def test_trace_segments_match_oracle(cuda, which, builder):
     import torch
     from relight_b200 import _abi
     if which == "room":
@@ -53,8 +54,9 @@ def test_trace_segments_match_oracle(cuda, which):
         w = scenes.terrain_scene(verts=48, n_boxes=60, size=128, tiles=2)
         scene = w.scene
     flat = scene.flat
-    rl = _relight()
+    rl = _relight(builder)
     ds = rl.device_scene(scene)
+    assert ds.bvh_stats()["depth"] > 4
     orc = Oracle(flat).bind_scene(scene)
     rng = np.random.default_rng(11)
     seg = _segments(rng, flat.bounds_lo - 1, flat.bounds_hi + 1, 20000)
@@ -402,3 +404,20 @@ def test_face_iterator_bakes_match_oracle(cuda):
     gl = _lumels(w.lightmap)
     assert (lm.color.sum(1) > 0).sum() > 500
     assert np.array_equal(gl["color"], lm.color)
+
+
+def test_device_lbvh_bakes_what_the_sah_tree_bakes(cuda):
+    """The device LBVH and the host SAH tree give bit-identical bakes (hits do
+    not depend on the tree), on the full terrain's geometry."""
+    colors = []
+    for builder in (0, 1):
+        w = scenes.terrain_scene(size=256, fg_samples=8, passes=1)
+        rl = _relight(builder)
+        rl.bake_direct_light(w.scene, w.meshes[0], None)
+        rl.bake_ambient_occlusion(w.scene, w.meshes[0], None, scenes.AmbientOcclusionSettings(8, 0.8, 2.0, 1.0),
+                                  seed=2)
+        colors.append(_lumels(w.lightmap)["color"])
+        stats = w.scene._device.bvh_stats()
+        assert stats["nodes"] > 100000 and stats["depth"] < 63
+    assert (colors[0].sum(1) > 0).sum() > 10000
+    assert np.array_equal(colors[0], colors[1])

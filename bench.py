@@ -335,6 +335,83 @@ def reference_arm(args, rank, world):
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+BATCH_METRIC = "lightmaps/s (uneven bake jobs: direct + AO 64 spp + final gather 128 spp)"
+
+
+def batch_arm(args):
+    """Uneven-size batching on one GPU: scenes of log-uniform 1k-500k
+    triangles, jobs with log-uniform 32^2-1024^2 lightmaps, each baked with
+    direct light, AO and final gather.  BVHs and gathered photonmaps are
+    resident; a step clears every job's lightmap colours and bakes all jobs,
+    (a) as one captured graph of the batch kernels, (b) as the plain per-job
+    loop of single-job calls.  Both arms are checked for identical bits."""
+    import torch
+    from relight_b200 import autotune, batch, scenes
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.Stream(dev)
+    sh = stream.cuda_stream
+    n_jobs, n_scenes = (64, 8) if SMALL else (512, 32)
+    t0 = time.perf_counter()
+    wl = scenes.batch_workload(n_jobs=n_jobs, n_scenes=n_scenes)
+    t_scenes = time.perf_counter() - t0
+    with torch.cuda.stream(stream):
+        t0 = time.perf_counter()
+        res = batch.make_resident(wl, stream=sh)
+        stream.synchronize()
+        t_resident = time.perf_counter() - t0
+        valid = sum(m.valid_count() for m in res.lightmaps)
+        b = batch.Batch(res.jobs)
+        b.capture(sh)
+        ev = lambda: torch.cuda.Event(enable_timing=True)
+        flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+        def timed(fn, steps, warmup):
+            for _ in range(warmup):
+                res.clear(stream=sh)
+                fn()
+            stream.synchronize()
+            ms = []
+            for _ in range(steps):
+                flush.zero_()
+                res.clear(stream=sh)
+                e0, e1 = ev(), ev()
+                e0.record(stream)
+                fn()
+                e1.record(stream)
+                stream.synchronize()
+                ms.append(e0.elapsed_time(e1))
+            return ms
+
+        with ClockSampler(0) as clocks:
+            batch_ms = timed(lambda: b.replay(sh), args.steps, args.warmup)
+        sample = list(range(0, len(res.lightmaps), max(1, len(res.lightmaps) // 16)))
+        got = [res.lightmaps[q].download(sh, fields=("color",))["color"] for q in sample]
+        loop_ms = timed(lambda: batch.run_per_job(res.jobs, sh), max(1, args.steps // 2), 1)
+        want = [res.lightmaps[q].download(sh, fields=("color",))["color"] for q in sample]
+    identical = all(np.array_equal(a.view(np.uint32), c.view(np.uint32)) for a, c in zip(got, want))
+    bm = statistics.mean(batch_ms)
+    lm_ = statistics.mean(loop_ms)
+    nl = [len(sc.scene.flat.lights) for sc in wl.scenes]
+    rays = sum(res.lightmaps[q].valid_count() * (nl[wl.jobs[q].scene] + wl.ao.samples + wl.scenes[0].settings.final_gather_samples)
+               for q in range(len(wl.jobs)))
+    return {
+        "metric": BATCH_METRIC, "value": n_jobs / (bm / 1e3), "unit": "lightmaps/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": bm, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded heightfield + boxes)",
+        "config": {"workload": f"{n_jobs} jobs over {n_scenes} scenes (log-uniform 1k-500k tris), lightmaps "
+                               f"log-uniform 32^2-1024^2, direct + AO 64 + FG 128 per job",
+                   "jobs": n_jobs, "scenes": n_scenes, "triangles": wl.triangles, "valid_texels": valid,
+                   "texels": res.texels, "l2": "flushed between steps (256 MiB write)",
+                   "tuning": {"fg": autotune.get("indirect"), "ao": autotune.get("ao")}},
+        "texels_per_s": valid / (bm / 1e3), "grays_per_s": rays / (bm / 1e3) / 1e9,
+        "per_job_loop": {"value": n_jobs / (lm_ / 1e3), "ms_per_step": lm_, "launches_per_step": len(res.jobs)},
+        "batch_over_loop": lm_ / bm, "identical_to_loop": identical,
+        "gpu_launches": 3 * args.steps, "clocks": clocks.summary(),
+        "setup_s": {"scenes_host": t_scenes, "resident": t_resident},
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -343,9 +420,14 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--small", action="store_true", help="512^2 / 64 spp / 2 passes case for ncu captures")
+    ap.add_argument("--workload", default="terrain", choices=["terrain", "batch"],
+                    help="terrain: the photon + final-gather bake (default); batch: uneven-size batching")
     args = ap.parse_args()
     global SMALL
     SMALL = args.small
+    if args.workload == "batch":
+        print(json.dumps(batch_arm(args)), flush=True)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

@@ -225,6 +225,55 @@ int rl_bake_indirect(const rl_scene* scene, rl_map* lightmap, rl_map* const* pho
                      float max_distance, const float sky[3], const float ambient[3], uint64_t seed,
                      const rl_iterator* iterator, void* stream);
 
+/* --------------------------------------------------------------- batches */
+
+/* Many bake jobs — any scenes, lightmaps, passes — in one persistent launch
+   (no counterpart in the reference, whose Worker/Job fan-out,
+   Worker.cpp:43-83, runs jobs one after another per thread).  Each job is a
+   single-job bake call (rl_bake_direct / rl_bake_ao / rl_bake_indirect)
+   restricted to the slice [begin, end) of its iterator's visits (end < 0:
+   all), with the same Philox keys, so a batch bakes bit-identical lumels.
+   Passes apply in the order direct light, AO, final gather (as a bake applies
+   them to one lightmap); two jobs of one pass may share a lightmap only over
+   provably disjoint lumels (different face-iterator meshes, lumel iterators
+   of one step with different residues, or disjoint slices of one iterator),
+   else rl_batch_create fails with RL_INVALID_CALL. */
+typedef struct {
+    int32_t kind;                     /* 0 direct light, 1 ambient occlusion, 2 final gather */
+    const rl_scene* scene;
+    rl_map* lightmap;
+    rl_map* const* photonmaps;        /* final gather: maps by photonmap slot */
+    int32_t nmaps;
+    const rl_light* lights;           /* direct light */
+    int32_t nlights;
+    const float* light_vertices;
+    int32_t nlight_vertices;
+    int32_t samples;                  /* AO / final gather */
+    float occluded_fraction;          /* AO */
+    float max_distance;               /* AO / final gather */
+    float exponent;                   /* AO */
+    float sky[3], ambient[3];         /* final gather */
+    uint64_t seed;                    /* AO / final gather */
+    rl_iterator iterator;
+    int64_t begin, end;
+} rl_batch_job;
+
+typedef struct rl_batch rl_batch;
+
+/* Upload a job table (host arrays are read before the call returns). */
+int rl_batch_create(const rl_batch_job* jobs, int njobs, rl_batch** out);
+/* One persistent launch per pass kind over every job's lumels (warps take
+   32 lumels at a time from a shared counter).  Launches of one batch must
+   not overlap on the GPU (they share the counters). */
+int rl_batch_launch(rl_batch* batch, void* stream);
+/* Capture the launch into a CUDA graph on `stream` (non-default), then
+   replay it; the batch reads its lightmaps' current contents at each replay. */
+int rl_batch_capture(rl_batch* batch, void* stream);
+int rl_batch_replay(rl_batch* batch, void* stream);
+/* Number of lumel work items (summed over jobs). */
+int rl_batch_work_items(const rl_batch* batch, int64_t* items);
+int rl_batch_destroy(rl_batch* batch);
+
 /* ------------------------------------------------------------- radiosity */
 
 /* RadiosityBuilder::computeFormFactors + distanceFormFactor +

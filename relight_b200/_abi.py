@@ -40,6 +40,16 @@ class Iterator(C.Structure):
     _fields_ = [("kind", C.c_int32), ("first", C.c_int32), ("step", C.c_int32), ("mesh", C.c_int32)]
 
 
+class BatchJob(C.Structure):
+    """rl_batch_job."""
+    _fields_ = [("kind", C.c_int32), ("scene", C.c_void_p), ("lightmap", C.c_void_p), ("photonmaps", C.c_void_p),
+                ("nmaps", C.c_int32), ("lights", C.c_void_p), ("nlights", C.c_int32),
+                ("light_vertices", C.c_void_p), ("nlight_vertices", C.c_int32), ("samples", C.c_int32),
+                ("occluded_fraction", C.c_float), ("max_distance", C.c_float), ("exponent", C.c_float),
+                ("sky", C.c_float * 3), ("ambient", C.c_float * 3), ("seed", C.c_uint64),
+                ("iterator", Iterator), ("begin", C.c_int64), ("end", C.c_int64)]
+
+
 def _ptr(a):
     """A c_void_p to `a`'s data that holds a reference to `a` (numpy's
     data_as), so the array outlives the pointer."""
@@ -112,6 +122,12 @@ SIGNATURES = {
     "rl_radiosity_solve": (_I, [_I, _P, _P, _P, _P, _P, _I, _P, _P]),
     "rl_radiosity_solve_noalloc": (_I, [_I, _P, _P, _P, _P, _P, _I, _P, _P]),
     "rl_radiosity_step": (_I, [_I, _I, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "rl_batch_create": (_I, [_P, _I, _P]),
+    "rl_batch_launch": (_I, [_P, _P]),
+    "rl_batch_capture": (_I, [_P, _P]),
+    "rl_batch_replay": (_I, [_P, _P]),
+    "rl_batch_work_items": (_I, [_P, _P]),
+    "rl_batch_destroy": (_I, [_P]),
     "rl_measure_read_bandwidth": (_I, [C.c_size_t, _I, _P]),
     "rl_tune_set": (_I, [_I, _I]),
     "rl_tune_get": (_I, [_I, _P]),
@@ -146,9 +162,14 @@ def lib():
     return _lib
 
 
+def last_error() -> str:
+    """rl_last_error: the message of this thread's last failed call."""
+    buf = C.create_string_buffer(1024)
+    lib().rl_last_error(buf, 1024)
+    return buf.value.decode(errors="replace")
+
+
 def check(rc):
     if rc != RL_OK:
-        buf = C.create_string_buffer(1024)
-        lib().rl_last_error(buf, 1024)
-        raise RelightCudaError(rc, buf.value.decode(errors="replace"))
+        raise RelightCudaError(rc, last_error())
     return rc

@@ -14,7 +14,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cstdarg>
+#include <map>
 #include <mutex>
 #include <cstdio>
 #include <cstring>
@@ -662,13 +664,8 @@ __device__ float influence_from_point(const DevScene& s, V3 lpos, V3 lnrm, V3 po
     return inf * att * cut;
 }
 
-// DirectLight::bakeLumel (baker/DirectLight.cpp:46-98), one thread per lumel.
-__global__ void k_direct(DevScene s, DevMap m, const __grid_constant__ LightTable T, Iter it, long long count,
-                         int* status) {
-    long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (k >= count) return;
-    long long i;
-    if (!iter_lumel(m, it, k, i)) return;
+// DirectLight::bakeLumel (baker/DirectLight.cpp:46-98) for lumel i.
+__device__ void direct_lumel(const DevScene& s, const DevMap& m, const LightTable& T, long long i, int* status) {
     V3 pos = ld3(m.position + 3 * i), nrm = ld3(m.normal + 3 * i);
     float* col = m.color + 3 * i;
     float cr = col[0], cg = col[1], cb = col[2];
@@ -692,6 +689,16 @@ __global__ void k_direct(DevScene s, DevMap m, const __grid_constant__ LightTabl
         cr = cr + infl.x; cg = cg + infl.y; cb = cb + infl.z;
     }
     col[0] = cr; col[1] = cg; col[2] = cb;
+}
+
+// One thread per visited lumel.
+__global__ void k_direct(DevScene s, DevMap m, const __grid_constant__ LightTable T, Iter it, long long count,
+                         int* status) {
+    long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    long long i;
+    if (!iter_lumel(m, it, k, i)) return;
+    direct_lumel(s, m, T, i, status);
 }
 
 // Validate an rl_iterator (NULL = LumelBakeIterator(0, 1)) and size the
@@ -1469,6 +1476,359 @@ extern "C" int rl_radiosity_solve(int n, const int64_t* d_row_ptr, const int32_t
         std::swap(src, dst);
     }
     if (src != d_B) CK(cudaMemcpyAsync(d_B, src, 12 * (size_t)n, cudaMemcpyDeviceToDevice, st));
+    return RL_OK;
+}
+
+// --------------------------------------------------------------- batches
+
+// One job of a batch on the device: its scene and lightmap views, pass and
+// parameters, and the slice [k_begin, k_begin + count) of its iterator.
+struct DevJob {
+    DevScene s;
+    DevMap m;
+    const LightTable* lights;
+    const GatherMaps* maps;
+    int* status;
+    Iter it;
+    long long k_begin, count;
+    int kind, samples;
+    float fraction, maxd, exponent;
+    V3 sky, amb;
+    uint2 key;
+};
+
+// The job table is split by pass: one persistent kernel per pass kind takes
+// the items of every job of that kind, so each kernel keeps only its own ray
+// loop's registers.
+struct rl_batch {
+    std::vector<DevJob> jobs[3];
+    std::vector<long long> prefix[3];  // work-item offset of each job (multiples of 32)
+    DevJob* d_jobs[3] = {nullptr, nullptr, nullptr};
+    long long* d_prefix[3] = {nullptr, nullptr, nullptr};
+    unsigned long long* d_counter = nullptr;  // one per kind
+    std::vector<void*> owned;
+    long long items = 0, total[3] = {0, 0, 0};
+    int grid[3] = {0, 0, 0}, block[3] = {128, 128, 128};
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    ~rl_batch() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        for (int k = 0; k < 3; k++) {
+            cudaFree(d_jobs[k]);
+            cudaFree(d_prefix[k]);
+        }
+        cudaFree(d_counter);
+        for (void* p : owned) cudaFree(p);
+    }
+};
+
+// Largest j with prefix[j] <= w.
+__device__ __forceinline__ int find_job(const long long* prefix, int njobs, long long w) {
+    int lo = 0, hi = njobs - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (__ldg(prefix + mid) <= w) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Persistent batch kernel for one pass kind (0 direct, 1 AO, 2 final
+// gather).  Warps take 32 work items at a time from one counter across all
+// the batch's jobs of that kind; every job's items are padded to a multiple
+// of 32, so a warp's chunk lies in one job and the scene and the ray loop's
+// warp votes are warp-uniform.  Each lane bakes one lumel with the same code
+// and Philox keys as the single-job calls, so the lumels come out
+// bit-identical to rl_bake_direct / rl_bake_ao / rl_bake_indirect.
+template <int kKind>
+__global__ void __launch_bounds__(kKind == 0 ? 128 : 256) k_batch(const DevJob* __restrict__ jobs, const long long* __restrict__ prefix,
+                                               int njobs, long long total, unsigned long long* counter,
+                                               int refill) {
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        unsigned long long base = 0;
+        int j = 0;
+        if (lane == 0) {
+            base = atomicAdd(counter, 32ull);
+            if (base < (unsigned long long)total) j = find_job(prefix, njobs, (long long)base);
+        }
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= (unsigned long long)total) break;
+        j = __shfl_sync(0xffffffffu, j, 0);
+        const DevJob& J = jobs[j];
+        const long long r = (long long)base - __ldg(prefix + j) + lane;
+        long long i = 0;
+        const bool valid = r < J.count && iter_lumel(J.m, J.it, J.k_begin + r, i);
+        if (kKind == 0) {
+            if (valid) direct_lumel(J.s, J.m, *J.lights, i, J.status);
+        } else if (kKind == 1) {
+            const DevScene s = J.s;
+            AoGen g;
+            g.pos = valid ? ld3(J.m.position + 3 * i) : mk3(0.f, 0.f, 0.f);
+            g.nrm = valid ? ld3(J.m.normal + 3 * i) : mk3(0.f, 0.f, 1.f);
+            g.key = J.key;
+            g.item = (uint32_t)i;
+            g.j = 0;
+            g.samples = valid ? J.samples : 0;
+            g.occluded = 0;
+            g.maxd = J.maxd;
+            __syncwarp();
+            ray_loop<true>(s, g, refill, J.status);
+            if (valid) {
+                float value = 1.0f - g.occluded / (J.samples * J.fraction);
+                if (fabsf(1.0f - J.exponent) > 0.01f) value = powf(value, J.exponent);
+                float* col = J.m.color + 3 * i;
+                col[0] = col[0] * value; col[1] = col[1] * value; col[2] = col[2] * value;
+            }
+        } else {
+            const DevScene s = J.s;
+            FgGen g;
+            g.s = &J.s;
+            g.G = J.maps;
+            g.pos = valid ? ld3(J.m.position + 3 * i) : mk3(0.f, 0.f, 0.f);
+            g.nrm = valid ? ld3(J.m.normal + 3 * i) : mk3(0.f, 0.f, 1.f);
+            g.sky = J.sky;
+            g.amb = J.amb;
+            g.key = J.key;
+            g.item = (uint32_t)i;
+            g.j = 0;
+            g.samples = valid ? J.samples : 0;
+            g.maxd = J.maxd;
+            g.gr = g.gg = g.gb = 0.f;
+            g.influence = 0.f;
+            g.dir = mk3(0.f, 0.f, 0.f);
+            __syncwarp();
+            ray_loop<false>(s, g, refill, J.status);
+            if (valid) {
+                float ns = (float)J.samples;
+                float* col = J.m.color + 3 * i;
+                col[0] = col[0] + g.gr / ns; col[1] = col[1] + g.gg / ns; col[2] = col[2] + g.gb / ns;
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// Whether two jobs of one pass kind may visit a common lumel (a race: both
+// read-modify-write its colour).  Disjoint for sure: different lightmaps;
+// face iterators over different meshes; lumel iterators of one step with
+// different residues; or one iterator with disjoint [begin, end) slices.
+static bool jobs_may_overlap(const rl_batch_job& a, const rl_batch_job& b) {
+    if (a.lightmap != b.lightmap) return false;
+    const rl_iterator &x = a.iterator, &y = b.iterator;
+    if (x.kind == 1 && y.kind == 1 && x.mesh != y.mesh) return false;
+    if (x.kind == 0 && y.kind == 0 && x.step == y.step && x.step > 0 && x.first % x.step != y.first % y.step)
+        return false;
+    if (x.kind == y.kind && x.first == y.first && x.step == y.step && (x.kind == 0 || x.mesh == y.mesh)) {
+        long long ab = a.begin < 0 ? 0 : a.begin, bb = b.begin < 0 ? 0 : b.begin;
+        long long ae = a.end < 0 ? LLONG_MAX : a.end, be = b.end < 0 ? LLONG_MAX : b.end;
+        return ab < be && bb < ae;
+    }
+    return true;
+}
+
+// Relative cost of one work item, for ordering the job table: the most
+// expensive items are handed out first so the launch ends on cheap ones.
+static double job_item_cost(const rl_batch_job& J) {
+    if (J.kind == 2) return 2.0 * J.samples;
+    if (J.kind == 1) return (double)J.samples;
+    double c = 0;
+    for (int l = 0; l < J.nlights; l++) c += J.lights[l].vertex_count > 0 ? J.lights[l].vertex_count : 1;
+    return c;
+}
+
+extern "C" int rl_batch_create(const rl_batch_job* jobs, int njobs, rl_batch** out) {
+    if (!out || njobs < 0 || (njobs > 0 && !jobs)) return fail(RL_INVALID_CALL, "rl_batch_create: bad arguments");
+    *out = nullptr;
+    rl_batch* b = new (std::nothrow) rl_batch;
+    if (!b) return fail(RL_OUT_OF_MEMORY, "host allocation failed");
+    std::vector<int> order(njobs);
+    for (int q = 0; q < njobs; q++) order[q] = q;
+    for (int q = 0; q < njobs; q++)
+        if (jobs[q].kind == 0 && jobs[q].nlights > 0 && !jobs[q].lights) {
+            delete b;
+            return fail(RL_INVALID_CALL, "batch job %d: null light array", q);
+        }
+    {
+        std::map<std::pair<int, const rl_map*>, std::vector<int>> by_map;
+        for (int q = 0; q < njobs; q++) by_map[{jobs[q].kind, jobs[q].lightmap}].push_back(q);
+        for (auto& kv : by_map)
+            for (size_t x = 0; x < kv.second.size(); x++)
+                for (size_t y = x + 1; y < kv.second.size(); y++)
+                    if (jobs_may_overlap(jobs[kv.second[x]], jobs[kv.second[y]])) {
+                        delete b;
+                        return fail(RL_INVALID_CALL, "batch jobs %d and %d: one pass over shared lumels of one lightmap",
+                                    kv.second[x], kv.second[y]);
+                    }
+    }
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int x, int y) { return job_item_cost(jobs[x]) > job_item_cost(jobs[y]); });
+    std::map<const rl_light*, LightTable*> light_tables;
+    int rc = RL_OK;
+    for (int q : order) {
+        const rl_batch_job& J = jobs[q];
+        if (!J.scene || !J.lightmap || J.kind < 0 || J.kind > 2) {
+            rc = fail(RL_INVALID_CALL, "batch job %d: bad scene, lightmap or kind", q);
+            break;
+        }
+        if ((J.kind == 1 || J.kind == 2) && J.samples <= 0) {
+            rc = fail(RL_INVALID_CALL, "batch job %d: samples must be positive", q);
+            break;
+        }
+        DevJob d;
+        memset(&d, 0, sizeof d);
+        d.s = J.scene->dev;
+        d.m = J.lightmap->dev;
+        d.status = J.scene->d_status;
+        d.kind = J.kind;
+        d.samples = J.samples;
+        d.fraction = J.occluded_fraction;
+        d.maxd = J.max_distance;
+        d.exponent = J.exponent;
+        d.sky = V3{J.sky[0], J.sky[1], J.sky[2]};
+        d.amb = V3{J.ambient[0], J.ambient[1], J.ambient[2]};
+        d.key = make_uint2((uint32_t)J.seed, (uint32_t)(J.seed >> 32));
+        long long n = (long long)J.lightmap->dev.width * J.lightmap->dev.height, count = 0;
+        rc = make_iter(&J.iterator, J.scene, n, d.it, count);
+        if (rc) break;
+        long long b0 = J.begin < 0 ? 0 : (J.begin < count ? J.begin : count);
+        long long e0 = J.end < 0 || J.end > count ? count : J.end;
+        if (e0 < b0) e0 = b0;
+        d.k_begin = b0;
+        d.count = e0 - b0;
+        if (J.kind == 0 && J.nlights == 0) d.count = 0;  // rl_bake_direct with no lights bakes nothing
+        if (J.kind == 0 && d.count > 0) {
+            auto it = light_tables.find(J.lights);
+            if (it == light_tables.end()) {
+                static thread_local LightTable T;
+                rc = make_light_table(J.lights, J.nlights, J.light_vertices, J.nlight_vertices, T);
+                if (rc) break;
+                LightTable* dl = nullptr;
+                cudaError_t e = cudaMalloc(&dl, sizeof(LightTable));
+                if (e == cudaSuccess) b->owned.push_back(dl);
+                if (e == cudaSuccess) e = cudaMemcpy(dl, &T, sizeof(LightTable), cudaMemcpyHostToDevice);
+                if (e != cudaSuccess) { rc = fail(RL_CUDA_ERROR, "light table: %s", cudaGetErrorString(e)); break; }
+                it = light_tables.emplace(J.lights, dl).first;
+            }
+            d.lights = it->second;
+        }
+        if (J.kind == 2 && d.count > 0) {
+            if (J.nmaps < 0 || J.nmaps > kMaxPhotonmaps || (J.nmaps > 0 && !J.photonmaps)) {
+                rc = fail(RL_INVALID_CALL, "batch job %d: bad photonmaps", q);
+                break;
+            }
+            static thread_local GatherMaps G;
+            memset(&G, 0, sizeof G);
+            G.nmaps = J.nmaps;
+            for (int k = 0; k < J.nmaps; k++) {
+                if (!J.photonmaps[k]) { rc = fail(RL_INVALID_CALL, "batch job %d: null photonmap", q); break; }
+                G.maps[k] = J.photonmaps[k]->dev;
+            }
+            if (rc) break;
+            GatherMaps* dg = nullptr;
+            cudaError_t e = cudaMalloc(&dg, sizeof(GatherMaps));
+            if (e == cudaSuccess) b->owned.push_back(dg);
+            if (e == cudaSuccess) e = cudaMemcpy(dg, &G, sizeof(GatherMaps), cudaMemcpyHostToDevice);
+            if (e != cudaSuccess) { rc = fail(RL_CUDA_ERROR, "gather maps: %s", cudaGetErrorString(e)); break; }
+            d.maps = dg;
+        }
+        if (d.count == 0) continue;
+        b->jobs[J.kind].push_back(d);
+        b->prefix[J.kind].push_back(b->total[J.kind]);
+        b->items += d.count;
+        b->total[J.kind] += (d.count + 31) / 32 * 32;
+    }
+    if (!rc) {
+        int dev = 0, sms = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        const void* kern[3] = {(const void*)k_batch<0>, (const void*)k_batch<1>, (const void*)k_batch<2>};
+        b->block[0] = 128;
+        b->block[1] = g_tune[RL_TUNE_AO_BLOCK];
+        b->block[2] = g_tune[RL_TUNE_FG_BLOCK];
+        for (int k = 0; k < 3 && e == cudaSuccess; k++) {
+            int per = 0;
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern[k], b->block[k], 0);
+            b->grid[k] = sms * std::max(per, 1);
+            size_t nj = b->jobs[k].size();
+            if (e == cudaSuccess && nj) e = cudaMalloc(&b->d_jobs[k], sizeof(DevJob) * nj);
+            if (e == cudaSuccess && nj) e = cudaMalloc(&b->d_prefix[k], sizeof(long long) * nj);
+            if (e == cudaSuccess && nj)
+                e = cudaMemcpy(b->d_jobs[k], b->jobs[k].data(), sizeof(DevJob) * nj, cudaMemcpyHostToDevice);
+            if (e == cudaSuccess && nj)
+                e = cudaMemcpy(b->d_prefix[k], b->prefix[k].data(), sizeof(long long) * nj, cudaMemcpyHostToDevice);
+        }
+        if (e == cudaSuccess) e = cudaMalloc(&b->d_counter, 3 * sizeof(unsigned long long));
+        if (e != cudaSuccess) rc = fail(RL_CUDA_ERROR, "batch upload: %s", cudaGetErrorString(e));
+    }
+    if (rc) {
+        delete b;
+        return rc;
+    }
+    *out = b;
+    return RL_OK;
+}
+
+// The kinds run in sequence on the stream in the order a bake applies them
+// to one lightmap (direct light adds, AO scales, final gather adds: the
+// demo's Bake job, src/demo/Lightmapping.cpp:270-279, plus AO between), so a
+// lightmap baked by several passes of one batch gets the sequential result.
+static int batch_enqueue(rl_batch* b, cudaStream_t st) {
+    if (b->items == 0) return RL_OK;
+    CK(cudaMemsetAsync(b->d_counter, 0, 3 * sizeof(unsigned long long), st));
+    const int refill[3] = {0, g_tune[RL_TUNE_AO_REFILL], g_tune[RL_TUNE_FG_REFILL]};
+    for (int k = 0; k < 3; k++) {
+        if (b->total[k] == 0) continue;
+        long long warps = b->total[k] / 32;
+        int wpb = b->block[k] / 32;
+        int grid = (int)std::min<long long>(b->grid[k], (warps + wpb - 1) / wpb);
+        auto kern = k == 0 ? k_batch<0> : k == 1 ? k_batch<1> : k_batch<2>;
+        kern<<<grid, b->block[k], 0, st>>>(b->d_jobs[k], b->d_prefix[k], (int)b->jobs[k].size(), b->total[k],
+                                           b->d_counter + k, refill[k]);
+        CK_LAUNCH("k_batch");
+    }
+    return RL_OK;
+}
+
+extern "C" int rl_batch_launch(rl_batch* b, void* stream) {
+    if (!b) return fail(RL_INVALID_CALL, "null batch");
+    return batch_enqueue(b, S(stream));
+}
+
+extern "C" int rl_batch_capture(rl_batch* b, void* stream) {
+    if (!b) return fail(RL_INVALID_CALL, "null batch");
+    if (!stream) return fail(RL_INVALID_CALL, "rl_batch_capture needs a non-default stream");
+    cudaStream_t st = S(stream);
+    if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; }
+    if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
+    CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    int rc = batch_enqueue(b, st);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(st, &g);
+    if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+    if (e != cudaSuccess) return fail(RL_CUDA_ERROR, "stream capture: %s", cudaGetErrorString(e));
+    b->graph = g;
+    CK(cudaGraphInstantiate(&b->exec, g, 0));
+    return RL_OK;
+}
+
+extern "C" int rl_batch_replay(rl_batch* b, void* stream) {
+    if (!b || !b->exec) return fail(RL_INVALID_CALL, "rl_batch_replay: batch has no captured graph");
+    CK(cudaGraphLaunch(b->exec, S(stream)));
+    return RL_OK;
+}
+
+extern "C" int rl_batch_work_items(const rl_batch* b, int64_t* items) {
+    if (!b || !items) return fail(RL_INVALID_CALL, "null argument");
+    *items = b->items;
+    return RL_OK;
+}
+
+extern "C" int rl_batch_destroy(rl_batch* b) {
+    if (!b) return fail(RL_INVALID_CALL, "null batch");
+    cudaDeviceSynchronize();
+    delete b;
     return RL_OK;
 }
 

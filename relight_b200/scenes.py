@@ -9,6 +9,10 @@
                   lightmap and photonmap.  The photon + final-gather workload.
   radiosity_room  10x5x10 room whose 128x128 radiancemap texels are the
                   16,384 radiosity patches.
+  batch_workload  uneven-size batching: scenes of log-uniform triangle
+                  counts (heightfield patch + boxes, terrain_scene's recipe)
+                  and bake jobs with log-uniform lightmap sides, each job
+                  baked with direct light, AO and final gather.
 
 Every chart is an axis-aligned rectangle in the lightmap with a one-texel
 gutter, so texel rasterisation (Lightmap::initializeLumels) covers it fully.
@@ -216,7 +220,13 @@ def terrain_scene(seed: int = 2, verts: int = 256, n_boxes: int = 2000, size: in
     cols = size // cell
     ncells = cols * (rows_px // cell)
     k = 0
-    for _ in range(n_boxes):
+    per_mesh = (Mesh.MAX_INDEX + 1) // 24  # 24 vertices per box, 16-bit indices
+    for b in range(n_boxes):
+        if b > 0 and b % per_mesh == 0:
+            inst = scene.add_mesh(src)
+            lm.add_mesh(inst); pm.add_mesh(inst)
+            meshes.append(inst)
+            src = Mesh.create()
         s = rng.uniform(0.5, 2.0, 3).astype(F32)
         cx, cz = rng.uniform(2, quads - 2, 2)
         base = h[int(round(cx)), int(round(cz))] - 0.1
@@ -281,3 +291,49 @@ def radiosity_room(size: int = 128, seed: int = 3, dims=(10.0, 5.0, 10.0)) -> Ra
     rm.add_mesh(mesh)
     scene.end()
     return RadiosityWorkload(scene, mesh, rm, seed)
+
+
+# ------------------------------------------------------------------ batches
+
+@dataclass
+class BatchJobSpec:
+    scene: int          # index into BatchWorkload.scenes
+    side: int           # lightmap width = height
+    seed: int
+
+
+@dataclass
+class BatchWorkload:
+    scenes: List[TerrainWorkload]
+    triangles: List[int]
+    jobs: List[BatchJobSpec]
+    ao: AmbientOcclusionSettings
+
+
+def _log_uniform(rng, lo, hi):
+    return float(np.exp(rng.uniform(np.log(lo), np.log(hi))))
+
+
+def batch_workload(n_jobs: int = 512, n_scenes: int = 32, seed: int = 4, tris=(1_000, 500_000),
+                   sides=(32, 1024), ao_samples: int = 64, fg_samples: int = 128, photon_map: int = 256,
+                   photon_passes: int = 1) -> BatchWorkload:
+    """Scenes: a heightfield patch (about 90% of the triangles, tiled under
+    the 16-bit index limit) plus boxes (about 10%), with terrain_scene's sun
+    and 4 point lights and one `photon_map`-sided photonmap.  Jobs: a scene
+    drawn uniformly and a lightmap side log-uniform in `sides`."""
+    rng = np.random.default_rng(seed)
+    scenes, counts = [], []
+    for k in range(n_scenes):
+        t = _log_uniform(rng, *tris)
+        verts = max(8, int(round(math.sqrt(0.9 * t / 2.0))) + 1)
+        n_boxes = max(1, int(round(0.1 * t / 12.0)))
+        tiles = max(1, int(math.ceil((verts - 1) / 255.0)))
+        wl = terrain_scene(seed=seed * 1000 + k, verts=verts, n_boxes=n_boxes, size=photon_map, tiles=tiles,
+                           fg_samples=fg_samples, passes=photon_passes)
+        scenes.append(wl)
+        counts.append(int(sum(m.face_count() for m in wl.meshes)))
+    jobs = []
+    for q in range(n_jobs):
+        side = int(round(_log_uniform(rng, *sides)))
+        jobs.append(BatchJobSpec(int(rng.integers(0, n_scenes)), side, int(rng.integers(0, 2 ** 63))))
+    return BatchWorkload(scenes, counts, jobs, AmbientOcclusionSettings(ao_samples, 0.8, 2.0, 1.0))

@@ -412,6 +412,51 @@ def batch_arm(args):
     }
 
 
+SERVE_METRIC = "bake-serving p99 latency at 100 req/s (Poisson; direct + AO 64 + FG 16 spp per request)"
+
+
+def serve_arm(args):
+    """Bake serving on one GPU: 32 resident scenes (log-uniform 1k-500k
+    triangles, BVH + gathered photonmap each), requests with log-uniform
+    32^2-1024^2 lightmaps arriving as Poisson streams at 20, 50 and 100
+    requests/s, admitted by a 16 GiB HBM budget and continuously batched.
+    Latency is arrival to colours-in-host-memory on the host clock; a
+    closed-loop run (all requests queued at once) gives the saturated
+    throughput."""
+    import torch
+    from relight_b200 import batch, scenes, serve
+    torch.cuda.set_device(0)
+    n_scenes = 8 if SMALL else 32
+    n_req = 40 if SMALL else 300
+    wl = scenes.batch_workload(n_jobs=1, n_scenes=n_scenes)
+    ts = torch.cuda.Stream()
+    rs = batch.make_resident_scenes(wl, stream=ts.cuda_stream)
+    ts.synchronize()
+    budget = 16 << 30
+    srv = serve.BakeServer(rs, budget_bytes=budget, quantum=1 << 18, fg_samples=16, torch_stream=ts)
+    srv.warm()
+    srv.run(serve.make_requests(wl, 1000.0, max(args.warmup, 3) * 4, seed=99))  # warm-up
+    rates = {}
+    with ClockSampler(0) as clocks:
+        for rate in (20.0, 50.0, 100.0):
+            st = srv.run(serve.make_requests(wl, rate, n_req, seed=int(rate)), keep_results=False)
+            rates[str(int(rate))] = st.as_dict()
+        closed = serve.make_requests(wl, 1e9, n_req, seed=7)
+        sat = srv.run(closed, keep_results=False).as_dict()
+    srv.close()
+    p99 = rates["100"]["p99_ms"]
+    return {
+        "metric": SERVE_METRIC, "value": p99, "unit": "ms", "n_gpus": 1, "steps": n_req, "warmup": args.warmup,
+        "ms_per_step": rates["100"]["mean_ms"], "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded heightfield + boxes, Poisson arrivals)",
+        "config": {"workload": f"{n_req} requests per rate over {n_scenes} resident scenes, lightmaps log-uniform "
+                               f"32^2-1024^2, direct + AO 64 + FG 16 spp",
+                   "hbm_budget_bytes": budget, "resident_scene_bytes": rs.nbytes(), "quantum_lumels": 1 << 18,
+                   "latency_clock": "host (arrival to colours in pinned host memory)"},
+        "rates": rates, "saturated": sat, "clocks": clocks.summary(),
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -420,13 +465,17 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--small", action="store_true", help="512^2 / 64 spp / 2 passes case for ncu captures")
-    ap.add_argument("--workload", default="terrain", choices=["terrain", "batch"],
-                    help="terrain: the photon + final-gather bake (default); batch: uneven-size batching")
+    ap.add_argument("--workload", default="terrain", choices=["terrain", "batch", "serve"],
+                    help="terrain: the photon + final-gather bake (default); batch: uneven-size batching; "
+                         "serve: the bake-serving loop")
     args = ap.parse_args()
     global SMALL
     SMALL = args.small
     if args.workload == "batch":
         print(json.dumps(batch_arm(args)), flush=True)
+        return
+    if args.workload == "serve":
+        print(json.dumps(serve_arm(args)), flush=True)
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -142,6 +142,21 @@ typedef struct rl_map rl_map;
    0 = Lightmap, 1 = Photonmap, 2 = Radiancemap (Lightmap.h:58-184). */
 int rl_map_create(int kind, int width, int height, rl_map** out);
 int rl_map_destroy(rl_map* map);
+/* The same map as one stream-ordered block (cudaMallocAsync, initialised by
+   a kernel on `stream`), and its stream-ordered release: neither call waits
+   for the device, so a serving loop can admit and retire lightmaps while
+   other bakes run.  rl_map_bytes gives the block size of a width x height
+   map (the unit of an HBM budget).  No reference counterpart. */
+int rl_map_bytes(int width, int height, int64_t* bytes);
+/* Those blocks (and batch tables) come from the library's memory pool on
+   the current device, which keeps freed memory for reuse instead of
+   returning it at every synchronisation.  rl_pool_trim returns all but
+   `keep_bytes` of the unused memory; rl_pool_bytes reports the pool's
+   reserved and in-use bytes (either pointer may be NULL). */
+int rl_pool_trim(int64_t keep_bytes);
+int rl_pool_bytes(int64_t* reserved, int64_t* used);
+int rl_map_create_async(int kind, int width, int height, void* stream, rl_map** out);
+int rl_map_destroy_async(rl_map* map, void* stream);
 /* Lightmap::addMesh / Photonmap::addMesh -> initializeLumels
    (Lightmap.cpp:93-164, 360-373): rasterise the mesh's faces into lumels
    (last face wins).  Call once per mesh, in the reference's addMesh order. */
@@ -150,6 +165,10 @@ int rl_map_add_mesh(rl_map* map, const rl_scene* scene, int mesh, void* stream);
    toHdr(), :332-349).  Host arrays [w*h] or [w*h][3]; any may be NULL. */
 int rl_map_download(const rl_map* map, int32_t* flags, int32_t* face, float* position, float* normal, float* color,
                     int32_t* photons, float* gathered, void* stream);
+/* The baked colours ([w*h][3]) copied to `color` in stream order, without
+   waiting: the data is there once `stream` has reached this point (pinned
+   host memory for a truly asynchronous copy).  No reference counterpart. */
+int rl_map_download_async(const rl_map* map, float* color, void* stream);
 int rl_map_upload(rl_map* map, const int32_t* flags, const int32_t* face, const float* position,
                   const float* normal, const float* color, const int32_t* photons, const float* gathered,
                   void* stream);
@@ -262,6 +281,12 @@ typedef struct rl_batch rl_batch;
 
 /* Upload a job table (host arrays are read before the call returns). */
 int rl_batch_create(const rl_batch_job* jobs, int njobs, rl_batch** out);
+/* Replace the job table, asynchronously on `stream` (host arrays are read
+   before the call returns; the copy runs in stream order, after the launches
+   already enqueued there).  A captured graph stays valid: its kernels read
+   the table from a fixed device header at run time.  Update and launch or
+   replay on the same stream.  On error the previous table stays. */
+int rl_batch_update(rl_batch* batch, const rl_batch_job* jobs, int njobs, void* stream);
 /* One persistent launch per pass kind over every job's lumels (warps take
    32 lumels at a time from a shared counter).  Launches of one batch must
    not overlap on the GPU (they share the counters). */
@@ -270,7 +295,7 @@ int rl_batch_launch(rl_batch* batch, void* stream);
    replay it; the batch reads its lightmaps' current contents at each replay. */
 int rl_batch_capture(rl_batch* batch, void* stream);
 int rl_batch_replay(rl_batch* batch, void* stream);
-/* Number of lumel work items (summed over jobs). */
+/* Number of lumel work items of the current table (summed over jobs). */
 int rl_batch_work_items(const rl_batch* batch, int64_t* items);
 int rl_batch_destroy(rl_batch* batch);
 

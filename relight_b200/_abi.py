@@ -123,6 +123,13 @@ SIGNATURES = {
     "rl_radiosity_solve_noalloc": (_I, [_I, _P, _P, _P, _P, _P, _I, _P, _P]),
     "rl_radiosity_step": (_I, [_I, _I, _P, _P, _P, _P, _P, _P, _P, _P]),
     "rl_batch_create": (_I, [_P, _I, _P]),
+    "rl_batch_update": (_I, [_P, _P, _I, _P]),
+    "rl_map_bytes": (_I, [_I, _I, _P]),
+    "rl_pool_trim": (_I, [_I64]),
+    "rl_pool_bytes": (_I, [_P, _P]),
+    "rl_map_download_async": (_I, [_P, _P, _P]),
+    "rl_map_create_async": (_I, [_I, _I, _I, _P, _P]),
+    "rl_map_destroy_async": (_I, [_P, _P]),
     "rl_batch_launch": (_I, [_P, _P]),
     "rl_batch_capture": (_I, [_P, _P]),
     "rl_batch_replay": (_I, [_P, _P]),

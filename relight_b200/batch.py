@@ -69,44 +69,54 @@ class BakeJob:
         return int(sum(int(l["vertex_count"]) for l in self.lights))
 
 
+def _job_array(jobs: Sequence[BakeJob]):
+    """rl_batch_job records for `jobs` (and the ctypes objects they point into)."""
+    keep: List[object] = []
+    arr = (_abi.BatchJob * max(len(jobs), 1))()
+    for q, j in enumerate(jobs):
+        b = arr[q]
+        b.kind = j.kind
+        b.scene = j.scene.handle.value
+        b.lightmap = j.lightmap.handle.value
+        if j.photonmaps:
+            maps = _map_array(j.photonmaps)
+            keep.append(maps)
+            b.photonmaps = C.cast(maps, C.c_void_p)
+        b.nmaps = len(j.photonmaps)
+        if j.lights is not None and len(j.lights):
+            b.lights = j.lights.ctypes.data
+            b.nlights = len(j.lights)
+        if j.light_vertices is not None and len(j.light_vertices):
+            b.light_vertices = j.light_vertices.ctypes.data
+            b.nlight_vertices = j.nlight_vertices()
+        b.samples = j.samples
+        b.occluded_fraction = j.occluded_fraction
+        b.max_distance = j.max_distance
+        b.exponent = j.exponent
+        b.sky = (C.c_float * 3)(*[float(x) for x in j.sky])
+        b.ambient = (C.c_float * 3)(*[float(x) for x in j.ambient])
+        b.seed = j.seed & 0xFFFFFFFFFFFFFFFF
+        b.iterator = _abi.Iterator(*j.iterator)
+        b.begin = j.begin
+        b.end = j.end
+    return arr, keep
+
+
 class Batch:
     """An rl_batch: the job table on the device, launched or replayed as a
     captured CUDA graph."""
 
     def __init__(self, jobs: Sequence[BakeJob]):
         self.jobs = list(jobs)
-        self._keep: List[object] = []
-        arr = (_abi.BatchJob * max(len(self.jobs), 1))()
-        for q, j in enumerate(self.jobs):
-            b = arr[q]
-            b.kind = j.kind
-            b.scene = j.scene.handle.value
-            b.lightmap = j.lightmap.handle.value
-            if j.photonmaps:
-                maps = _map_array(j.photonmaps)
-                self._keep.append(maps)
-                b.photonmaps = C.cast(maps, C.c_void_p)
-            b.nmaps = len(j.photonmaps)
-            if j.lights is not None and len(j.lights):
-                b.lights = j.lights.ctypes.data
-                b.nlights = len(j.lights)
-                self._keep.append(j.lights)
-            if j.light_vertices is not None and len(j.light_vertices):
-                b.light_vertices = j.light_vertices.ctypes.data
-                b.nlight_vertices = j.nlight_vertices()
-                self._keep.append(j.light_vertices)
-            b.samples = j.samples
-            b.occluded_fraction = j.occluded_fraction
-            b.max_distance = j.max_distance
-            b.exponent = j.exponent
-            b.sky = (C.c_float * 3)(*[float(x) for x in j.sky])
-            b.ambient = (C.c_float * 3)(*[float(x) for x in j.ambient])
-            b.seed = j.seed & 0xFFFFFFFFFFFFFFFF
-            b.iterator = _abi.Iterator(*j.iterator)
-            b.begin = j.begin
-            b.end = j.end
+        arr, keep = _job_array(self.jobs)
         self.handle = C.c_void_p()
         check(lib().rl_batch_create(arr, len(self.jobs), C.byref(self.handle)))
+
+    def update(self, jobs: Sequence[BakeJob], stream=None):
+        """Replace the job table in stream order (a captured graph stays valid)."""
+        self.jobs = list(jobs)
+        arr, keep = _job_array(self.jobs)
+        check(lib().rl_batch_update(self.handle, arr, len(self.jobs), stream))
 
     def launch(self, stream=None):
         check(lib().rl_batch_launch(self.handle, stream))
@@ -180,19 +190,50 @@ class ResidentBatch:
             m.clear(colors=True, photons=False, stream=stream)
 
 
-def make_resident(workload, stream=None, builder: int = 1, passes=(DIRECT, AO, INDIRECT)) -> ResidentBatch:
-    """Upload a scenes.BatchWorkload: build each scene's BVH (the device LBVH
-    by default), emit and gather its photons, rasterise each job's lightmap
-    over all its scene's meshes, and make one BakeJob per pass per job."""
+@dataclass
+class ResidentScenes:
+    """Scenes on the device: each one's BVH and its gathered photonmaps."""
+    scenes: List[DeviceScene]
+    photonmaps: List[List[DeviceMap]]
+    workload: object
+
+    def nbytes(self) -> int:
+        """Device bytes held: BVH nodes and triangle records, the flat
+        scene's arrays as uploaded, and the photonmaps."""
+        total = 0
+        for ds, pms in zip(self.scenes, self.photonmaps):
+            st = ds.bvh_stats()
+            f = ds.flat
+            total += st["nodes"] * 64 + f.ntris * 48
+            for name in ("pos", "nrm", "uv0", "uv1", "vmat", "tris", "mat_rgb", "tex_pixels"):
+                a = getattr(f, name, None)
+                if isinstance(a, np.ndarray):
+                    total += a.nbytes
+            total += sum(DeviceMap.nbytes(m.width, m.height) for m in pms)
+        return total
+
+
+def make_resident_scenes(workload, stream=None, builder: int = 0, photons: bool = True) -> ResidentScenes:
+    """Build each scene's BVH (binned SAH on the host by default; 1 = the
+    device LBVH), then emit and gather its photons."""
     from .device import Relight
     scenes, pmaps = [], []
     for k, wl in enumerate(workload.scenes):
         rl = Relight(stream, seed=0xBA7C + k, builder=builder)
         ds = rl.device_scene(wl.scene)
-        if INDIRECT in passes:
+        if photons:
             rl.emit_photons(wl.scene, wl.settings)
         scenes.append(ds)
         pmaps.append([m._device for m in wl.scene.flat.photonmaps])
+    return ResidentScenes(scenes, pmaps, workload)
+
+
+def make_resident(workload, stream=None, builder: int = 0, passes=(DIRECT, AO, INDIRECT)) -> ResidentBatch:
+    """Upload a scenes.BatchWorkload: make its scenes resident, rasterise
+    each job's lightmap over all its scene's meshes, and make one BakeJob
+    per pass per job."""
+    rs = make_resident_scenes(workload, stream, builder, photons=INDIRECT in passes)
+    scenes, pmaps = rs.scenes, rs.photonmaps
     lightmaps, jobs = [], []
     texels = 0
     for spec in workload.jobs:

@@ -130,7 +130,12 @@ struct rl_map {
     int kind = 0;
     DevMap dev{};
     int* d_owner = nullptr;  // rasterisation scratch: winning face per texel
+    char* block = nullptr;   // rl_map_create_async: every array carved from this block
     ~rl_map() {
+        if (block) {
+            cudaFree(block);
+            return;
+        }
         cudaFree(dev.flags); cudaFree(dev.face); cudaFree(dev.position); cudaFree(dev.normal);
         cudaFree(dev.color); cudaFree(dev.photons); cudaFree(dev.gathered); cudaFree(dev.mesh); cudaFree(d_owner);
     }
@@ -404,6 +409,156 @@ extern "C" int rl_map_create(int kind, int width, int height, rl_map** out) {
     return RL_OK;
 }
 
+// The library's stream-ordered memory pool on the current device: lightmap
+// blocks and batch tables come from it.  Freed blocks stay in the pool (no
+// release at synchronisation points) until rl_pool_trim, so a serving loop
+// that admits and retires lightmaps reuses memory without remapping it.
+static std::mutex g_pool_mutex;
+static cudaMemPool_t g_pool[64];
+
+static int device_pool(cudaMemPool_t* out) {
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return fail(RL_INVALID_CALL, "device %d out of range", dev);
+    std::lock_guard<std::mutex> lk(g_pool_mutex);
+    if (!g_pool[dev]) {
+        cudaMemPoolProps props;
+        memset(&props, 0, sizeof props);
+        props.allocType = cudaMemAllocationTypePinned;
+        props.handleTypes = cudaMemHandleTypeNone;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t pool = nullptr;
+        CK(cudaMemPoolCreate(&pool, &props));
+        uint64_t keep = UINT64_MAX;
+        cudaError_t e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        if (e != cudaSuccess) {
+            cudaMemPoolDestroy(pool);
+            return fail(RL_CUDA_ERROR, "memory pool: %s", cudaGetErrorString(e));
+        }
+        g_pool[dev] = pool;
+    }
+    *out = g_pool[dev];
+    return RL_OK;
+}
+
+static int pool_alloc(void** p, size_t bytes, cudaStream_t st) {
+    cudaMemPool_t pool;
+    if (int rc = device_pool(&pool)) return rc;
+    cudaError_t e = cudaMallocFromPoolAsync(p, bytes, pool, st);
+    if (e != cudaSuccess)
+        return fail(e == cudaErrorMemoryAllocation ? RL_OUT_OF_MEMORY : RL_CUDA_ERROR, "pool allocation: %s",
+                    cudaGetErrorString(e));
+    return RL_OK;
+}
+
+extern "C" int rl_pool_trim(int64_t keep_bytes) {
+    cudaMemPool_t pool;
+    if (int rc = device_pool(&pool)) return rc;
+    CK(cudaMemPoolTrimTo(pool, keep_bytes < 0 ? 0 : (size_t)keep_bytes));
+    return RL_OK;
+}
+
+extern "C" int rl_pool_bytes(int64_t* reserved, int64_t* used) {
+    cudaMemPool_t pool;
+    if (int rc = device_pool(&pool)) return rc;
+    uint64_t r = 0, u = 0;
+    CK(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &r));
+    CK(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &u));
+    if (reserved) *reserved = (int64_t)r;
+    if (used) *used = (int64_t)u;
+    return RL_OK;
+}
+
+// Lumel::Lumel (Lightmap.h:52) for a map carved from one block.
+__global__ void k_map_init(DevMap m, int* owner, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        m.flags[i] = 0;
+        m.face[i] = 0xffff;
+        m.mesh[i] = -1;
+        owner[i] = -1;
+        m.photons[i] = 0;
+        for (int c = 0; c < 3; c++) {
+            m.position[3 * i + c] = 0.f;
+            m.normal[3 * i + c] = 0.f;
+            m.color[3 * i + c] = 0.f;
+            m.gathered[3 * i + c] = 0.f;
+        }
+    }
+}
+
+static size_t map_block_bytes(size_t n, size_t offs[9]) {
+    const size_t sz[9] = {4 * n, 4 * n, 4 * n, 12 * n, 12 * n, 12 * n, 4 * n, 12 * n, 4 * n};
+    size_t off = 0;
+    for (int k = 0; k < 9; k++) {
+        offs[k] = off;
+        off = (off + sz[k] + 255) & ~(size_t)255;
+    }
+    return off;
+}
+
+extern "C" int rl_map_bytes(int width, int height, int64_t* bytes) {
+    if (!bytes || width <= 0 || height <= 0) return fail(RL_INVALID_CALL, "rl_map_bytes: bad arguments");
+    size_t offs[9];
+    *bytes = (int64_t)map_block_bytes((size_t)width * height, offs);
+    return RL_OK;
+}
+
+extern "C" int rl_map_create_async(int kind, int width, int height, void* stream, rl_map** out) {
+    if (!out || width <= 0 || height <= 0 || kind < 0 || kind > 2)
+        return fail(RL_INVALID_CALL, "rl_map_create_async: bad arguments");
+    if ((long long)width * height > (1ll << 30)) return fail(RL_INVALID_CALL, "map too large");
+    *out = nullptr;
+    cudaStream_t st = S(stream);
+    size_t n = (size_t)width * height, offs[9];
+    size_t bytes = map_block_bytes(n, offs);
+    char* blk = nullptr;
+    if (int rc = pool_alloc((void**)&blk, bytes, st)) return rc;
+    rl_map* m = new (std::nothrow) rl_map;
+    if (!m) {
+        cudaFreeAsync(blk, st);
+        return fail(RL_OUT_OF_MEMORY, "host allocation failed");
+    }
+    m->kind = kind;
+    m->block = blk;
+    m->dev.width = width;
+    m->dev.height = height;
+    m->dev.flags = (int*)(blk + offs[0]);
+    m->dev.face = (int*)(blk + offs[1]);
+    m->dev.mesh = (int*)(blk + offs[2]);
+    m->dev.position = (float*)(blk + offs[3]);
+    m->dev.normal = (float*)(blk + offs[4]);
+    m->dev.color = (float*)(blk + offs[5]);
+    m->dev.photons = (int*)(blk + offs[6]);
+    m->dev.gathered = (float*)(blk + offs[7]);
+    m->d_owner = (int*)(blk + offs[8]);
+    int grid = (int)std::min<long long>(((long long)n + 255) / 256, 148 * 16);
+    k_map_init<<<grid, 256, 0, st>>>(m->dev, m->d_owner, (long long)n);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        m->block = nullptr;
+        m->dev = DevMap{};
+        m->d_owner = nullptr;
+        cudaFreeAsync(blk, st);
+        delete m;
+        return fail(RL_CUDA_ERROR, "k_map_init: %s", cudaGetErrorString(e));
+    }
+    *out = m;
+    return RL_OK;
+}
+
+extern "C" int rl_map_destroy_async(rl_map* m, void* stream) {
+    if (!m) return fail(RL_INVALID_CALL, "null map");
+    if (!m->block) return fail(RL_INVALID_CALL, "rl_map_destroy_async: map was not made by rl_map_create_async");
+    cudaError_t e = cudaFreeAsync(m->block, S(stream));
+    m->block = nullptr;
+    m->dev = DevMap{};
+    m->d_owner = nullptr;
+    delete m;
+    if (e != cudaSuccess) return fail(RL_CUDA_ERROR, "map free: %s", cudaGetErrorString(e));
+    return RL_OK;
+}
+
 extern "C" int rl_map_destroy(rl_map* m) {
     if (!m) return fail(RL_INVALID_CALL, "null map");
     cudaDeviceSynchronize();
@@ -512,6 +667,13 @@ extern "C" int rl_map_download(const rl_map* m, int32_t* flags, int32_t* face, f
     if (photons) CK(cudaMemcpyAsync(photons, m->dev.photons, 4 * n, cudaMemcpyDeviceToHost, st));
     if (gathered) CK(cudaMemcpyAsync(gathered, m->dev.gathered, 12 * n, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
+    return RL_OK;
+}
+
+extern "C" int rl_map_download_async(const rl_map* m, float* color, void* stream) {
+    if (!m || !color) return fail(RL_INVALID_CALL, "rl_map_download_async: null argument");
+    size_t n = (size_t)m->dev.width * m->dev.height;
+    CK(cudaMemcpyAsync(color, m->dev.color, 12 * n, cudaMemcpyDeviceToHost, S(stream)));
     return RL_OK;
 }
 
@@ -1497,29 +1659,44 @@ struct DevJob {
     uint2 key;
 };
 
+// Where the batch kernel of one pass kind finds its jobs.  The headers sit
+// at a fixed device address and the kernels read them at run time, so a
+// captured launch stays valid when rl_batch_update rewrites the tables.
+struct BatchHeader {
+    const DevJob* jobs;
+    const long long* prefix;  // work-item offset of each job (multiples of 32)
+    long long total;          // work items incl. padding
+    int njobs, pad;
+};
+
 // The job table is split by pass: one persistent kernel per pass kind takes
 // the items of every job of that kind, so each kernel keeps only its own ray
-// loop's registers.
+// loop's registers.  Tables live in one device buffer, written from pinned
+// staging that alternates between two slots so the host can fill the next
+// table while the previous copy is in flight.
 struct rl_batch {
-    std::vector<DevJob> jobs[3];
-    std::vector<long long> prefix[3];  // work-item offset of each job (multiples of 32)
-    DevJob* d_jobs[3] = {nullptr, nullptr, nullptr};
-    long long* d_prefix[3] = {nullptr, nullptr, nullptr};
-    unsigned long long* d_counter = nullptr;  // one per kind
-    std::vector<void*> owned;
+    BatchHeader* d_hdr = nullptr;             // 3 headers
+    unsigned long long* d_counter = nullptr;  // 3 work counters
+    char* d_buf = nullptr;
+    size_t d_cap = 0;
+    char* h_stage[2] = {nullptr, nullptr};
+    size_t h_cap[2] = {0, 0};
+    cudaEvent_t staged[2] = {nullptr, nullptr};
+    int slot = 0;
     long long items = 0, total[3] = {0, 0, 0};
-    int grid[3] = {0, 0, 0}, block[3] = {128, 128, 128};
+    int grid[3] = {0, 0, 0}, block[3] = {128, 128, 128}, refill[3] = {0, 0, 0};
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     ~rl_batch() {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
-        for (int k = 0; k < 3; k++) {
-            cudaFree(d_jobs[k]);
-            cudaFree(d_prefix[k]);
+        for (int k = 0; k < 2; k++) {
+            if (staged[k]) cudaEventDestroy(staged[k]);
+            if (h_stage[k]) cudaFreeHost(h_stage[k]);
         }
+        cudaFree(d_buf);
+        cudaFree(d_hdr);
         cudaFree(d_counter);
-        for (void* p : owned) cudaFree(p);
     }
 };
 
@@ -1528,7 +1705,7 @@ __device__ __forceinline__ int find_job(const long long* prefix, int njobs, long
     int lo = 0, hi = njobs - 1;
     while (lo < hi) {
         int mid = (lo + hi + 1) >> 1;
-        if (__ldg(prefix + mid) <= w) lo = mid;
+        if (prefix[mid] <= w) lo = mid;
         else hi = mid - 1;
     }
     return lo;
@@ -1542,22 +1719,31 @@ __device__ __forceinline__ int find_job(const long long* prefix, int njobs, long
 // and Philox keys as the single-job calls, so the lumels come out
 // bit-identical to rl_bake_direct / rl_bake_ao / rl_bake_indirect.
 template <int kKind>
-__global__ void __launch_bounds__(kKind == 0 ? 128 : 256) k_batch(const DevJob* __restrict__ jobs, const long long* __restrict__ prefix,
-                                               int njobs, long long total, unsigned long long* counter,
-                                               int refill) {
+__global__ void __launch_bounds__(kKind == 0 ? 128 : 256, kKind == 0 ? 1 : 3) k_batch(const BatchHeader* __restrict__ hdrs,
+                                                                  unsigned long long* counter, int refill) {
+    if (hdrs[kKind].total <= 0) return;
     const int lane = threadIdx.x & 31;
     for (;;) {
-        unsigned long long base = 0;
-        int j = 0;
+        // lane 0 takes the next chunk and finds its job; the header is
+        // re-read per chunk (L1-resident) so no table state stays live in
+        // registers across the ray loop
+        unsigned long long jp = 0;
+        long long off = -1;
         if (lane == 0) {
-            base = atomicAdd(counter, 32ull);
-            if (base < (unsigned long long)total) j = find_job(prefix, njobs, (long long)base);
+            const BatchHeader* H = hdrs + kKind;
+            unsigned long long base = atomicAdd(counter + kKind, 32ull);
+            long long total = H->total;
+            if (base < (unsigned long long)total) {
+                int j = find_job(H->prefix, H->njobs, (long long)base);
+                jp = (unsigned long long)(H->jobs + j);
+                off = (long long)base - H->prefix[j];
+            }
         }
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (base >= (unsigned long long)total) break;
-        j = __shfl_sync(0xffffffffu, j, 0);
-        const DevJob& J = jobs[j];
-        const long long r = (long long)base - __ldg(prefix + j) + lane;
+        off = __shfl_sync(0xffffffffu, off, 0);
+        if (off < 0) break;
+        jp = __shfl_sync(0xffffffffu, jp, 0);
+        const DevJob& J = *(const DevJob*)jp;
+        const long long r = off + lane;
         long long i = 0;
         const bool valid = r < J.count && iter_lumel(J.m, J.it, J.k_begin + r, i);
         if (kKind == 0) {
@@ -1638,131 +1824,218 @@ static double job_item_cost(const rl_batch_job& J) {
     return c;
 }
 
-extern "C" int rl_batch_create(const rl_batch_job* jobs, int njobs, rl_batch** out) {
-    if (!out || njobs < 0 || (njobs > 0 && !jobs)) return fail(RL_INVALID_CALL, "rl_batch_create: bad arguments");
-    *out = nullptr;
-    rl_batch* b = new (std::nothrow) rl_batch;
-    if (!b) return fail(RL_OUT_OF_MEMORY, "host allocation failed");
-    std::vector<int> order(njobs);
-    for (int q = 0; q < njobs; q++) order[q] = q;
-    for (int q = 0; q < njobs; q++)
-        if (jobs[q].kind == 0 && jobs[q].nlights > 0 && !jobs[q].lights) {
-            delete b;
-            return fail(RL_INVALID_CALL, "batch job %d: null light array", q);
-        }
+static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+static int batch_init(rl_batch* b) {
+    CK(cudaMalloc(&b->d_hdr, 3 * sizeof(BatchHeader)));
+    CK(cudaMemset(b->d_hdr, 0, 3 * sizeof(BatchHeader)));
+    CK(cudaMalloc(&b->d_counter, 3 * sizeof(unsigned long long)));
+    for (int k = 0; k < 2; k++) CK(cudaEventCreateWithFlags(&b->staged[k], cudaEventDisableTiming));
+    int dev = 0, sms = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const void* kern[3] = {(const void*)k_batch<0>, (const void*)k_batch<1>, (const void*)k_batch<2>};
+    b->block[0] = 128;
+    b->block[1] = g_tune[RL_TUNE_AO_BLOCK];
+    b->block[2] = g_tune[RL_TUNE_FG_BLOCK];
+    b->refill[1] = g_tune[RL_TUNE_AO_REFILL];
+    b->refill[2] = g_tune[RL_TUNE_FG_REFILL];
+    for (int k = 0; k < 3; k++) {
+        int per = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern[k], b->block[k], 0));
+        b->grid[k] = sms * std::max(per, 1);
+    }
+    return RL_OK;
+}
+
+// Validate `jobs`, lay out the tables (jobs sorted by kind, then by item
+// cost), fill the pinned staging slot with device addresses, and enqueue
+// the copies on `st`.  On error the batch keeps its previous tables.
+// Host-side checks of a job table (no device access).
+static int batch_validate(const rl_batch_job* jobs, int njobs) {
+    if (njobs < 0 || (njobs > 0 && !jobs)) return fail(RL_INVALID_CALL, "batch: bad job array");
+    for (int q = 0; q < njobs; q++) {
+        const rl_batch_job& J = jobs[q];
+        if (!J.scene || !J.lightmap || J.kind < 0 || J.kind > 2)
+            return fail(RL_INVALID_CALL, "batch job %d: bad scene, lightmap or kind", q);
+        if (J.kind == 0 && J.nlights > 0 && !J.lights) return fail(RL_INVALID_CALL, "batch job %d: null light array", q);
+        if ((J.kind == 1 || J.kind == 2) && J.samples <= 0)
+            return fail(RL_INVALID_CALL, "batch job %d: samples must be positive", q);
+        if (J.kind == 2 && (J.nmaps < 0 || J.nmaps > kMaxPhotonmaps || (J.nmaps > 0 && !J.photonmaps)))
+            return fail(RL_INVALID_CALL, "batch job %d: bad photonmaps", q);
+        for (int k = 0; J.kind == 2 && k < J.nmaps; k++)
+            if (!J.photonmaps[k]) return fail(RL_INVALID_CALL, "batch job %d: null photonmap", q);
+    }
     {
         std::map<std::pair<int, const rl_map*>, std::vector<int>> by_map;
         for (int q = 0; q < njobs; q++) by_map[{jobs[q].kind, jobs[q].lightmap}].push_back(q);
         for (auto& kv : by_map)
             for (size_t x = 0; x < kv.second.size(); x++)
                 for (size_t y = x + 1; y < kv.second.size(); y++)
-                    if (jobs_may_overlap(jobs[kv.second[x]], jobs[kv.second[y]])) {
-                        delete b;
+                    if (jobs_may_overlap(jobs[kv.second[x]], jobs[kv.second[y]]))
                         return fail(RL_INVALID_CALL, "batch jobs %d and %d: one pass over shared lumels of one lightmap",
                                     kv.second[x], kv.second[y]);
-                    }
     }
-    std::stable_sort(order.begin(), order.end(),
-                     [&](int x, int y) { return job_item_cost(jobs[x]) > job_item_cost(jobs[y]); });
-    std::map<const rl_light*, LightTable*> light_tables;
-    int rc = RL_OK;
+    return RL_OK;
+}
+
+static int batch_update(rl_batch* b, const rl_batch_job* jobs, int njobs, cudaStream_t st) {
+    if (int rc = batch_validate(jobs, njobs)) return rc;
+    std::vector<int> order(njobs);
+    for (int q = 0; q < njobs; q++) order[q] = q;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+        if (jobs[x].kind != jobs[y].kind) return jobs[x].kind < jobs[y].kind;
+        return job_item_cost(jobs[x]) > job_item_cost(jobs[y]);
+    });
+    // pass 1: slices, counts and the distinct light tables / photonmap sets
+    struct Slot { int q; long long b0, count; Iter it; };
+    std::vector<Slot> live[3];
+    std::map<const rl_light*, int> light_idx;
+    std::map<std::vector<const rl_map*>, int> maps_idx;
+    std::vector<const rl_batch_job*> light_src, maps_src;
     for (int q : order) {
         const rl_batch_job& J = jobs[q];
-        if (!J.scene || !J.lightmap || J.kind < 0 || J.kind > 2) {
-            rc = fail(RL_INVALID_CALL, "batch job %d: bad scene, lightmap or kind", q);
-            break;
-        }
-        if ((J.kind == 1 || J.kind == 2) && J.samples <= 0) {
-            rc = fail(RL_INVALID_CALL, "batch job %d: samples must be positive", q);
-            break;
-        }
-        DevJob d;
-        memset(&d, 0, sizeof d);
-        d.s = J.scene->dev;
-        d.m = J.lightmap->dev;
-        d.status = J.scene->d_status;
-        d.kind = J.kind;
-        d.samples = J.samples;
-        d.fraction = J.occluded_fraction;
-        d.maxd = J.max_distance;
-        d.exponent = J.exponent;
-        d.sky = V3{J.sky[0], J.sky[1], J.sky[2]};
-        d.amb = V3{J.ambient[0], J.ambient[1], J.ambient[2]};
-        d.key = make_uint2((uint32_t)J.seed, (uint32_t)(J.seed >> 32));
         long long n = (long long)J.lightmap->dev.width * J.lightmap->dev.height, count = 0;
-        rc = make_iter(&J.iterator, J.scene, n, d.it, count);
-        if (rc) break;
+        Iter it;
+        int rc = make_iter(&J.iterator, J.scene, n, it, count);
+        if (rc) return rc;
         long long b0 = J.begin < 0 ? 0 : (J.begin < count ? J.begin : count);
         long long e0 = J.end < 0 || J.end > count ? count : J.end;
         if (e0 < b0) e0 = b0;
-        d.k_begin = b0;
-        d.count = e0 - b0;
-        if (J.kind == 0 && J.nlights == 0) d.count = 0;  // rl_bake_direct with no lights bakes nothing
-        if (J.kind == 0 && d.count > 0) {
-            auto it = light_tables.find(J.lights);
-            if (it == light_tables.end()) {
-                static thread_local LightTable T;
-                rc = make_light_table(J.lights, J.nlights, J.light_vertices, J.nlight_vertices, T);
-                if (rc) break;
-                LightTable* dl = nullptr;
-                cudaError_t e = cudaMalloc(&dl, sizeof(LightTable));
-                if (e == cudaSuccess) b->owned.push_back(dl);
-                if (e == cudaSuccess) e = cudaMemcpy(dl, &T, sizeof(LightTable), cudaMemcpyHostToDevice);
-                if (e != cudaSuccess) { rc = fail(RL_CUDA_ERROR, "light table: %s", cudaGetErrorString(e)); break; }
-                it = light_tables.emplace(J.lights, dl).first;
+        if (J.kind == 0 && J.nlights == 0) e0 = b0;  // rl_bake_direct with no lights bakes nothing
+        if (e0 == b0) continue;
+        if (J.kind == 0) {
+            if (J.nlights > kMaxLights || J.nlight_vertices < 0 || J.nlight_vertices > kMaxLightVerts)
+                return fail(RL_INVALID_CALL, "batch job %d: too many lights or light vertices", q);
+            if (!light_idx.count(J.lights)) {
+                light_idx[J.lights] = (int)light_src.size();
+                light_src.push_back(&J);
             }
-            d.lights = it->second;
         }
-        if (J.kind == 2 && d.count > 0) {
-            if (J.nmaps < 0 || J.nmaps > kMaxPhotonmaps || (J.nmaps > 0 && !J.photonmaps)) {
-                rc = fail(RL_INVALID_CALL, "batch job %d: bad photonmaps", q);
-                break;
+        if (J.kind == 2) {
+            std::vector<const rl_map*> key(J.photonmaps, J.photonmaps + J.nmaps);
+            if (!maps_idx.count(key)) {
+                maps_idx[key] = (int)maps_src.size();
+                maps_src.push_back(&J);
             }
-            static thread_local GatherMaps G;
-            memset(&G, 0, sizeof G);
-            G.nmaps = J.nmaps;
-            for (int k = 0; k < J.nmaps; k++) {
-                if (!J.photonmaps[k]) { rc = fail(RL_INVALID_CALL, "batch job %d: null photonmap", q); break; }
-                G.maps[k] = J.photonmaps[k]->dev;
-            }
-            if (rc) break;
-            GatherMaps* dg = nullptr;
-            cudaError_t e = cudaMalloc(&dg, sizeof(GatherMaps));
-            if (e == cudaSuccess) b->owned.push_back(dg);
-            if (e == cudaSuccess) e = cudaMemcpy(dg, &G, sizeof(GatherMaps), cudaMemcpyHostToDevice);
-            if (e != cudaSuccess) { rc = fail(RL_CUDA_ERROR, "gather maps: %s", cudaGetErrorString(e)); break; }
-            d.maps = dg;
         }
-        if (d.count == 0) continue;
-        b->jobs[J.kind].push_back(d);
-        b->prefix[J.kind].push_back(b->total[J.kind]);
-        b->items += d.count;
-        b->total[J.kind] += (d.count + 31) / 32 * 32;
+        live[J.kind].push_back(Slot{q, b0, e0 - b0, it});
     }
-    if (!rc) {
-        int dev = 0, sms = 0;
-        cudaError_t e = cudaGetDevice(&dev);
-        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        const void* kern[3] = {(const void*)k_batch<0>, (const void*)k_batch<1>, (const void*)k_batch<2>};
-        b->block[0] = 128;
-        b->block[1] = g_tune[RL_TUNE_AO_BLOCK];
-        b->block[2] = g_tune[RL_TUNE_FG_BLOCK];
-        for (int k = 0; k < 3 && e == cudaSuccess; k++) {
-            int per = 0;
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern[k], b->block[k], 0);
-            b->grid[k] = sms * std::max(per, 1);
-            size_t nj = b->jobs[k].size();
-            if (e == cudaSuccess && nj) e = cudaMalloc(&b->d_jobs[k], sizeof(DevJob) * nj);
-            if (e == cudaSuccess && nj) e = cudaMalloc(&b->d_prefix[k], sizeof(long long) * nj);
-            if (e == cudaSuccess && nj)
-                e = cudaMemcpy(b->d_jobs[k], b->jobs[k].data(), sizeof(DevJob) * nj, cudaMemcpyHostToDevice);
-            if (e == cudaSuccess && nj)
-                e = cudaMemcpy(b->d_prefix[k], b->prefix[k].data(), sizeof(long long) * nj, cudaMemcpyHostToDevice);
+    // layout
+    size_t off_jobs[3], off_prefix[3], off = 0;
+    for (int k = 0; k < 3; k++) {
+        off_jobs[k] = off;
+        off = align256(off + live[k].size() * sizeof(DevJob));
+        off_prefix[k] = off;
+        off = align256(off + live[k].size() * sizeof(long long));
+    }
+    size_t off_lights = off;
+    off = align256(off + light_src.size() * sizeof(LightTable));
+    size_t off_maps = off;
+    off = align256(off + maps_src.size() * sizeof(GatherMaps));
+    size_t off_hdr = off;
+    size_t bytes = off + 3 * sizeof(BatchHeader);
+    // device buffer (stream-ordered, so growing it does not stall the device)
+    if (bytes > b->d_cap) {
+        size_t cap = std::max(bytes, b->d_cap * 2);
+        char* nb = nullptr;
+        if (int rc = pool_alloc((void**)&nb, cap, st)) return rc;
+        if (b->d_buf) CK(cudaFreeAsync(b->d_buf, st));
+        b->d_buf = nb;
+        b->d_cap = cap;
+    }
+    // staging slot: wait for the copy that used it last
+    int sl = b->slot;
+    CK(cudaEventSynchronize(b->staged[sl]));
+    if (bytes > b->h_cap[sl]) {
+        if (b->h_stage[sl]) CK(cudaFreeHost(b->h_stage[sl]));
+        b->h_stage[sl] = nullptr;
+        b->h_cap[sl] = 0;
+        size_t cap = std::max(bytes, (size_t)1 << 16);
+        CK(cudaHostAlloc((void**)&b->h_stage[sl], cap, cudaHostAllocDefault));
+        b->h_cap[sl] = cap;
+    }
+    char* h = b->h_stage[sl];
+    char* d = b->d_buf;
+    for (size_t t = 0; t < light_src.size(); t++) {
+        const rl_batch_job& J = *light_src[t];
+        LightTable* T = (LightTable*)(h + off_lights + t * sizeof(LightTable));
+        int rc = make_light_table(J.lights, J.nlights, J.light_vertices, J.nlight_vertices, *T);
+        if (rc) return rc;
+    }
+    for (size_t t = 0; t < maps_src.size(); t++) {
+        const rl_batch_job& J = *maps_src[t];
+        GatherMaps* G = (GatherMaps*)(h + off_maps + t * sizeof(GatherMaps));
+        memset(G, 0, sizeof(GatherMaps));
+        G->nmaps = J.nmaps;
+        for (int k = 0; k < J.nmaps; k++) G->maps[k] = J.photonmaps[k]->dev;
+    }
+    BatchHeader hdr[3];
+    long long items = 0;
+    for (int k = 0; k < 3; k++) {
+        DevJob* tab = (DevJob*)(h + off_jobs[k]);
+        long long* pre = (long long*)(h + off_prefix[k]);
+        long long total = 0;
+        for (size_t t = 0; t < live[k].size(); t++) {
+            const Slot& L = live[k][t];
+            const rl_batch_job& J = jobs[L.q];
+            DevJob dj;
+            memset(&dj, 0, sizeof dj);
+            dj.s = J.scene->dev;
+            dj.m = J.lightmap->dev;
+            dj.status = J.scene->d_status;
+            dj.it = L.it;
+            dj.k_begin = L.b0;
+            dj.count = L.count;
+            dj.kind = J.kind;
+            dj.samples = J.samples;
+            dj.fraction = J.occluded_fraction;
+            dj.maxd = J.max_distance;
+            dj.exponent = J.exponent;
+            dj.sky = V3{J.sky[0], J.sky[1], J.sky[2]};
+            dj.amb = V3{J.ambient[0], J.ambient[1], J.ambient[2]};
+            dj.key = make_uint2((uint32_t)J.seed, (uint32_t)(J.seed >> 32));
+            if (k == 0)
+                dj.lights = (const LightTable*)(d + off_lights + light_idx[J.lights] * sizeof(LightTable));
+            if (k == 2) {
+                std::vector<const rl_map*> key(J.photonmaps, J.photonmaps + J.nmaps);
+                dj.maps = (const GatherMaps*)(d + off_maps + maps_idx[key] * sizeof(GatherMaps));
+            }
+            tab[t] = dj;
+            pre[t] = total;
+            items += L.count;
+            total += (L.count + 31) / 32 * 32;
         }
-        if (e == cudaSuccess) e = cudaMalloc(&b->d_counter, 3 * sizeof(unsigned long long));
+        hdr[k].jobs = (const DevJob*)(d + off_jobs[k]);
+        hdr[k].prefix = (const long long*)(d + off_prefix[k]);
+        hdr[k].total = total;
+        hdr[k].njobs = (int)live[k].size();
+        hdr[k].pad = 0;
+        b->total[k] = total;
+    }
+    memcpy(h + off_hdr, hdr, sizeof hdr);
+    b->items = items;
+    if (off_hdr > 0) CK(cudaMemcpyAsync(d, h, off_hdr, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(b->d_hdr, h + off_hdr, sizeof hdr, cudaMemcpyHostToDevice, st));
+    CK(cudaEventRecord(b->staged[sl], st));
+    b->slot ^= 1;
+    return RL_OK;
+}
+
+extern "C" int rl_batch_create(const rl_batch_job* jobs, int njobs, rl_batch** out) {
+    if (!out || njobs < 0 || (njobs > 0 && !jobs)) return fail(RL_INVALID_CALL, "rl_batch_create: bad arguments");
+    *out = nullptr;
+    if (int rc = batch_validate(jobs, njobs)) return rc;
+    rl_batch* b = new (std::nothrow) rl_batch;
+    if (!b) return fail(RL_OUT_OF_MEMORY, "host allocation failed");
+    int rc = batch_init(b);
+    if (!rc) rc = batch_update(b, jobs, njobs, 0);
+    if (!rc) {
+        cudaError_t e = cudaStreamSynchronize(0);
         if (e != cudaSuccess) rc = fail(RL_CUDA_ERROR, "batch upload: %s", cudaGetErrorString(e));
     }
     if (rc) {
+        cudaDeviceSynchronize();
         delete b;
         return rc;
     }
@@ -1770,22 +2043,22 @@ extern "C" int rl_batch_create(const rl_batch_job* jobs, int njobs, rl_batch** o
     return RL_OK;
 }
 
+extern "C" int rl_batch_update(rl_batch* b, const rl_batch_job* jobs, int njobs, void* stream) {
+    if (!b) return fail(RL_INVALID_CALL, "null batch");
+    return batch_update(b, jobs, njobs, S(stream));
+}
+
 // The kinds run in sequence on the stream in the order a bake applies them
 // to one lightmap (direct light adds, AO scales, final gather adds: the
 // demo's Bake job, src/demo/Lightmapping.cpp:270-279, plus AO between), so a
 // lightmap baked by several passes of one batch gets the sequential result.
+// Every kind is launched (an empty one returns at once), so the launch
+// sequence is the same for any table.
 static int batch_enqueue(rl_batch* b, cudaStream_t st) {
-    if (b->items == 0) return RL_OK;
     CK(cudaMemsetAsync(b->d_counter, 0, 3 * sizeof(unsigned long long), st));
-    const int refill[3] = {0, g_tune[RL_TUNE_AO_REFILL], g_tune[RL_TUNE_FG_REFILL]};
     for (int k = 0; k < 3; k++) {
-        if (b->total[k] == 0) continue;
-        long long warps = b->total[k] / 32;
-        int wpb = b->block[k] / 32;
-        int grid = (int)std::min<long long>(b->grid[k], (warps + wpb - 1) / wpb);
         auto kern = k == 0 ? k_batch<0> : k == 1 ? k_batch<1> : k_batch<2>;
-        kern<<<grid, b->block[k], 0, st>>>(b->d_jobs[k], b->d_prefix[k], (int)b->jobs[k].size(), b->total[k],
-                                           b->d_counter + k, refill[k]);
+        kern<<<b->grid[k], b->block[k], 0, st>>>(b->d_hdr, b->d_counter, b->refill[k]);
         CK_LAUNCH("k_batch");
     }
     return RL_OK;
@@ -1793,6 +2066,7 @@ static int batch_enqueue(rl_batch* b, cudaStream_t st) {
 
 extern "C" int rl_batch_launch(rl_batch* b, void* stream) {
     if (!b) return fail(RL_INVALID_CALL, "null batch");
+    if (b->items == 0) return RL_OK;
     return batch_enqueue(b, S(stream));
 }
 

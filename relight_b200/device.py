@@ -64,10 +64,25 @@ class DeviceScene:
 class DeviceMap:
     """An rl_map: lumel arrays of one lightmap / photonmap on the device."""
 
-    def __init__(self, kind: int, width: int, height: int):
+    def __init__(self, kind: int, width: int, height: int, stream=None, stream_ordered: bool = False):
+        """stream_ordered: one block from the stream-ordered allocator
+        (rl_map_create_async on `stream`), released by close() in stream
+        order as well; neither waits for the device."""
         self.kind, self.width, self.height = kind, width, height
         self.handle = C.c_void_p()
-        check(lib().rl_map_create(kind, width, height, C.byref(self.handle)))
+        self.stream_ordered = stream_ordered
+        self.stream = stream
+        if stream_ordered:
+            check(lib().rl_map_create_async(kind, width, height, stream, C.byref(self.handle)))
+        else:
+            check(lib().rl_map_create(kind, width, height, C.byref(self.handle)))
+
+    @staticmethod
+    def nbytes(width: int, height: int) -> int:
+        """Device bytes of a stream-ordered width x height map (rl_map_bytes)."""
+        b = C.c_int64()
+        check(lib().rl_map_bytes(width, height, C.byref(b)))
+        return b.value
 
     def add_mesh(self, scene: DeviceScene, mesh_index: int, stream=None):
         check(lib().rl_map_add_mesh(self.handle, scene.handle, mesh_index, stream))
@@ -87,6 +102,11 @@ class DeviceMap:
                 args.append(None)
         check(lib().rl_map_download(self.handle, *args, stream))
         return out
+
+    def download_color_async(self, out_ptr: int, stream=None):
+        """Copy the colours ([w*h][3] float32) to host memory at `out_ptr` in
+        stream order, without waiting (rl_map_download_async)."""
+        check(lib().rl_map_download_async(self.handle, C.c_void_p(out_ptr), stream))
 
     def upload(self, stream=None, **arrays):
         args = []
@@ -114,9 +134,12 @@ class DeviceMap:
         check(lib().rl_map_valid_count(self.handle, C.byref(c)))
         return c.value
 
-    def close(self):
+    def close(self, stream=None):
         if self.handle:
-            check(lib().rl_map_destroy(self.handle))
+            if self.stream_ordered:
+                check(lib().rl_map_destroy_async(self.handle, stream if stream is not None else self.stream))
+            else:
+                check(lib().rl_map_destroy(self.handle))
             self.handle = C.c_void_p()
 
     def __del__(self):

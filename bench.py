@@ -43,9 +43,10 @@ RAY_MODEL = {"n_box": 43.78, "n_tri": 2.80, "bytes_per_ray": 1583.6}
 METRIC = "lightmap texels/s (photons + gather + final gather 256 spp, 1024^2)"
 UNIT = "texels/s"
 WORKLOAD = "terrain 256^2 verts + 2000 boxes (154,050 tris), 1M photons x3 bounces, gather r7, FG 256 spp, 1024^2"
-# DRAM bytes (read + write) of one k_indirect launch, from the ncu capture in
-# profiles/ (None until captured).
-FG_DRAM_TRAFFIC = None
+# DRAM bytes (read + write) of one full-size k_indirect launch, from the ncu
+# capture summarised in profiles/k_indirect_terrain_launches.md
+# (dram__bytes_read.sum 75,599,104 + dram__bytes_write.sum 4,105,984).
+FG_DRAM_TRAFFIC = 79_705_088
 
 
 def load_peaks():

@@ -362,6 +362,9 @@ def batch_arm(args):
         stream.synchronize()
         t_resident = time.perf_counter() - t0
         valid = sum(m.valid_count() for m in res.lightmaps)
+        t0 = time.perf_counter()
+        tuned = autotune.tune_batch(res.jobs, stream, sample=8, reset=lambda: res.clear(stream=sh))
+        t_tune = time.perf_counter() - t0
         b = batch.Batch(res.jobs)
         b.capture(sh)
         ev = lambda: torch.cuda.Event(enable_timing=True)
@@ -404,12 +407,15 @@ def batch_arm(args):
                                f"log-uniform 32^2-1024^2, direct + AO 64 + FG 128 per job",
                    "jobs": n_jobs, "scenes": n_scenes, "triangles": wl.triangles, "valid_texels": valid,
                    "texels": res.texels, "l2": "flushed between steps (256 MiB write)",
-                   "tuning": {"fg": autotune.get("indirect"), "ao": autotune.get("ao")}},
+                   "tuning": {"fg": autotune.get("indirect"), "ao": autotune.get("ao"),
+                              "source": "autotune.tune_batch on every 8th job",
+                              "fg_table_ms": {f"{k[0]}/{k[1]}": v for k, v in tuned.get("indirect", ({}, {}))[1].items()},
+                              "ao_table_ms": {f"{k[0]}/{k[1]}": v for k, v in tuned.get("ao", ({}, {}))[1].items()}}},
         "texels_per_s": valid / (bm / 1e3), "grays_per_s": rays / (bm / 1e3) / 1e9,
         "per_job_loop": {"value": n_jobs / (lm_ / 1e3), "ms_per_step": lm_, "launches_per_step": len(res.jobs)},
         "batch_over_loop": lm_ / bm, "identical_to_loop": identical,
         "gpu_launches": 3 * args.steps, "clocks": clocks.summary(),
-        "setup_s": {"scenes_host": t_scenes, "resident": t_resident},
+        "setup_s": {"scenes_host": t_scenes, "resident": t_resident, "tune": t_tune},
     }
 
 

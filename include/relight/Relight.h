@@ -167,6 +167,9 @@ typedef std::vector<Index> IndexBuffer;
 class Mesh {
 public:
     static Mesh* create() { return new Mesh; }
+    // Mesh::createFromFile (scene/Mesh.cpp:111-122): a Wavefront OBJ read
+    // with MeshLoader's rules (rl_obj_load); NULL if it cannot be loaded.
+    static Mesh* createFromFile(const std::string& fileName);
     // Mesh::addFaces (scene/Mesh.cpp:146-165): indices offset by the current
     // vertex count, one material for the added vertices.
     void addFaces(const VertexBuffer& vertices, const IndexBuffer& indices, const Material* material = nullptr);
@@ -330,8 +333,13 @@ public:
     virtual RelightStatus addMesh(const Mesh* mesh);
     // Lightmap::toHdr (Lightmap.cpp:332-349); the caller deletes[] the buffer.
     float* toHdr();
-    // Lightmap::save, RawHdr format (Lightmap.cpp:232-239).
+    // Lightmap::save (Lightmap.cpp:223-283): RawHdr, TgaDoubleLdr or TgaRgbm,
+    // the reference's file byte for byte (TGA encoding on the device; a
+    // lightmap that was never baked saves RawHdr only).
     bool save(const std::string& fileName, StorageFormat format);
+    // Lightmap::expand / blur (Lightmap.cpp:167-220), on the device.
+    void expand();
+    void blur();
 
     // device side (used by Relight)
     rl_map* device() const { return m_device; }

@@ -172,6 +172,21 @@ int rl_map_download_async(const rl_map* map, float* color, void* stream);
 int rl_map_upload(rl_map* map, const int32_t* flags, const int32_t* face, const float* position,
                   const float* normal, const float* color, const int32_t* photons, const float* gathered,
                   void* stream);
+/* Lightmap::expand (Lightmap.cpp:167-193) and Lightmap::blur (:196-220) on
+   the device, bit-identical to the reference's in-place scan-order loops
+   (blur runs as a one-block wavefront). */
+int rl_map_expand(rl_map* map, void* stream);
+int rl_map_blur(rl_map* map, void* stream);
+/* relight::StorageFormat (Relight.h:89-93). */
+enum { RL_RAW_HDR = 0, RL_TGA_DOUBLE_LDR = 1, RL_TGA_RGBM = 2 };
+/* The pixel buffer Lightmap::toHdr / toDoubleLdr / toRgbmLdr
+   (Lightmap.cpp:288-349) returns, encoded on the device and copied to host
+   `out` (w*h*12, w*h*3 or w*h*4 bytes; waits for `stream`).  RGBM keeps the
+   reference's row layout (pixel offset x*3 in rows of w*4 bytes); the bytes
+   the reference leaves uninitialised are 0. */
+int rl_map_encode(const rl_map* map, int format, uint8_t* out, void* stream);
+/* Lightmap::save (Lightmap.cpp:223-283): the same file, byte for byte. */
+int rl_map_save(const rl_map* map, const char* path, int format, void* stream);
 /* Set every lumel colour / photon accumulator to zero. */
 int rl_map_clear(rl_map* map, int colors, int photons, void* stream);
 /* Device pointers of the lumel arrays (SoA, [w*h] or [w*h][3]); any may be NULL. */
@@ -243,6 +258,23 @@ int rl_photonmap_gather(rl_map* photonmap, int radius, void* stream);
 int rl_bake_indirect(const rl_scene* scene, rl_map* lightmap, rl_map* const* photonmaps, int nmaps, int samples,
                      float max_distance, const float sky[3], const float ambient[3], uint64_t seed,
                      const rl_iterator* iterator, void* stream);
+
+/* ------------------------------------------------------------ OBJ ingest */
+
+/* Mesh::createFromFile -> MeshLoader::load (scene/Mesh.cpp:111-122,
+   scene/MeshLoader.cpp:44-226): Wavefront OBJ with the reference's
+   submesh commits, face forms, float-equality vertex sharing and uv clamp.
+   Host-only (no device needed).  Face indices outside the parsed arrays and
+   meshes beyond 16-bit indices fail with RL_INVALID_CALL (undefined in the
+   reference). */
+typedef struct rl_obj_mesh rl_obj_mesh;
+int rl_obj_load(const char* path, rl_obj_mesh** out);
+int rl_obj_mesh_counts(const rl_obj_mesh* mesh, int32_t* nvertices, int32_t* nindices, int32_t* nsubmeshes);
+/* positions/normals [n][3], uv_lightmap [n][2] (uv[Vertex::Lightmap]; the
+   diffuse layer is 0), indices [nindices]; any may be NULL. */
+int rl_obj_mesh_arrays(const rl_obj_mesh* mesh, float* positions, float* normals, float* uv_lightmap,
+                       int32_t* indices);
+int rl_obj_mesh_destroy(rl_obj_mesh* mesh);
 
 /* --------------------------------------------------------------- batches */
 

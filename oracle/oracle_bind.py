@@ -39,6 +39,68 @@ class Lumels(C.Structure):
                 ("normal", _P), ("color", _P), ("photons", _P), ("gathered", _P), ("mesh", _P)]
 
 
+# ------------------------------------------------------------ post-process
+
+RAW_HDR, TGA_DOUBLE_LDR, TGA_RGBM = 0, 1, 2   # relight::StorageFormat (Relight.h:89-93)
+
+
+def expand(lm: LumelMap):
+    """Lightmap::expand in place (oro_expand)."""
+    s = lm.struct()
+    oracle_lib().oro_expand(C.byref(s))
+
+
+def blur(lm: LumelMap):
+    """Lightmap::blur in place (oro_blur)."""
+    s = lm.struct()
+    oracle_lib().oro_blur(C.byref(s))
+
+
+def to_double_ldr(lm: LumelMap) -> np.ndarray:
+    out = np.zeros(lm.width * lm.height * 3, np.uint8)
+    s = lm.struct()
+    oracle_lib().oro_to_double_ldr(C.byref(s), ptr(out))
+    return out
+
+
+def to_rgbm(lm: LumelMap) -> np.ndarray:
+    """The RGBM buffer with the bytes the reference never writes left 0."""
+    out = np.zeros(lm.width * lm.height * 4, np.uint8)
+    s = lm.struct()
+    oracle_lib().oro_to_rgbm(C.byref(s), ptr(out))
+    return out
+
+
+def rgbm_written_mask(width: int, height: int) -> np.ndarray:
+    """Bytes of the RGBM buffer that Lightmap::toRgbmLdr writes: 3w + 1 of
+    every 4w-byte row (Lightmap.cpp:288-308)."""
+    m = np.zeros((height, width * 4), bool)
+    m[:, :3 * width + 1] = True
+    return m.reshape(-1)
+
+
+def save_bytes(lm: LumelMap, fmt: int) -> bytes:
+    """The file Lightmap::save (Lightmap.cpp:223-283) writes, as bytes."""
+    w, h = lm.width, lm.height
+    if fmt == RAW_HDR:
+        return np.array([w, h], np.int32).tobytes() + np.ascontiguousarray(lm.color, np.float32).tobytes()
+    ch = 3 if fmt == TGA_DOUBLE_LDR else 4
+    px = (to_double_ldr(lm) if fmt == TGA_DOUBLE_LDR else to_rgbm(lm)).reshape(-1, ch)
+    head = bytes([0, 0, 2, 0, 0, 0, 0, 0, 0, 0, 0, 0]) + bytes([w % 256, w // 256, h % 256, h // 256, ch * 8, 0])
+    order = [2, 1, 0] + ([3] if ch == 4 else [])
+    return head + np.ascontiguousarray(px[:, order]).tobytes()
+
+
+def tga_written_mask(width: int, height: int, fmt: int) -> np.ndarray:
+    """Bytes of a saved file that the reference determines (RGBM leaves
+    some pixel bytes uninitialised)."""
+    if fmt != TGA_RGBM:
+        n = 8 + width * height * 12 if fmt == RAW_HDR else 18 + width * height * 3
+        return np.ones(n, bool)
+    px = rgbm_written_mask(width, height).reshape(-1, 4)[:, [2, 1, 0, 3]].reshape(-1)
+    return np.concatenate([np.ones(18, bool), px])
+
+
 class Iterator(C.Structure):
     """rl_iterator (oracle/rl_oracle.h)."""
     _fields_ = [("kind", C.c_int32), ("first", C.c_int32), ("step", C.c_int32), ("mesh", C.c_int32)]
@@ -107,6 +169,11 @@ def _load_oracle():
         "oro_jacobi_f32": (None, [C.c_int, _P, _P, _P, _P, _P, C.c_int, _P]),
         "oro_ao_expect_f64": (None, [_P, _P, C.c_int, _P, C.c_int, C.c_float, C.c_float, C.c_uint64, _P]),
         "oro_fg_expect_f64": (None, [_P, _P, _P, C.c_int, _P, C.c_int, C.c_float, _P, _P, C.c_uint64, _P]),
+        "oro_expand": (None, [_P]),
+        "oro_blur": (None, [_P]),
+        "oro_to_double_ldr": (None, [_P, _P]),
+        "oro_to_rgbm": (None, [_P, _P]),
+        "oro_f2u8": (C.c_uint8, [C.c_float]),
         "oro_last_stats": (None, [_P, _P]),
         "oro_trace_stats": (None, [_P, C.c_int, _P, C.c_int, _P]),
     }
@@ -318,6 +385,12 @@ def _load_ref(path):
         "ref_map_lumels": (None, [_P, I, _P, _P, _P, _P, _P, _P, _P]),
         "ref_map_set_colors": (None, [_P, I, _P]),
         "ref_map_set_photons": (None, [_P, I, _P, _P]),
+        "ref_map_set_flags": (None, [_P, I, _P]),
+        "ref_load_obj": (I, [C.c_char_p, _P]),
+        "ref_obj_arrays": (None, [_P, _P, _P, _P, _P]),
+        "ref_map_expand": (None, [_P, I]),
+        "ref_map_blur": (None, [_P, I]),
+        "ref_map_save": (I, [_P, I, C.c_char_p, I]),
         "ref_bake_direct": (I, [_P, I, I, I, I]),
         "ref_bake_ao": (I, [_P, I, I, F, F, F, I, I, I]),
         "ref_emit_photons": (I, [_P, I, I, F, F, I]),
@@ -434,6 +507,24 @@ class RefScene:
         out = LumelMap(m.width, m.height)
         self.lib.ref_map_lumels(self.h, k, ptr(out.flags), ptr(out.face), ptr(out.position), ptr(out.normal),
                                 ptr(out.color), ptr(out.photons), ptr(out.gathered))
+        return out
+
+    def post_map(self, width, height, flags, color) -> int:
+        """A fresh Lightmap of the reference with the given lumel flags and
+        colours (for expand / blur / save)."""
+        k = self.lib.ref_create_map(self.h, 0, width, height)
+        self.set_map(k, flags, color)
+        return k
+
+    def set_map(self, k, flags, color):
+        flags = np.ascontiguousarray(flags, np.int32)
+        color = np.ascontiguousarray(color, np.float32)
+        self.lib.ref_map_set_flags(self.h, k, ptr(flags))
+        self.lib.ref_map_set_colors(self.h, k, ptr(color))
+
+    def map_colors(self, k, width, height):
+        out = np.zeros((width * height, 3), np.float32)
+        self.lib.ref_map_lumels(self.h, k, None, None, None, None, ptr(out), None, None)
         return out
 
     def mesh_vertices(self, inst):

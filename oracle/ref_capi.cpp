@@ -335,6 +335,51 @@ void ref_map_set_colors(void* h, int map, const float* color) {
     for (int i = 0; i < n; i++) L[i].m_color = Rgb(color[3 * i], color[3 * i + 1], color[3 * i + 2]);
 }
 
+/* Mesh::createFromFile -> MeshLoader::load (scene/Mesh.cpp:111-122,
+   scene/MeshLoader.cpp:44-226), run by the reference itself.  Returns the
+   vertex count (-1 if the file cannot be opened); the arrays (any may be
+   NULL) receive position, normal, uv[Diffuse], uv[Lightmap] per vertex and
+   the 16-bit indices. */
+static Mesh* g_obj_mesh = nullptr;
+int ref_load_obj(const char* path, int* nindices) {
+    delete g_obj_mesh;
+    g_obj_mesh = Mesh::createFromFile(path);
+    if (!g_obj_mesh) return -1;
+    if (nindices) *nindices = g_obj_mesh->indexCount();
+    return g_obj_mesh->vertexCount();
+}
+void ref_obj_arrays(float* pos, float* nrm, float* uv0, float* uv1, int* idx) {
+    Mesh* m = g_obj_mesh;
+    if (!m) return;
+    for (int i = 0; i < m->vertexCount(); i++) {
+        const Vertex& v = m->vertex(i);
+        if (pos) { pos[3 * i] = v.position.x; pos[3 * i + 1] = v.position.y; pos[3 * i + 2] = v.position.z; }
+        if (nrm) { nrm[3 * i] = v.normal.x; nrm[3 * i + 1] = v.normal.y; nrm[3 * i + 2] = v.normal.z; }
+        if (uv0) { uv0[2 * i] = v.uv[0].x; uv0[2 * i + 1] = v.uv[0].y; }
+        if (uv1) { uv1[2 * i] = v.uv[1].x; uv1[2 * i + 1] = v.uv[1].y; }
+    }
+    if (idx)
+        for (int i = 0; i < m->indexCount(); i++) idx[i] = m->index(i);
+}
+
+/* Lumel flags (Lumel::m_flags) of any map, for post-process tests on
+   arbitrary validity patterns. */
+void ref_map_set_flags(void* h, int map, const int* flags) {
+    RefCtx* c = (RefCtx*)h;
+    Lightmap* m = c->maps[map];
+    int n = m->width() * m->height();
+    Lumel* L = m->lumels();
+    for (int i = 0; i < n; i++) L[i].m_flags = flags[i];
+}
+
+/* Lightmap::expand / blur (Lightmap.cpp:167-220) and Lightmap::save
+   (:223-283) run by the reference itself. */
+void ref_map_expand(void* h, int map) { ((RefCtx*)h)->maps[map]->expand(); }
+void ref_map_blur(void* h, int map) { ((RefCtx*)h)->maps[map]->blur(); }
+int ref_map_save(void* h, int map, const char* path, int format) {
+    return ((RefCtx*)h)->maps[map]->save(path, (StorageFormat)format) ? 1 : 0;
+}
+
 /* Photon accumulators (Lumel::m_color, m_photons) of a photonmap. */
 void ref_map_set_photons(void* h, int map, const float* color, const int* photons) {
     RefCtx* c = (RefCtx*)h;

@@ -581,6 +581,84 @@ void oro_photonmap_gather(rl_lumels* pm, int radius) {
     }
 }
 
+/* ------------------------------------------------------- post-process */
+
+void oro_expand(rl_lumels* lm) {
+    int W = lm->width, H = lm->height;
+    /* Lightmap::expand (Lightmap.cpp:167-182) + fillInvalidAt (:185-193) */
+    for (int y = 1; y < H - 1; y++) {
+        for (int x = 1; x < W - 1; x++) {
+            size_t c = (size_t)y * W + x;
+            if (!(lm->flags[c] & 1)) continue;
+            const int dx[4] = {-1, -1, 1, 1}, dy[4] = {-1, 1, -1, 1};
+            for (int k = 0; k < 4; k++) {
+                size_t t = (size_t)(y + dy[k]) * W + (x + dx[k]);
+                if (lm->flags[t] & 1) continue;
+                lm->color[3 * t] = lm->color[3 * c];
+                lm->color[3 * t + 1] = lm->color[3 * c + 1];
+                lm->color[3 * t + 2] = lm->color[3 * c + 2];
+            }
+        }
+    }
+}
+
+void oro_blur(rl_lumels* lm) {
+    int W = lm->width, H = lm->height;
+    /* Lightmap::blur (Lightmap.cpp:196-220) */
+    for (int y = 1; y < H - 1; y++) {
+        for (int x = 1; x < W - 1; x++) {
+            float r = 0.0f, g = 0.0f, b = 0.0f;
+            int count = 0;
+            for (int j = y - 1; j <= y + 1; j++) {
+                for (int i = x - 1; i <= x + 1; i++) {
+                    size_t l = (size_t)j * W + i;
+                    if (lm->flags[l] & 1) {
+                        r += lm->color[3 * l]; g += lm->color[3 * l + 1]; b += lm->color[3 * l + 2];
+                        count++;
+                    }
+                }
+            }
+            if (count) {
+                float inv = 1.0f / (float)count;
+                size_t o = (size_t)y * W + x;
+                lm->color[3 * o] = r * inv; lm->color[3 * o + 1] = g * inv; lm->color[3 * o + 2] = b * inv;
+            }
+        }
+    }
+}
+
+uint8_t oro_f2u8(float v) {
+    if (!(v > -2147483648.0f && v < 2147483648.0f)) return 0;
+    return (uint8_t)(uint32_t)(int32_t)v;
+}
+
+static float min2f(float a, float b) { return a < b ? a : b; }   /* Types.h:87-89 */
+static float max2f(float a, float b) { return a > b ? a : b; }   /* Types.h:99-101 */
+
+void oro_to_double_ldr(const rl_lumels* lm, uint8_t* out) {
+    size_t n = (size_t)lm->width * lm->height;
+    /* Rgb::doubleLdr (Types.h:215-221) */
+    for (size_t i = 0; i < n; i++)
+        for (int k = 0; k < 3; k++) out[3 * i + k] = oro_f2u8(min2f(255.0f, lm->color[3 * i + k] * 0.5f * 255.0f));
+}
+
+void oro_to_rgbm(const rl_lumels* lm, uint8_t* out) {
+    int W = lm->width, H = lm->height;
+    size_t stride = (size_t)W * 4;
+    /* Lightmap::toRgbmLdr (Lightmap.cpp:288-308), Rgb::rgbm (Types.h:224-235) */
+    for (int y = 0; y < H; y++) {
+        for (int x = 0; x < W; x++) {
+            const float* c = lm->color + 3 * ((size_t)y * W + x);
+            float m = 255.0f / max2f(c[0], max2f(c[1], c[2]));
+            uint8_t* px = out + (size_t)y * stride + (size_t)x * 3;
+            px[0] = oro_f2u8(min2f(255.0f, c[0] / m * 255.0f));
+            px[1] = oro_f2u8(min2f(255.0f, c[1] / m * 255.0f));
+            px[2] = oro_f2u8(min2f(255.0f, c[2] / m * 255.0f));
+            px[3] = oro_f2u8(min2f(255.0f, m * 255.0f));
+        }
+    }
+}
+
 /* ---------------------------------------------------------- final gather */
 
 void oro_bake_indirect(const oro_ctx* c, rl_lumels* lm, const rl_lumels* photonmaps, int samples,

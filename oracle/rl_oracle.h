@@ -132,6 +132,26 @@ long long oro_emit_photons_range(const oro_ctx* c, const rl_light* lights, int n
 /* Photonmap::gather(radius) (Lightmap.cpp:376-413). */
 void oro_photonmap_gather(rl_lumels* pm, int radius);
 
+/* Lightmap::expand (Lightmap.cpp:167-193): every valid interior lumel copies
+   its colour into its invalid diagonal neighbours, in scan order (the last
+   writer wins), in place. */
+void oro_expand(rl_lumels* lm);
+/* Lightmap::blur (Lightmap.cpp:196-220): each interior texel becomes the mean
+   of the valid texels of its 3x3 window, computed in place in scan order, so
+   the window's upper row and left neighbour are already blurred. */
+void oro_blur(rl_lumels* lm);
+/* Lightmap::toDoubleLdr / toRgbmLdr (Lightmap.cpp:288-330) with
+   Rgb::doubleLdr / Rgb::rgbm (Types.h:215-235).  DoubleLdr: out[w*h*3].
+   RGBM: out[w*h*4] with the reference's pixel offset x*3 inside a row of
+   stride w*4, so each pixel's m byte is overwritten by the next pixel's r
+   and the bytes past 3w+1 of a row are never written (left as they are). */
+void oro_to_double_ldr(const rl_lumels* lm, uint8_t* out);
+void oro_to_rgbm(const rl_lumels* lm, uint8_t* out);
+/* static_cast<unsigned char>(float) as x86-64 code performs it: truncate to
+   a 32-bit integer (the out-of-range / NaN result is 0x80000000) and keep
+   the low byte. */
+uint8_t oro_f2u8(float v);
+
 /* Relight::bakeIndirectLight (baker/IndirectLight.cpp:47-75). */
 void oro_bake_indirect(const oro_ctx* c, rl_lumels* lm, const rl_lumels* photonmaps, int samples,
                        float max_distance, const float sky[3], const float ambient[3], uint64_t seed,

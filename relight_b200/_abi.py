@@ -122,9 +122,17 @@ SIGNATURES = {
     "rl_radiosity_solve": (_I, [_I, _P, _P, _P, _P, _P, _I, _P, _P]),
     "rl_radiosity_solve_noalloc": (_I, [_I, _P, _P, _P, _P, _P, _I, _P, _P]),
     "rl_radiosity_step": (_I, [_I, _I, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "rl_obj_load": (_I, [C.c_char_p, _P]),
+    "rl_obj_mesh_counts": (_I, [_P, _P, _P, _P]),
+    "rl_obj_mesh_arrays": (_I, [_P, _P, _P, _P, _P]),
+    "rl_obj_mesh_destroy": (_I, [_P]),
     "rl_batch_create": (_I, [_P, _I, _P]),
     "rl_batch_update": (_I, [_P, _P, _I, _P]),
     "rl_map_bytes": (_I, [_I, _I, _P]),
+    "rl_map_expand": (_I, [_P, _P]),
+    "rl_map_blur": (_I, [_P, _P]),
+    "rl_map_encode": (_I, [_P, _I, _P, _P]),
+    "rl_map_save": (_I, [_P, C.c_char_p, _I, _P]),
     "rl_pool_trim": (_I, [_I64]),
     "rl_pool_bytes": (_I, [_P, _P]),
     "rl_map_download_async": (_I, [_P, _P, _P]),

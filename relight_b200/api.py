@@ -183,6 +183,34 @@ class Mesh:
     def create():
         return Mesh()
 
+    @staticmethod
+    def create_from_file(file_name) -> Optional["Mesh"]:
+        """Mesh::createFromFile (scene/Mesh.cpp:111-122): a Wavefront OBJ
+        read with MeshLoader's rules (rl_obj_load), uvs in the lightmap
+        layer, no material; None if the file cannot be opened."""
+        import ctypes as C
+        import os
+        from ._abi import check, lib
+        if not os.path.isfile(file_name):
+            return None
+        h = C.c_void_p()
+        check(lib().rl_obj_load(str(file_name).encode(), C.byref(h)))
+        try:
+            nv, ni, ns = C.c_int32(), C.c_int32(), C.c_int32()
+            check(lib().rl_obj_mesh_counts(h, C.byref(nv), C.byref(ni), C.byref(ns)))
+            pos = np.zeros((nv.value, 3), np.float32)
+            nrm = np.zeros((nv.value, 3), np.float32)
+            uv = np.zeros((nv.value, 2), np.float32)
+            idx = np.zeros(ni.value, np.int32)
+            ptr = lambda a: C.c_void_p(a.ctypes.data)
+            check(lib().rl_obj_mesh_arrays(h, ptr(pos), ptr(nrm), ptr(uv), ptr(idx)))
+        finally:
+            lib().rl_obj_mesh_destroy(h)
+        m = Mesh()
+        if nv.value:
+            m.add_faces(pos, nrm, None, uv, idx)
+        return m
+
     def vertex_count(self):
         return int(self.positions.shape[0])
 

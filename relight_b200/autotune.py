@@ -86,3 +86,41 @@ def tune(run, kernel="indirect", refills=REFILLS, blocks=BLOCKS, widths=(2,), sp
     set_width(best[2])
     set_speculative(best[3])
     return {"refill": best[0], "block": best[1], "width": best[2], "speculative": best[3], "ms": table[best]}, table
+
+
+def tune_batch(jobs, stream=None, refills=(16, 24, 32), blocks=(64, 128), sample=8, reps=2, reset=None):
+    """Tune the batch kernels' refill threshold (rays in flight per warp)
+    and block size, per pass kind, on every `sample`-th job of `jobs` (a
+    list of batch.BakeJob).  Each candidate builds a batch (the launch shape
+    is fixed when a batch is made) and times one launch per rep; `reset()`
+    (optional) restores the lightmaps between launches.  The best setting
+    per kind is left applied, so batches made afterwards use it.  Returns
+    {kind: (best, table)}."""
+    import torch
+    from . import batch as B
+    st = stream or torch.cuda.current_stream()
+    out = {}
+    for kind, name in ((B.AO, "ao"), (B.INDIRECT, "indirect")):
+        sub = [j for j in jobs if j.kind == kind][::max(sample, 1)]
+        if not sub:
+            continue
+        table = {}
+        for refill, block in itertools.product(refills, blocks):
+            set(refill, block, name)
+            b = B.Batch(sub)
+            ms = []
+            for _ in range(reps + 1):
+                if reset:
+                    reset()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(st)
+                b.launch(st.cuda_stream)
+                e1.record(st)
+                e1.synchronize()
+                ms.append(e0.elapsed_time(e1))
+            b.close()
+            table[(refill, block)] = min(ms[1:])
+        best = min(table, key=table.get)
+        set(best[0], best[1], name)
+        out[name] = ({"refill": best[0], "block": best[1], "ms": table[best]}, table)
+    return out

@@ -20,7 +20,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "librelight_b200.so")
 
-SOURCES = ["rl_capi.cu", "rl_lbvh.cu", "rl_bvh.cpp", os.path.join("host", "relight_api.cpp")]
+SOURCES = ["rl_capi.cu", "rl_lbvh.cu", "rl_bvh.cpp", os.path.join("host", "relight_api.cpp"),
+           os.path.join("host", "obj_loader.cpp")]
 HEADERS = ["rl_device.cuh", "rl_bvh.h", "rl_lbvh.h", os.path.join("..", "..", "include", "relight_b200.h"),
            os.path.join("..", "..", "include", "relight", "Relight.h")]
 
@@ -60,11 +61,11 @@ def build(force: bool = False, verbose: bool = False) -> str:
     return OUT
 
 
-def build_cpp_example(out_dir: str) -> str:
-    """Compile tests/cpp/bake_room.cpp, a Relight C++ program, against the
-    C++ API (include/relight/Relight.h) and this library."""
-    src = os.path.join(ROOT, "tests", "cpp", "bake_room.cpp")
-    exe = os.path.join(out_dir, "bake_room")
+def build_cpp_example(out_dir: str, name: str = "bake_room") -> str:
+    """Compile tests/cpp/<name>.cpp, a Relight C++ program, against the C++
+    API (include/relight/Relight.h) and this library."""
+    src = os.path.join(ROOT, "tests", "cpp", name + ".cpp")
+    exe = os.path.join(out_dir, name)
     cmd = [os.environ.get("CXX", "g++"), "-std=c++17", "-O2", "-I", os.path.join(ROOT, "include"), src,
            "-L", HERE, "-lrelight_b200", "-Wl,-rpath," + HERE, "-o", exe]
     r = subprocess.run(cmd, capture_output=True, text=True)

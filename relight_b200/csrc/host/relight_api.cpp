@@ -71,6 +71,27 @@ void Mesh::updateBounds() {
     for (const Vertex& v : m_vertices) m_bounds.add(v.position);
 }
 
+Mesh* Mesh::createFromFile(const std::string& fileName) {
+    rl_obj_mesh* obj = nullptr;
+    if (rl_obj_load(fileName.c_str(), &obj) != RL_OK) return nullptr;
+    int32_t nv = 0, ni = 0;
+    rl_obj_mesh_counts(obj, &nv, &ni, nullptr);
+    std::vector<float> pos(3 * (size_t)nv), nrm(3 * (size_t)nv), uv(2 * (size_t)nv);
+    std::vector<int32_t> idx((size_t)ni);
+    rl_obj_mesh_arrays(obj, pos.data(), nrm.data(), uv.data(), idx.data());
+    rl_obj_mesh_destroy(obj);
+    VertexBuffer vertices((size_t)nv);
+    for (int32_t i = 0; i < nv; i++) {
+        vertices[i].position = Vec3(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]);
+        vertices[i].normal = Vec3(nrm[3 * i], nrm[3 * i + 1], nrm[3 * i + 2]);
+        vertices[i].uv[Vertex::Lightmap] = Uv(uv[2 * i], uv[2 * i + 1]);
+    }
+    IndexBuffer indices(idx.begin(), idx.end());
+    Mesh* m = new Mesh;
+    m->addFaces(vertices, indices, nullptr);
+    return m;
+}
+
 void Mesh::addFaces(const VertexBuffer& vertices, const IndexBuffer& indices, const Material* material) {
     size_t base = m_vertices.size();
     for (Index i : indices) m_indices.push_back((Index)(i + base));
@@ -252,7 +273,27 @@ float* Lightmap::toHdr() {
     return px;
 }
 
+void Lightmap::expand() {
+    if (!m_device) return;  // never rasterised: no valid lumel to spread
+    beforeDevice();
+    rl_map_expand(m_device, nullptr);
+    cudaStreamSynchronize(nullptr);
+    afterDevice();
+}
+
+void Lightmap::blur() {
+    if (!m_device) return;
+    beforeDevice();
+    rl_map_blur(m_device, nullptr);
+    cudaStreamSynchronize(nullptr);
+    afterDevice();
+}
+
 bool Lightmap::save(const std::string& fileName, StorageFormat format) {
+    if (m_device) {
+        beforeDevice();
+        return rl_map_save(m_device, fileName.c_str(), (int)format, nullptr) == RL_OK;
+    }
     if (format != RawHdr) return false;
     FILE* f = fopen(fileName.c_str(), "wb");
     if (!f) return false;

@@ -141,6 +141,9 @@ struct rl_map {
     }
 };
 
+// Error entry for the host-only sources of the library (e.g. the OBJ loader).
+int rl_internal_fail(int code, const char* msg) { return fail(code, "%s", msg); }
+
 extern "C" int rl_last_error(char* buf, size_t len) {
     if (buf && len) {
         snprintf(buf, len, "%s", g_error.c_str());
@@ -1638,6 +1641,184 @@ extern "C" int rl_radiosity_solve(int n, const int64_t* d_row_ptr, const int32_t
         std::swap(src, dst);
     }
     if (src != d_B) CK(cudaMemcpyAsync(d_B, src, 12 * (size_t)n, cudaMemcpyDeviceToDevice, st));
+    return RL_OK;
+}
+
+// ---------------------------------------------------------- post-process
+
+// Lightmap::expand (Lightmap.cpp:167-193).  The reference walks the interior
+// in scan order and every valid lumel copies its colour into its invalid
+// diagonal neighbours; only invalid texels change, so each invalid texel
+// ends with the colour of the LAST valid interior writer in scan order:
+// (x+1, y+1), else (x-1, y+1), else (x+1, y-1), else (x-1, y-1).
+__global__ void k_expand(DevMap m) {
+    const int W = m.width, H = m.height;
+    const long long n = (long long)W * H;
+    const int dx[4] = {1, -1, 1, -1}, dy[4] = {1, 1, -1, -1};
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        if (m.flags[t] & 1) continue;
+        int x = (int)(t % W), y = (int)(t / W);
+        for (int k = 0; k < 4; k++) {
+            int cx = x + dx[k], cy = y + dy[k];
+            if (cx < 1 || cx > W - 2 || cy < 1 || cy > H - 2) continue;
+            long long c = (long long)cy * W + cx;
+            if (!(m.flags[c] & 1)) continue;
+            m.color[3 * t] = m.color[3 * c];
+            m.color[3 * t + 1] = m.color[3 * c + 1];
+            m.color[3 * t + 2] = m.color[3 * c + 2];
+            break;
+        }
+    }
+}
+
+// Lightmap::blur (Lightmap.cpp:196-220).  The reference blurs in place in
+// scan order, so texel (x, y) reads the already-blurred (x-1..x+1, y-1) and
+// (x-1, y) and the original rest of its window.  Every such input has a
+// smaller t = (x-1) + 2(y-1), and texels of one t never share a window, so
+// one block walks t = 0, 1, ... with a barrier per step (a wavefront), each
+// thread owning rows y = 1 + tid, 1 + tid + blockDim, ...  Sums run in the
+// reference's window order, so the result is bit-identical.
+__global__ void __launch_bounds__(1024) k_blur(DevMap m) {
+    const int W = m.width, H = m.height;
+    if (W < 3 || H < 3) return;
+    const long long T = (long long)(W - 3) + 2LL * (H - 3);
+    for (long long t = 0; t <= T; t++) {
+        for (int y = 1 + threadIdx.x; y <= H - 2; y += blockDim.x) {
+            long long x = t - 2LL * (y - 1) + 1;
+            if (x < 1 || x > W - 2) continue;
+            float r = 0.0f, g = 0.0f, b = 0.0f;
+            int count = 0;
+            for (int j = y - 1; j <= y + 1; j++) {
+                for (long long i = x - 1; i <= x + 1; i++) {
+                    long long l = (long long)j * W + i;
+                    if (m.flags[l] & 1) {
+                        r += m.color[3 * l]; g += m.color[3 * l + 1]; b += m.color[3 * l + 2];
+                        count++;
+                    }
+                }
+            }
+            if (count) {
+                float inv = 1.0f / (float)count;
+                long long o = (long long)y * W + x;
+                m.color[3 * o] = r * inv; m.color[3 * o + 1] = g * inv; m.color[3 * o + 2] = b * inv;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// static_cast<unsigned char>(float) as x86-64 code performs it: truncation
+// to a 32-bit integer (0x80000000 when out of range or NaN), low byte kept.
+__device__ __forceinline__ uint8_t f2u8(float v) {
+    if (!(v > -2147483648.0f && v < 2147483648.0f)) return 0;
+    return (uint8_t)(uint32_t)__float2int_rz(v);
+}
+__device__ __forceinline__ float min2f(float a, float b) { return a < b ? a : b; }  // Types.h:87-89
+__device__ __forceinline__ float max2f(float a, float b) { return a > b ? a : b; }  // Types.h:99-101
+
+// Lightmap::toDoubleLdr / toRgbmLdr (Lightmap.cpp:288-330) with
+// Rgb::doubleLdr / Rgb::rgbm (Types.h:215-235), into the reference's pixel
+// buffer layout.  RGBM keeps the reference's pixel offset x*3 inside a row
+// of stride w*4: pixel x writes bytes 3x..3x+2 and, being overwritten there
+// by pixel x+1's r, its m byte survives only for the last pixel of a row.
+__global__ void k_encode(DevMap m, int format, uint8_t* out) {
+    const int W = m.width;
+    const long long n = (long long)W * m.height;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const float* c = m.color + 3 * i;
+        if (format == 1) {
+            for (int k = 0; k < 3; k++) out[3 * i + k] = f2u8(min2f(255.0f, c[k] * 0.5f * 255.0f));
+        } else {
+            long long x = i % W, y = i / W;
+            float mm = 255.0f / max2f(c[0], max2f(c[1], c[2]));
+            uint8_t* px = out + y * (4LL * W) + 3 * x;
+            px[0] = f2u8(min2f(255.0f, c[0] / mm * 255.0f));
+            px[1] = f2u8(min2f(255.0f, c[1] / mm * 255.0f));
+            px[2] = f2u8(min2f(255.0f, c[2] / mm * 255.0f));
+            if (x == W - 1) px[3] = f2u8(min2f(255.0f, mm * 255.0f));
+        }
+    }
+}
+
+static int grid_for(long long n, int block) {
+    long long g = (n + block - 1) / block;
+    return (int)std::max<long long>(1, std::min<long long>(g, 148LL * 32));
+}
+
+extern "C" int rl_map_expand(rl_map* m, void* stream) {
+    if (!m) return fail(RL_INVALID_CALL, "null map");
+    long long n = (long long)m->dev.width * m->dev.height;
+    k_expand<<<grid_for(n, 256), 256, 0, S(stream)>>>(m->dev);
+    CK_LAUNCH("k_expand");
+    return RL_OK;
+}
+
+extern "C" int rl_map_blur(rl_map* m, void* stream) {
+    if (!m) return fail(RL_INVALID_CALL, "null map");
+    k_blur<<<1, 1024, 0, S(stream)>>>(m->dev);
+    CK_LAUNCH("k_blur");
+    return RL_OK;
+}
+
+static long long encoded_bytes(const rl_map* m, int format) {
+    long long n = (long long)m->dev.width * m->dev.height;
+    return format == 0 ? 12 * n : format == 1 ? 3 * n : 4 * n;
+}
+
+extern "C" int rl_map_encode(const rl_map* m, int format, uint8_t* out, void* stream) {
+    if (!m || !out || format < 0 || format > 2) return fail(RL_INVALID_CALL, "rl_map_encode: bad arguments");
+    cudaStream_t st = S(stream);
+    long long bytes = encoded_bytes(m, format), n = (long long)m->dev.width * m->dev.height;
+    if (format == 0) {
+        CK(cudaMemcpyAsync(out, m->dev.color, bytes, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        return RL_OK;
+    }
+    uint8_t* d = nullptr;
+    if (int rc = pool_alloc((void**)&d, (size_t)bytes, st)) return rc;
+    int rc = RL_OK;
+    cudaError_t e = cudaMemsetAsync(d, 0, bytes, st);
+    if (e == cudaSuccess) {
+        k_encode<<<grid_for(n, 256), 256, 0, st>>>(m->dev, format, d);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, d, bytes, cudaMemcpyDeviceToHost, st);
+    cudaFreeAsync(d, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) rc = fail(RL_CUDA_ERROR, "rl_map_encode: %s", cudaGetErrorString(e));
+    return rc;
+}
+
+// Lightmap::save (Lightmap.cpp:223-283): RawHdr = width, height (int32)
+// and the colours; TGA = the 18-byte uncompressed true-colour header and
+// each pixel's bytes 2, 1, 0 (and 3 for RGBM) of the encoded buffer.
+extern "C" int rl_map_save(const rl_map* m, const char* path, int format, void* stream) {
+    if (!m || !path || format < 0 || format > 2) return fail(RL_INVALID_CALL, "rl_map_save: bad arguments");
+    std::vector<uint8_t> buf((size_t)encoded_bytes(m, format));
+    if (int rc = rl_map_encode(m, format, buf.data(), stream)) return rc;
+    FILE* f = fopen(path, "wb");
+    if (!f) return fail(RL_INVALID_CALL, "rl_map_save: cannot open %s", path);
+    int W = m->dev.width, H = m->dev.height;
+    bool ok = true;
+    if (format == 0) {
+        ok = fwrite(&W, sizeof(int), 1, f) == 1 && fwrite(&H, sizeof(int), 1, f) == 1 &&
+             fwrite(buf.data(), 1, buf.size(), f) == buf.size();
+    } else {
+        int ch = format == 1 ? 3 : 4;
+        uint8_t head[18] = {0, 0, 2, 0, 0, 0, 0, 0, 0, 0, 0, 0, (uint8_t)(W % 256), (uint8_t)(W / 256),
+                            (uint8_t)(H % 256), (uint8_t)(H / 256), (uint8_t)(ch * 8), 0};
+        std::vector<uint8_t> px(buf.size());
+        size_t n = (size_t)W * H;
+        for (size_t i = 0; i < n; i++) {
+            const uint8_t* s = &buf[i * ch];
+            uint8_t* d = &px[i * ch];
+            d[0] = s[2]; d[1] = s[1]; d[2] = s[0];
+            if (ch == 4) d[3] = s[3];
+        }
+        ok = fwrite(head, 1, 18, f) == 18 && fwrite(px.data(), 1, px.size(), f) == px.size();
+    }
+    if (fclose(f) != 0) ok = false;
+    if (!ok) return fail(RL_INVALID_CALL, "rl_map_save: write to %s failed", path);
     return RL_OK;
 }
 

@@ -103,6 +103,26 @@ class DeviceMap:
         check(lib().rl_map_download(self.handle, *args, stream))
         return out
 
+    def expand(self, stream=None):
+        """Lightmap::expand on the device (rl_map_expand)."""
+        check(lib().rl_map_expand(self.handle, stream))
+
+    def blur(self, stream=None):
+        """Lightmap::blur on the device (rl_map_blur)."""
+        check(lib().rl_map_blur(self.handle, stream))
+
+    def encode(self, fmt: int, stream=None) -> np.ndarray:
+        """The reference's pixel buffer for a StorageFormat (0 RawHdr floats
+        as bytes, 1 DoubleLdr, 2 RGBM), encoded on the device (rl_map_encode)."""
+        n = self.width * self.height
+        out = np.zeros(n * (12 if fmt == 0 else 3 if fmt == 1 else 4), np.uint8)
+        check(lib().rl_map_encode(self.handle, int(fmt), C.c_void_p(out.ctypes.data), stream))
+        return out
+
+    def save(self, path: str, fmt: int, stream=None):
+        """Lightmap::save: the reference's file, byte for byte (rl_map_save)."""
+        check(lib().rl_map_save(self.handle, str(path).encode(), int(fmt), stream))
+
     def download_color_async(self, out_ptr: int, stream=None):
         """Copy the colours ([w*h][3] float32) to host memory at `out_ptr` in
         stream order, without waiting (rl_map_download_async)."""
@@ -281,6 +301,24 @@ def lumels(lightmap: Lightmap, stream=None):
     if lightmap._device is None:
         raise RuntimeError("the lightmap has not been baked yet")
     return lightmap._device.download(stream)
+
+
+RAW_HDR, TGA_DOUBLE_LDR, TGA_RGBM = 0, 1, 2   # relight::StorageFormat (Relight.h:89-93)
+
+
+def expand(lightmap: Lightmap, stream=None):
+    """Lightmap::expand (Lightmap.cpp:167-193) on the baked lightmap."""
+    lightmap._device.expand(stream)
+
+
+def blur(lightmap: Lightmap, stream=None):
+    """Lightmap::blur (Lightmap.cpp:196-220) on the baked lightmap."""
+    lightmap._device.blur(stream)
+
+
+def save(lightmap: Lightmap, path: str, fmt: int = RAW_HDR, stream=None):
+    """Lightmap::save (Lightmap.cpp:223-283)."""
+    lightmap._device.save(path, fmt, stream)
 
 
 def to_hdr(lightmap: Lightmap, stream=None):

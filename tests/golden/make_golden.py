@@ -14,6 +14,12 @@ Every fixture is a deterministic output of the reference's code:
                     square and non-square maps.
   ff_room24.npz     RadiosityBuilder::build(0.1) on a 24x24-texel
                     radiancemap room: form-factor CSR and patch positions.
+  obj.npz           Mesh::createFromFile (MeshLoader) on the synthetic OBJ
+                    files of obj_texts(): vertices, lightmap uvs, indices.
+  post.npz          Lightmap::expand, Lightmap::blur and the files
+                    Lightmap::save writes (RawHdr, TgaDoubleLdr, TgaRgbm)
+                    for seeded lumel flags and colours (NaN, inf and
+                    negative colours included) on four map shapes.
 The inputs are rebuilt from relight_b200.scenes with the same seeds.
 """
 import os
@@ -46,8 +52,114 @@ def gather_inputs(W, H, seed):
     return color, photons
 
 
+def obj_texts():
+    """Synthetic OBJ files exercising MeshLoader's rules: submeshes (v / vt /
+    vn blocks after faces), quads (first triangle only), shared and -0.0 /
+    0.0 vertices, uvs outside [0, 1], octal / hex / signed indices, CRLF
+    endings, no final newline, position-only faces."""
+    rng = np.random.default_rng(42)
+    texts = {}
+    # two objects, each with its own v / vt / vn blocks, triangles and quads
+    lines = []
+    base_v = base_t = base_n = 0
+    for obj in range(2):
+        nv = 12
+        lines.append(f"o part{obj}")
+        for _ in range(nv):
+            x, y, z = rng.uniform(-3, 3, 3)
+            lines.append(f"v {x:.6f} {y:.6f} {z:.6f}")
+        for _ in range(nv):
+            u, v = rng.uniform(-0.3, 1.3, 2)
+            lines.append(f"vt {u:.5f} {v:.5f}")
+        for _ in range(4):
+            n = rng.normal(size=3)
+            n /= np.linalg.norm(n)
+            lines.append(f"vn {n[0]:.4f} {n[1]:.4f} {n[2]:.4f}")
+        for f in range(16):
+            k = 4 if f % 5 == 0 else 3
+            vs = rng.choice(nv, k, replace=False) + 1 + base_v
+            ts = rng.choice(nv, k, replace=False) + 1 + base_t
+            ns = rng.integers(0, 4, k) + 1 + base_n
+            lines.append("f " + " ".join(f"{a}/{b}/{c}" for a, b, c in zip(vs, ts, ns)))
+        base_v += nv; base_t += nv; base_n += 4
+    texts["objects"] = "\n".join(lines) + "\n"
+    # shared corners, -0.0 vs 0.0, integer forms, CRLF, no final newline
+    texts["shared"] = ("v 0 0 0\r\nv -0.0 0 1\r\nv 1 0 0\r\nv 0.0 0 1\r\nv 1 1 1e-3\r\n"
+                       "vt 0.5 0.5\r\nvt 2 -1\r\nvn 0 1 0\r\nvn -0 1 0\r\n"
+                       "f 1/1/1 2/1/1 3/2/1\r\nf 1/1/1 4/1/2 3/2/1\r\nf 01/1/1 0x3/2/1 +5/1/2\r\n"
+                       "f 2/1/1 4/1/1 5/2/2")
+    # position-only faces
+    texts["plain"] = "v 0 0 0\nv 1 0 0\nv 0 1 0\nv 1 1 0\nf 1 2 3\nf 2 4 3\nf 3 2 1 4\n"
+    return texts
+
+
+def obj_fixture():
+    import tempfile
+    from oracle_bind import ref_lib
+    L = ref_lib()
+    g = {}
+    for name, text in obj_texts().items():
+        fd, path = tempfile.mkstemp(suffix=".obj")
+        with os.fdopen(fd, "wb") as f:
+            f.write(text.encode())
+        ni = __import__("ctypes").c_int()
+        nv = L.ref_load_obj(path.encode(), __import__("ctypes").byref(ni))
+        os.unlink(path)
+        arr = {k: np.zeros(shape, np.float32) for k, shape in
+               (("pos", (nv, 3)), ("nrm", (nv, 3)), ("uv0", (nv, 2)), ("uv1", (nv, 2)))}
+        idx = np.zeros(ni.value, np.int32)
+        L.ref_obj_arrays(ptr(arr["pos"]), ptr(arr["nrm"]), ptr(arr["uv0"]), ptr(arr["uv1"]), ptr(idx))
+        for k, v in arr.items():
+            g[f"{name}_{k}"] = v
+        g[f"{name}_idx"] = idx
+    np.savez_compressed(os.path.join(HERE, "obj.npz"), **g)
+    return len(g)
+
+
+POST_SHAPES = [(37, 23, 0.3), (64, 64, 0.6), (2, 5, 0.5), (48, 40, 0.85)]
+
+
+def post_inputs(W, H, density, seed):
+    rng = np.random.default_rng(seed)
+    flags = (rng.random(W * H) < density).astype(np.int32)
+    color = rng.uniform(-0.5, 3.0, (W * H, 3)).astype(np.float32)
+    color[rng.random(W * H) < 0.02] = np.nan
+    color[rng.random(W * H) < 0.02, 1] = np.inf
+    color[rng.random(W * H) < 0.02, 2] = -1e10
+    return flags, color
+
+
+def post_fixture():
+    import tempfile
+    w = scenes.room_scene(size=16)
+    ref = RefScene(w.scene)
+    g = {}
+    for c, (W, H, dens) in enumerate(POST_SHAPES):
+        flags, color = post_inputs(W, H, dens, 100 + c)
+        for op in ("expand", "blur"):
+            k = ref.post_map(W, H, flags, color)
+            getattr(ref.lib, "ref_map_" + op)(ref.h, k)
+            g[f"{op}{c}"] = ref.map_colors(k, W, H)
+        for fmt in (0, 1, 2):
+            k = ref.post_map(W, H, flags, color)
+            fd, path = tempfile.mkstemp()
+            os.close(fd)
+            ref.lib.ref_map_save(ref.h, k, path.encode(), fmt)
+            with open(path, "rb") as f:
+                g[f"file{c}_{fmt}"] = np.frombuffer(f.read(), np.uint8)
+            os.unlink(path)
+    np.savez_compressed(os.path.join(HERE, "post.npz"), **g)
+    return len(POST_SHAPES)
+
+
 def main():
     out = {}
+    if sys.argv[1:] == ["post"]:
+        print({"post": post_fixture()})
+        return
+    if sys.argv[1:] == ["obj"]:
+        print({"obj": obj_fixture()})
+        return
     # room, direct light
     w = scenes.room_scene(size=64)
     ref = RefScene(w.scene)
@@ -82,6 +194,8 @@ def main():
     row, cols, vals, ppos, pnrm = ref.radiosity(0.1)
     np.savez_compressed(os.path.join(HERE, "ff_room24.npz"), row=row, cols=cols, vals=vals, pos=ppos, nrm=pnrm)
     out["ff_room24"] = int(len(cols))
+    out["post"] = post_fixture()
+    out["obj"] = obj_fixture()
     print(out)
 
 

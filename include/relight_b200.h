@@ -276,6 +276,30 @@ int rl_obj_mesh_arrays(const rl_obj_mesh* mesh, float* positions, float* normals
                        int32_t* indices);
 int rl_obj_mesh_destroy(rl_obj_mesh* mesh);
 
+/* ------------------------------------------------------------- denoiser */
+
+/* Building blocks of the lightmap denoiser (no reference counterpart: the
+   reference has no denoiser).  Tensors are device NHWC BF16 arrays whose
+   channel stride is a multiple of 16; convolutions run on the tensor cores
+   (tcgen05, FP32 accumulation).  `d_err` (device int, may be NULL) gets a
+   nonzero bit if a kernel's bounded wait ran out.
+
+   rl_dn_conv3x3: out = act(conv3x3(concat(in0, in1)) + bias) with zero
+   padding; c0 / c1 are the inputs' stored channel counts (multiples of 8).
+   `weights` is BF16 [ncols][9][64*(ceil(c0/64) + ceil(c1/64))], tap =
+   3*(dy+1) + (dx+1), each input segment's channels starting at a multiple
+   of 64 (zero-padded).  Accumulator columns
+   [outK_c0, outK_c0 + outK_cn) go to outK (channel stride outK_cs), times
+   (maskK > 0) when maskK is given; in1/out1 may be NULL. */
+int rl_dn_conv3x3(const void* in0, int c0, const void* in1, int c1, int width, int height, int images,
+                  const void* weights, int ncols, const float* bias, int relu, void* out0, int out0_c0,
+                  int out0_cn, int out0_cs, const void* mask0, void* out1, int out1_c0, int out1_cn, int out1_cs,
+                  const void* mask1, int* d_err, void* stream);
+/* dw[co][tap][ci_off + ci] += sum_p grad[p][co] * in[p + offset(tap)][ci]
+   (FP32, accumulated), co < cout <= 128, ci < cin. */
+int rl_dn_conv3x3_wgrad(const void* grad, int cout, int grad_cs, const void* in, int cin, int in_cs, int width,
+                        int height, int images, float* dw, int ci_off, int ci_total, int* d_err, void* stream);
+
 /* --------------------------------------------------------------- batches */
 
 /* Many bake jobs — any scenes, lightmaps, passes — in one persistent launch

@@ -126,6 +126,9 @@ SIGNATURES = {
     "rl_obj_mesh_counts": (_I, [_P, _P, _P, _P]),
     "rl_obj_mesh_arrays": (_I, [_P, _P, _P, _P, _P]),
     "rl_obj_mesh_destroy": (_I, [_P]),
+    "rl_dn_conv3x3": (_I, [_P, _I, _P, _I, _I, _I, _I, _P, _I, _P, _I, _P, _I, _I, _I, _P, _P, _I, _I, _I, _P,
+                           _P, _P]),
+    "rl_dn_conv3x3_wgrad": (_I, [_P, _I, _I, _P, _I, _I, _I, _I, _I, _P, _I, _I, _P, _P]),
     "rl_batch_create": (_I, [_P, _I, _P]),
     "rl_batch_update": (_I, [_P, _P, _I, _P]),
     "rl_map_bytes": (_I, [_I, _I, _P]),

@@ -144,6 +144,11 @@ struct rl_map {
 // Error entry for the host-only sources of the library (e.g. the OBJ loader).
 int rl_internal_fail(int code, const char* msg) { return fail(code, "%s", msg); }
 
+// Device views of handles, for the library's other translation units.
+const DevMap* rl_internal_map(const rl_map* m) { return m ? &m->dev : nullptr; }
+const DevScene* rl_internal_scene(const rl_scene* s) { return s ? &s->dev : nullptr; }
+int rl_internal_pool_alloc(void** p, size_t bytes, cudaStream_t st);
+
 extern "C" int rl_last_error(char* buf, size_t len) {
     if (buf && len) {
         snprintf(buf, len, "%s", g_error.c_str());
@@ -454,6 +459,8 @@ static int pool_alloc(void** p, size_t bytes, cudaStream_t st) {
                     cudaGetErrorString(e));
     return RL_OK;
 }
+
+int rl_internal_pool_alloc(void** p, size_t bytes, cudaStream_t st) { return pool_alloc(p, bytes, st); }
 
 extern "C" int rl_pool_trim(int64_t keep_bytes) {
     cudaMemPool_t pool;

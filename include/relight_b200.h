@@ -300,6 +300,38 @@ int rl_dn_conv3x3(const void* in0, int c0, const void* in1, int c1, int width, i
 int rl_dn_conv3x3_wgrad(const void* grad, int cout, int grad_cs, const void* in, int cin, int in_cs, int width,
                         int height, int images, float* dw, int ci_off, int ci_total, int* d_err, void* stream);
 
+/* The denoiser network: 8 convolutions over 4 levels (32, 64, 96, 128
+   channels; 2x2 average pooling, nearest upsampling, skip concatenation),
+   input features [h][w][16] = (log1p noisy rgb, normal, albedo, valid, 0),
+   output = residual on log1p rgb.  Parameters are FP32 masters updated by
+   Adam; the convolutions run in BF16 on the tensor cores. */
+typedef struct rl_denoiser rl_denoiser;
+int rl_denoiser_create(uint64_t seed, rl_denoiser** out);
+int rl_denoiser_destroy(rl_denoiser* dn);
+int rl_denoiser_param_count(const rl_denoiser* dn, int64_t* count);
+/* Per layer: weights [cout][9][k] (k = input channels padded per segment to
+   64) then biases [cout], as one FP32 host array. */
+int rl_denoiser_get_params(const rl_denoiser* dn, float* host);
+int rl_denoiser_set_params(rl_denoiser* dn, const float* host);
+int rl_denoiser_get_grads(rl_denoiser* dn, float* host);
+/* Features of a baked lightmap (d_x: BF16 [h][w][16]) and training targets
+   (d_t: FP32 [h][w][4] = log1p rgb, valid). */
+int rl_denoiser_features(const rl_scene* scene, const rl_map* lightmap, void* d_x, void* stream);
+int rl_denoiser_targets(const rl_map* lightmap, float* d_t, void* stream);
+/* One Adam step on a batch of square patches; *d_loss += the batch's mean L1
+   (log space) when d_loss is not NULL.  lr < 0: accumulate the gradients
+   only, for rl_denoiser_get_grads (which returns and clears them). */
+int rl_denoiser_train_step(rl_denoiser* dn, const void* d_x, const float* d_t, int batch, int patch, float lr,
+                           float* d_loss, void* stream);
+/* Denoise a lightmap in place: colour = base + expm1(prediction) on valid
+   lumels (d_base [w*h][3] or NULL for 0). */
+int rl_denoiser_apply(rl_denoiser* dn, const rl_scene* scene, rl_map* lightmap, const float* d_base, void* stream);
+/* Raw network output (BF16 [n][h][w][16]) for features d_x. */
+int rl_denoiser_forward(rl_denoiser* dn, const void* d_x, int images, int height, int width, void* d_y,
+                        void* stream);
+/* Bits set by bounded waits that ran out in the denoiser's kernels (0 = none). */
+int rl_denoiser_status(rl_denoiser* dn, int* flags);
+
 /* --------------------------------------------------------------- batches */
 
 /* Many bake jobs — any scenes, lightmaps, passes — in one persistent launch

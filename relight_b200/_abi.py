@@ -129,6 +129,18 @@ SIGNATURES = {
     "rl_dn_conv3x3": (_I, [_P, _I, _P, _I, _I, _I, _I, _P, _I, _P, _I, _P, _I, _I, _I, _P, _P, _I, _I, _I, _P,
                            _P, _P]),
     "rl_dn_conv3x3_wgrad": (_I, [_P, _I, _I, _P, _I, _I, _I, _I, _I, _P, _I, _I, _P, _P]),
+    "rl_denoiser_create": (_I, [_U64, _P]),
+    "rl_denoiser_destroy": (_I, [_P]),
+    "rl_denoiser_param_count": (_I, [_P, _P]),
+    "rl_denoiser_get_params": (_I, [_P, _P]),
+    "rl_denoiser_set_params": (_I, [_P, _P]),
+    "rl_denoiser_get_grads": (_I, [_P, _P]),
+    "rl_denoiser_features": (_I, [_P, _P, _P, _P]),
+    "rl_denoiser_targets": (_I, [_P, _P, _P]),
+    "rl_denoiser_train_step": (_I, [_P, _P, _P, _I, _I, _F, _P, _P]),
+    "rl_denoiser_apply": (_I, [_P, _P, _P, _P, _P]),
+    "rl_denoiser_forward": (_I, [_P, _P, _I, _I, _I, _P, _P]),
+    "rl_denoiser_status": (_I, [_P, _P]),
     "rl_batch_create": (_I, [_P, _I, _P]),
     "rl_batch_update": (_I, [_P, _P, _I, _P]),
     "rl_map_bytes": (_I, [_I, _I, _P]),

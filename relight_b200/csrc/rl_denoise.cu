@@ -594,3 +594,666 @@ extern "C" int rl_dn_conv3x3_wgrad(const void* grad, int cout, int grad_cs, cons
     }
     return RL_OK;
 }
+
+// ================================================================ network
+//
+//   x (16: log1p noisy rgb, normal, albedo, valid)
+//   e0 = relu(c0(x))            32  full       p0 = pool(e0)
+//   e1 = relu(c1(p0))           64  1/2        p1 = pool(e1)
+//   e2 = relu(c2(p1))           96  1/4        p2 = pool(e2)
+//   e3 = relu(c3(p2))          128  1/8
+//   d2 = relu(c4(up(e3), e2))   96  1/4
+//   d1 = relu(c5(up(d2), e1))   64  1/2
+//   d0 = relu(c6(up(d1), e0))   32  full
+//   y  = c7(d0)                  3  full;   prediction = y + log1p(noisy)
+//
+// Loss: mean |prediction - log1p(clean)| over valid texels (L1 in log space).
+
+namespace {
+
+constexpr int kFeat = 16;
+
+__device__ __forceinline__ float bf(bf16 v) { return __bfloat162float(v); }
+
+// 2x2 average pooling; odd edges average the children that exist.
+__global__ void k_dn_pool(const bf16* in, bf16* out, int C, int W, int H, int N) {
+    const int W2 = (W + 1) / 2, H2 = (H + 1) / 2;
+    const long long total = (long long)N * H2 * W2 * C;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+        int c = (int)(i % C);
+        long long p = i / C;
+        int x = (int)(p % W2), y = (int)((p / W2) % H2), n = (int)(p / ((long long)W2 * H2));
+        float s = 0.f;
+        int cnt = 0;
+        for (int dy = 0; dy < 2; dy++)
+            for (int dx = 0; dx < 2; dx++) {
+                int xx = 2 * x + dx, yy = 2 * y + dy;
+                if (xx < W && yy < H) {
+                    s += bf(in[(((long long)n * H + yy) * W + xx) * C + c]);
+                    cnt++;
+                }
+            }
+        out[i] = __float2bfloat16(s / cnt);
+    }
+}
+
+// gin += (gout / children) * (mask > 0), gin and mask at the fine size.
+__global__ void k_dn_pool_bwd(const bf16* gout, const bf16* mask, bf16* gin, int C, int W, int H, int N) {
+    const int W2 = (W + 1) / 2, H2 = (H + 1) / 2;
+    const long long total = (long long)N * H * W * C;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+        int c = (int)(i % C);
+        long long p = i / C;
+        int x = (int)(p % W), y = (int)((p / W) % H), n = (int)(p / ((long long)W * H));
+        int x2 = x / 2, y2 = y / 2;
+        int cnt = (2 * x2 + 1 < W ? 2 : 1) * (2 * y2 + 1 < H ? 2 : 1);
+        float g = bf(gout[(((long long)n * H2 + y2) * W2 + x2) * C + c]) / cnt;
+        if (!(bf(mask[i]) > 0.f)) g = 0.f;
+        gin[i] = __float2bfloat16(bf(gin[i]) + g);
+    }
+}
+
+// Nearest 2x upsampling to W x H.
+__global__ void k_dn_up(const bf16* in, bf16* out, int C, int W, int H, int N) {
+    const int W2 = (W + 1) / 2, H2 = (H + 1) / 2;
+    const long long total = (long long)N * H * W * C;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+        int c = (int)(i % C);
+        long long p = i / C;
+        int x = (int)(p % W), y = (int)((p / W) % H), n = (int)(p / ((long long)W * H));
+        out[i] = in[(((long long)n * H2 + y / 2) * W2 + x / 2) * C + c];
+    }
+}
+
+// gin (coarse) = sum of the gradients of its children.
+__global__ void k_dn_up_bwd(const bf16* gout, bf16* gin, int C, int W, int H, int N) {
+    const int W2 = (W + 1) / 2, H2 = (H + 1) / 2;
+    const long long total = (long long)N * H2 * W2 * C;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+        int c = (int)(i % C);
+        long long p = i / C;
+        int x = (int)(p % W2), y = (int)((p / W2) % H2), n = (int)(p / ((long long)W2 * H2));
+        float s = 0.f;
+        for (int dy = 0; dy < 2; dy++)
+            for (int dx = 0; dx < 2; dx++) {
+                int xx = 2 * x + dx, yy = 2 * y + dy;
+                if (xx < W && yy < H) s += bf(gout[(((long long)n * H + yy) * W + xx) * C + c]);
+            }
+        gin[i] = __float2bfloat16(s);
+    }
+}
+
+// db[c] += sum over pixels of g[p][c], c < cout (blockDim.x = channel stride).
+__global__ void k_dn_bias_grad(const bf16* g, int cs, int cout, long long P, float* db) {
+    const int c = threadIdx.x;
+    float s = 0.f;
+    for (long long p = blockIdx.x; p < P; p += gridDim.x) s += bf(g[p * cs + c]);
+    if (c < cout) atomicAdd(db + c, s);
+}
+
+// L1 loss on log1p colours: pred = y[:3] + x[:3]; gy = sign(pred - t) * valid * scale.
+__global__ void k_dn_loss(const bf16* y, const bf16* x, const float4* t, long long P, float scale, bf16* gy,
+                          float* loss) {
+    float acc = 0.f;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < P; p += (long long)gridDim.x * blockDim.x) {
+        float4 tt = t[p];
+        float tv[3] = {tt.x, tt.y, tt.z};
+        for (int c = 0; c < kFeat; c++) {
+            float g = 0.f;
+            if (c < 3 && tt.w > 0.f) {
+                float d = bf(y[p * kFeat + c]) + bf(x[p * kFeat + c]) - tv[c];
+                acc += fabsf(d);
+                g = (d > 0.f ? 1.f : d < 0.f ? -1.f : 0.f) * scale;
+            }
+            gy[p * kFeat + c] = __float2bfloat16(g);
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0 && loss) atomicAdd(loss, acc * scale);
+}
+
+__global__ void k_dn_adam(float* p, float* g, float* m, float* v, long long n, float lr, float b1, float b2, float eps,
+                          float bc1, float bc2) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        float gi = g[i];
+        float mi = b1 * m[i] + (1.f - b1) * gi;
+        float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        p[i] -= lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
+        g[i] = 0.f;
+    }
+}
+
+// Master weights [cout][9][kpad] -> forward BF16 [ncols][9][kpad] and the
+// data-gradient BF16 [kpad][9][copad] (taps flipped, co contiguous).
+__global__ void k_dn_pack(const float* w, int cout, int ncols, int kpad, int copad, bf16* wp, bf16* wt) {
+    const long long nf = (long long)ncols * 9 * kpad, nt = (long long)kpad * 9 * copad;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nf + nt; i += (long long)gridDim.x * blockDim.x) {
+        if (i < nf) {
+            int k = (int)(i % kpad), t = (int)((i / kpad) % 9), r = (int)(i / (9LL * kpad));
+            wp[i] = __float2bfloat16(r < cout ? w[((long long)r * 9 + t) * kpad + k] : 0.f);
+        } else {
+            long long j = i - nf;
+            int co = (int)(j % copad), t = (int)((j / copad) % 9), k = (int)(j / (9LL * copad));
+            wt[j] = __float2bfloat16(co < cout ? w[((long long)co * 9 + (8 - t)) * kpad + k] : 0.f);
+        }
+    }
+}
+
+// Face::colorAt at each valid lumel's texel centre (the surface albedo).
+__device__ __forceinline__ bool uv_bary(float2 a, float2 b, float2 c, float2 uv, float& bu, float& bv) {
+    float v0x = c.x - a.x, v0y = c.y - a.y, v1x = b.x - a.x, v1y = b.y - a.y, v2x = uv.x - a.x, v2y = uv.y - a.y;
+    float d00 = v0x * v0x + v0y * v0y, d01 = v0x * v1x + v0y * v1y, d02 = v0x * v2x + v0y * v2y;
+    float d11 = v1x * v1x + v1y * v1y, d12 = v1x * v2x + v1y * v2y;
+    float inv = 1.0f / (d00 * d11 - d01 * d01);
+    bu = (d11 * d02 - d01 * d12) * inv;
+    bv = (d00 * d12 - d01 * d02) * inv;
+    return true;
+}
+
+// Features of one lightmap: [h][w][16] = log1p(max(colour, 0)), normal,
+// albedo, valid, zeros.
+__global__ void k_dn_features(rl::DevScene s, rl::DevMap m, bf16* x) {
+    const long long n = (long long)m.width * m.height;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        float f[kFeat];
+        for (int c = 0; c < kFeat; c++) f[c] = 0.f;
+        if (m.flags[i] & 1) {
+            for (int c = 0; c < 3; c++) {
+                f[c] = log1pf(fmaxf(m.color[3 * i + c], 0.f));
+                f[3 + c] = m.normal[3 * i + c];
+            }
+            int mesh = m.mesh[i], face = m.face[i];
+            float4 alb = make_float4(1.f, 1.f, 1.f, 1.f);
+            if (mesh >= 0 && mesh < s.nmeshes) {
+                int tri = s.mesh_first_tri[mesh] + face;
+                int4 fv = s.tri_vidx[tri];
+                float2 a = make_float2(s.uv1[2 * fv.x], s.uv1[2 * fv.x + 1]);
+                float2 b = make_float2(s.uv1[2 * fv.y], s.uv1[2 * fv.y + 1]);
+                float2 c = make_float2(s.uv1[2 * fv.z], s.uv1[2 * fv.z + 1]);
+                int u = (int)(i % m.width), v = (int)(i / m.width);
+                float2 uv = make_float2((u + 0.5f) / (float)m.width, (v + 0.5f) / (float)m.height);
+                float bu, bv;
+                uv_bary(a, b, c, uv, bu, bv);
+                alb = rl::face_color(s, fv, bu, bv);
+            }
+            f[6] = alb.x;
+            f[7] = alb.y;
+            f[8] = alb.z;
+            f[9] = 1.f;
+        }
+        for (int c = 0; c < kFeat; c++) x[i * kFeat + c] = __float2bfloat16(f[c]);
+    }
+}
+
+// Targets of one lightmap: (log1p(max(colour, 0)), valid).
+__global__ void k_dn_targets(rl::DevMap m, float4* t) {
+    const long long n = (long long)m.width * m.height;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        bool v = m.flags[i] & 1;
+        t[i] = v ? make_float4(log1pf(fmaxf(m.color[3 * i], 0.f)), log1pf(fmaxf(m.color[3 * i + 1], 0.f)),
+                               log1pf(fmaxf(m.color[3 * i + 2], 0.f)), 1.f)
+                 : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+}
+
+// colour = base + expm1(prediction) on valid lumels (base may be null = 0).
+__global__ void k_dn_apply(const bf16* y, const bf16* x, rl::DevMap m, const float* base) {
+    const long long n = (long long)m.width * m.height;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        if (!(m.flags[i] & 1)) continue;
+        for (int c = 0; c < 3; c++) {
+            float v = expm1f(bf(y[i * kFeat + c]) + bf(x[i * kFeat + c]));
+            m.color[3 * i + c] = (base ? base[3 * i + c] : 0.f) + fmaxf(v, 0.f);
+        }
+    }
+}
+
+int grid_of(long long n, int block) {
+    long long g = (n + block - 1) / block;
+    return (int)std::max<long long>(1, std::min<long long>(g, 148LL * 16));
+}
+
+struct Conv {
+    int cout, ncols, segs[2], kpad, copad;
+    float *w, *b, *gw, *gb, *mw, *vw, *mb, *vb;
+    bf16 *wp, *wt;
+    float* bias;  // [ncols]
+    long long nw() const { return (long long)cout * 9 * kpad; }
+};
+
+struct Level {
+    int w, h;
+};
+
+}  // namespace
+
+struct rl_denoiser {
+    Conv conv[8];
+    float* params = nullptr;  // one block: every layer's w, b, gw, gb, mw, vw, mb, vb, bias
+    bf16* packed = nullptr;
+    long long nparam = 0;      // weights + biases
+    int* d_err = nullptr;
+    long long step = 0;
+    // activation / gradient buffers for the current shape
+    int bn = 0, bh = 0, bw = 0, btrain = 0;
+    bf16* act = nullptr;
+    size_t act_bytes = 0;
+    bf16 *x, *e0, *p0, *e1, *p1, *e2, *p2, *e3, *u2, *d2, *u1, *d1, *u0, *d0, *y;
+    bf16 *gy, *gd0, *gu0, *ge0, *gd1, *gu1, *ge1, *gd2, *gu2, *ge2, *ge3, *gp2, *gp1, *gp0;
+    float4* tgt = nullptr;
+    ~rl_denoiser() {
+        cudaFree(params);
+        cudaFree(packed);
+        cudaFree(d_err);
+        cudaFree(act);
+    }
+};
+
+namespace {
+
+const int kCout[8] = {32, 64, 96, 128, 96, 64, 32, 3};
+const int kSeg0[8] = {16, 32, 64, 96, 128, 96, 64, 32};
+const int kSeg1[8] = {0, 0, 0, 0, 96, 64, 32, 0};
+
+int pad64(int c) { return (c + 63) / 64 * 64; }
+int pad16(int c) { return (c + 15) / 16 * 16; }
+
+// Deterministic He-uniform initialisation from a 64-bit seed.
+void init_weights(std::vector<float>& w, int fan_in, uint64_t seed) {
+    uint64_t s = seed * 0x9E3779B97F4A7C15ull + 1;
+    float lim = sqrtf(6.0f / (float)fan_in);
+    for (float& v : w) {
+        s ^= s << 13;
+        s ^= s >> 7;
+        s ^= s << 17;
+        v = ((float)((s >> 11) & 0xFFFFFF) / 16777216.0f * 2.0f - 1.0f) * lim;
+    }
+}
+
+// Carve the activation (and, for training, gradient) buffers of an n x h x
+// w batch from one allocation that only grows.  Every buffer is fully
+// written before it is read, so reuse needs no clearing.
+int alloc_shapes(rl_denoiser* d, int n, int h, int w, bool train, cudaStream_t st) {
+    if (d->bn == n && d->bh == h && d->bw == w && (d->btrain || !train) && d->act) return RL_OK;
+    (void)st;
+    Level L[4];
+    L[0] = {w, h};
+    for (int k = 1; k < 4; k++) L[k] = {(L[k - 1].w + 1) / 2, (L[k - 1].h + 1) / 2};
+    auto sz = [&](int lvl, int c) { return (size_t)n * L[lvl].w * L[lvl].h * c * sizeof(bf16); };
+    struct Buf { bf16** p; int lvl, c; bool grad; };
+    Buf bufs[] = {{&d->x, 0, 16, 0},   {&d->e0, 0, 32, 0},  {&d->p0, 1, 32, 0},  {&d->e1, 1, 64, 0},
+                  {&d->p1, 2, 64, 0},  {&d->e2, 2, 96, 0},  {&d->p2, 3, 96, 0},  {&d->e3, 3, 128, 0},
+                  {&d->u2, 2, 128, 0}, {&d->d2, 2, 96, 0},  {&d->u1, 1, 96, 0},  {&d->d1, 1, 64, 0},
+                  {&d->u0, 0, 64, 0},  {&d->d0, 0, 32, 0},  {&d->y, 0, 16, 0},   {&d->gy, 0, 16, 1},
+                  {&d->gd0, 0, 32, 1}, {&d->gu0, 0, 64, 1}, {&d->ge0, 0, 32, 1}, {&d->gd1, 1, 64, 1},
+                  {&d->gu1, 1, 96, 1}, {&d->ge1, 1, 64, 1}, {&d->gd2, 2, 96, 1}, {&d->gu2, 2, 128, 1},
+                  {&d->ge2, 2, 96, 1}, {&d->ge3, 3, 128, 1}, {&d->gp2, 3, 96, 1}, {&d->gp1, 2, 64, 1},
+                  {&d->gp0, 1, 32, 1}};
+    size_t total = 0;
+    for (const Buf& b : bufs)
+        if (train || !b.grad) total += (sz(b.lvl, b.c) + 255) / 256 * 256;
+    size_t tbytes = train ? (size_t)n * h * w * sizeof(float4) : 0;
+    total += tbytes + 256;
+    if (total > d->act_bytes) {
+        DN_CK(cudaDeviceSynchronize());
+        cudaFree(d->act);
+        d->act = nullptr;
+        d->act_bytes = 0;
+        DN_CK(cudaMalloc(&d->act, total));
+        d->act_bytes = total;
+    }
+    char* p = (char*)d->act;
+    for (const Buf& b : bufs) {
+        if (!train && b.grad) {
+            *b.p = nullptr;
+            continue;
+        }
+        *b.p = (bf16*)p;
+        p += (sz(b.lvl, b.c) + 255) / 256 * 256;
+    }
+    d->tgt = train ? (float4*)p : nullptr;
+    d->bn = n;
+    d->bh = h;
+    d->bw = w;
+    d->btrain = train;
+    return RL_OK;
+}
+
+int conv_fwd(rl_denoiser* d, int l, const bf16* in0, const bf16* in1, int w, int h, int n, bf16* out, bool relu,
+             cudaStream_t st) {
+    Conv& c = d->conv[l];
+    return rl_dn_conv3x3(in0, c.segs[0], in1, c.segs[1], w, h, n, c.wp, c.ncols, c.bias, relu ? 1 : 0, out, 0,
+                         c.ncols, c.ncols, nullptr, nullptr, 0, 0, 0, nullptr, d->d_err, st);
+}
+
+// Data gradient of layer l: gout (ncols stored) -> g0 (segment 0) / g1,
+// each masked by the matching forward input (relu outputs; the upsampled
+// inputs carry their source's sign).
+int conv_dgrad(rl_denoiser* d, int l, const bf16* gout, int w, int h, int n, bf16* g0, const bf16* m0, bf16* g1,
+               const bf16* m1, cudaStream_t st) {
+    Conv& c = d->conv[l];
+    return rl_dn_conv3x3(gout, c.ncols, nullptr, 0, w, h, n, c.wt, c.kpad, nullptr, 0, g0, 0, c.segs[0], c.segs[0],
+                         m0, g1, pad64(c.segs[0]), g1 ? c.segs[1] : 0, g1 ? c.segs[1] : 0, m1, d->d_err, st);
+}
+
+int conv_wgrad(rl_denoiser* d, int l, const bf16* gout, const bf16* in0, const bf16* in1, int w, int h, int n,
+               cudaStream_t st) {
+    Conv& c = d->conv[l];
+    if (int rc = rl_dn_conv3x3_wgrad(gout, c.cout, c.ncols, in0, c.segs[0], c.segs[0], w, h, n, c.gw, 0, c.kpad,
+                                     d->d_err, st))
+        return rc;
+    if (in1)
+        if (int rc = rl_dn_conv3x3_wgrad(gout, c.cout, c.ncols, in1, c.segs[1], c.segs[1], w, h, n, c.gw,
+                                         pad64(c.segs[0]), c.kpad, d->d_err, st))
+            return rc;
+    const long long P = (long long)n * w * h;
+    k_dn_bias_grad<<<(int)std::min<long long>(P, 2048), c.ncols, 0, st>>>(gout, c.ncols, c.cout, P, c.gb);
+    return RL_OK;
+}
+
+int forward(rl_denoiser* d, int n, int h, int w, cudaStream_t st) {
+    Level L[4];
+    L[0] = {w, h};
+    for (int k = 1; k < 4; k++) L[k] = {(L[k - 1].w + 1) / 2, (L[k - 1].h + 1) / 2};
+    auto pool = [&](const bf16* in, bf16* out, int c, int lvl) {
+        long long tot = (long long)n * L[lvl + 1].w * L[lvl + 1].h * c;
+        k_dn_pool<<<grid_of(tot, 256), 256, 0, st>>>(in, out, c, L[lvl].w, L[lvl].h, n);
+    };
+    auto up = [&](const bf16* in, bf16* out, int c, int lvl) {
+        long long tot = (long long)n * L[lvl].w * L[lvl].h * c;
+        k_dn_up<<<grid_of(tot, 256), 256, 0, st>>>(in, out, c, L[lvl].w, L[lvl].h, n);
+    };
+    int rc;
+    if ((rc = conv_fwd(d, 0, d->x, nullptr, L[0].w, L[0].h, n, d->e0, true, st))) return rc;
+    pool(d->e0, d->p0, 32, 0);
+    if ((rc = conv_fwd(d, 1, d->p0, nullptr, L[1].w, L[1].h, n, d->e1, true, st))) return rc;
+    pool(d->e1, d->p1, 64, 1);
+    if ((rc = conv_fwd(d, 2, d->p1, nullptr, L[2].w, L[2].h, n, d->e2, true, st))) return rc;
+    pool(d->e2, d->p2, 96, 2);
+    if ((rc = conv_fwd(d, 3, d->p2, nullptr, L[3].w, L[3].h, n, d->e3, true, st))) return rc;
+    up(d->e3, d->u2, 128, 2);
+    if ((rc = conv_fwd(d, 4, d->u2, d->e2, L[2].w, L[2].h, n, d->d2, true, st))) return rc;
+    up(d->d2, d->u1, 96, 1);
+    if ((rc = conv_fwd(d, 5, d->u1, d->e1, L[1].w, L[1].h, n, d->d1, true, st))) return rc;
+    up(d->d1, d->u0, 64, 0);
+    if ((rc = conv_fwd(d, 6, d->u0, d->e0, L[0].w, L[0].h, n, d->d0, true, st))) return rc;
+    if ((rc = conv_fwd(d, 7, d->d0, nullptr, L[0].w, L[0].h, n, d->y, false, st))) return rc;
+    DN_CK(cudaGetLastError());
+    return RL_OK;
+}
+
+int backward(rl_denoiser* d, int n, int h, int w, cudaStream_t st) {
+    Level L[4];
+    L[0] = {w, h};
+    for (int k = 1; k < 4; k++) L[k] = {(L[k - 1].w + 1) / 2, (L[k - 1].h + 1) / 2};
+    auto up_bwd = [&](const bf16* gfine, bf16* gcoarse, int c, int lvl) {
+        long long tot = (long long)n * L[lvl + 1].w * L[lvl + 1].h * c;
+        k_dn_up_bwd<<<grid_of(tot, 256), 256, 0, st>>>(gfine, gcoarse, c, L[lvl].w, L[lvl].h, n);
+    };
+    auto pool_bwd = [&](const bf16* gcoarse, const bf16* mask, bf16* gfine, int c, int lvl) {
+        long long tot = (long long)n * L[lvl].w * L[lvl].h * c;
+        k_dn_pool_bwd<<<grid_of(tot, 256), 256, 0, st>>>(gcoarse, mask, gfine, c, L[lvl].w, L[lvl].h, n);
+    };
+    int rc;
+    const int W0 = L[0].w, H0 = L[0].h;
+    // output layer
+    if ((rc = conv_wgrad(d, 7, d->gy, d->d0, nullptr, W0, H0, n, st))) return rc;
+    if ((rc = conv_dgrad(d, 7, d->gy, W0, H0, n, d->gd0, d->d0, nullptr, nullptr, st))) return rc;
+    // level 0 decoder: d0 = c6(u0, e0)
+    if ((rc = conv_wgrad(d, 6, d->gd0, d->u0, d->e0, W0, H0, n, st))) return rc;
+    if ((rc = conv_dgrad(d, 6, d->gd0, W0, H0, n, d->gu0, d->u0, d->ge0, d->e0, st))) return rc;
+    up_bwd(d->gu0, d->gd1, 64, 0);
+    // level 1 decoder: d1 = c5(u1, e1)
+    if ((rc = conv_wgrad(d, 5, d->gd1, d->u1, d->e1, L[1].w, L[1].h, n, st))) return rc;
+    if ((rc = conv_dgrad(d, 5, d->gd1, L[1].w, L[1].h, n, d->gu1, d->u1, d->ge1, d->e1, st))) return rc;
+    up_bwd(d->gu1, d->gd2, 96, 1);
+    // level 2 decoder: d2 = c4(u2, e2)
+    if ((rc = conv_wgrad(d, 4, d->gd2, d->u2, d->e2, L[2].w, L[2].h, n, st))) return rc;
+    if ((rc = conv_dgrad(d, 4, d->gd2, L[2].w, L[2].h, n, d->gu2, d->u2, d->ge2, d->e2, st))) return rc;
+    up_bwd(d->gu2, d->ge3, 128, 2);
+    // bottleneck e3 = c3(p2)
+    if ((rc = conv_wgrad(d, 3, d->ge3, d->p2, nullptr, L[3].w, L[3].h, n, st))) return rc;
+    if ((rc = conv_dgrad(d, 3, d->ge3, L[3].w, L[3].h, n, d->gp2, nullptr, nullptr, nullptr, st))) return rc;
+    pool_bwd(d->gp2, d->e2, d->ge2, 96, 2);
+    // encoder e2 = c2(p1)
+    if ((rc = conv_wgrad(d, 2, d->ge2, d->p1, nullptr, L[2].w, L[2].h, n, st))) return rc;
+    if ((rc = conv_dgrad(d, 2, d->ge2, L[2].w, L[2].h, n, d->gp1, nullptr, nullptr, nullptr, st))) return rc;
+    pool_bwd(d->gp1, d->e1, d->ge1, 64, 1);
+    // encoder e1 = c1(p0)
+    if ((rc = conv_wgrad(d, 1, d->ge1, d->p0, nullptr, L[1].w, L[1].h, n, st))) return rc;
+    if ((rc = conv_dgrad(d, 1, d->ge1, L[1].w, L[1].h, n, d->gp0, nullptr, nullptr, nullptr, st))) return rc;
+    pool_bwd(d->gp0, d->e0, d->ge0, 32, 0);
+    // encoder e0 = c0(x)
+    if ((rc = conv_wgrad(d, 0, d->ge0, d->x, nullptr, W0, H0, n, st))) return rc;
+    DN_CK(cudaGetLastError());
+    return RL_OK;
+}
+
+int pack_all(rl_denoiser* d, cudaStream_t st) {
+    for (int l = 0; l < 8; l++) {
+        Conv& c = d->conv[l];
+        long long tot = (long long)c.ncols * 9 * c.kpad + (long long)c.kpad * 9 * c.copad;
+        k_dn_pack<<<grid_of(tot, 256), 256, 0, st>>>(c.w, c.cout, c.ncols, c.kpad, c.copad, c.wp, c.wt);
+        DN_CK(cudaMemcpyAsync(c.bias, c.b, c.cout * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    }
+    DN_CK(cudaGetLastError());
+    return RL_OK;
+}
+
+}  // namespace
+
+extern "C" int rl_denoiser_create(uint64_t seed, rl_denoiser** out) {
+    if (!out) return dn_fail(RL_INVALID_CALL, "rl_denoiser_create: null argument");
+    *out = nullptr;
+    rl_denoiser* d = new (std::nothrow) rl_denoiser;
+    if (!d) return dn_fail(RL_OUT_OF_MEMORY, "host allocation failed");
+    long long floats = 0, halves = 0;
+    for (int l = 0; l < 8; l++) {
+        Conv& c = d->conv[l];
+        c.cout = kCout[l];
+        c.ncols = pad16(kCout[l]);
+        c.segs[0] = kSeg0[l];
+        c.segs[1] = kSeg1[l];
+        c.kpad = pad64(c.segs[0]) + (c.segs[1] ? pad64(c.segs[1]) : 0);
+        c.copad = pad64(c.ncols);
+        floats += 4 * c.nw() + 4 * c.cout + c.ncols + 64;
+        halves += (long long)c.ncols * 9 * c.kpad + (long long)c.kpad * 9 * c.copad + 128;
+        d->nparam += c.nw() + c.cout;
+    }
+    cudaError_t e = cudaMalloc(&d->params, floats * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&d->packed, halves * sizeof(bf16));
+    if (e == cudaSuccess) e = cudaMalloc(&d->d_err, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(d->params, 0, floats * sizeof(float));
+    if (e == cudaSuccess) e = cudaMemset(d->d_err, 0, sizeof(int));
+    if (e != cudaSuccess) {
+        delete d;
+        return dn_fail(RL_OUT_OF_MEMORY, "denoiser parameters: %s", cudaGetErrorString(e));
+    }
+    float* p = d->params;
+    bf16* q = d->packed;
+    auto take = [&](long long n) { float* r = p; p += (n + 15) / 16 * 16; return r; };
+    for (int l = 0; l < 8; l++) {
+        Conv& c = d->conv[l];
+        c.w = take(c.nw());
+        c.b = take(c.cout);
+        c.gw = take(c.nw());
+        c.gb = take(c.cout);
+        c.mw = take(c.nw());
+        c.vw = take(c.nw());
+        c.mb = take(c.cout);
+        c.vb = take(c.cout);
+        c.bias = take(c.ncols);
+        c.wp = q;
+        q += ((long long)c.ncols * 9 * c.kpad + 63) / 64 * 64;
+        c.wt = q;
+        q += ((long long)c.kpad * 9 * c.copad + 63) / 64 * 64;
+    }
+    // weights of the real input channels only; padding columns stay zero
+    for (int l = 0; l < 8; l++) {
+        Conv& c = d->conv[l];
+        std::vector<float> w(c.nw(), 0.f);
+        int real0 = l == 0 ? 10 : c.segs[0], real1 = c.segs[1];
+        std::vector<float> r((size_t)c.cout * 9 * (real0 + real1));
+        init_weights(r, 9 * (real0 + real1), seed + 7919 * (l + 1));
+        if (l == 7)
+            for (float& v : r) v *= 0.1f;  // start near the identity (prediction = noisy input)
+        for (int co = 0; co < c.cout; co++)
+            for (int t = 0; t < 9; t++) {
+                for (int k = 0; k < real0; k++)
+                    w[((size_t)co * 9 + t) * c.kpad + k] = r[((size_t)co * 9 + t) * (real0 + real1) + k];
+                for (int k = 0; k < real1; k++)
+                    w[((size_t)co * 9 + t) * c.kpad + pad64(c.segs[0]) + k] =
+                        r[((size_t)co * 9 + t) * (real0 + real1) + real0 + k];
+            }
+        e = cudaMemcpy(c.w, w.data(), w.size() * sizeof(float), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) {
+            delete d;
+            return dn_fail(RL_CUDA_ERROR, "denoiser init: %s", cudaGetErrorString(e));
+        }
+    }
+    if (int rc = pack_all(d, 0)) {
+        delete d;
+        return rc;
+    }
+    e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) {
+        delete d;
+        return dn_fail(RL_CUDA_ERROR, "denoiser init: %s", cudaGetErrorString(e));
+    }
+    *out = d;
+    return RL_OK;
+}
+
+extern "C" int rl_denoiser_destroy(rl_denoiser* d) {
+    if (!d) return dn_fail(RL_INVALID_CALL, "null denoiser");
+    cudaDeviceSynchronize();
+    delete d;
+    return RL_OK;
+}
+
+extern "C" int rl_denoiser_param_count(const rl_denoiser* d, int64_t* n) {
+    if (!d || !n) return dn_fail(RL_INVALID_CALL, "null argument");
+    *n = d->nparam;
+    return RL_OK;
+}
+
+// Parameters as one host array: per layer, weights [cout][9][kpad] then biases.
+extern "C" int rl_denoiser_get_params(const rl_denoiser* d, float* host) {
+    if (!d || !host) return dn_fail(RL_INVALID_CALL, "null argument");
+    for (int l = 0; l < 8; l++) {
+        const Conv& c = d->conv[l];
+        DN_CK(cudaMemcpy(host, c.w, c.nw() * sizeof(float), cudaMemcpyDeviceToHost));
+        host += c.nw();
+        DN_CK(cudaMemcpy(host, c.b, c.cout * sizeof(float), cudaMemcpyDeviceToHost));
+        host += c.cout;
+    }
+    return RL_OK;
+}
+
+extern "C" int rl_denoiser_set_params(rl_denoiser* d, const float* host) {
+    if (!d || !host) return dn_fail(RL_INVALID_CALL, "null argument");
+    for (int l = 0; l < 8; l++) {
+        Conv& c = d->conv[l];
+        DN_CK(cudaMemcpy(c.w, host, c.nw() * sizeof(float), cudaMemcpyHostToDevice));
+        host += c.nw();
+        DN_CK(cudaMemcpy(c.b, host, c.cout * sizeof(float), cudaMemcpyHostToDevice));
+        host += c.cout;
+    }
+    if (int rc = pack_all(d, 0)) return rc;
+    DN_CK(cudaDeviceSynchronize());
+    return RL_OK;
+}
+
+// Accumulated gradients in the rl_denoiser_get_params layout; clears them.
+extern "C" int rl_denoiser_get_grads(rl_denoiser* d, float* host) {
+    if (!d || !host) return dn_fail(RL_INVALID_CALL, "null argument");
+    DN_CK(cudaDeviceSynchronize());
+    for (int l = 0; l < 8; l++) {
+        Conv& c = d->conv[l];
+        DN_CK(cudaMemcpy(host, c.gw, c.nw() * sizeof(float), cudaMemcpyDeviceToHost));
+        host += c.nw();
+        DN_CK(cudaMemcpy(host, c.gb, c.cout * sizeof(float), cudaMemcpyDeviceToHost));
+        host += c.cout;
+        DN_CK(cudaMemset(c.gw, 0, c.nw() * sizeof(float)));
+        DN_CK(cudaMemset(c.gb, 0, c.cout * sizeof(float)));
+    }
+    return RL_OK;
+}
+
+extern "C" int rl_denoiser_features(const rl_scene* scene, const rl_map* map, void* d_x, void* stream) {
+    const rl::DevMap* m = rl_internal_map(map);
+    const rl::DevScene* s = rl_internal_scene(scene);
+    if (!m || !s || !d_x) return dn_fail(RL_INVALID_CALL, "rl_denoiser_features: null argument");
+    long long n = (long long)m->width * m->height;
+    k_dn_features<<<grid_of(n, 256), 256, 0, (cudaStream_t)stream>>>(*s, *m, (bf16*)d_x);
+    DN_CK(cudaGetLastError());
+    return RL_OK;
+}
+
+extern "C" int rl_denoiser_targets(const rl_map* map, float* d_t, void* stream) {
+    const rl::DevMap* m = rl_internal_map(map);
+    if (!m || !d_t) return dn_fail(RL_INVALID_CALL, "rl_denoiser_targets: null argument");
+    long long n = (long long)m->width * m->height;
+    k_dn_targets<<<grid_of(n, 256), 256, 0, (cudaStream_t)stream>>>(*m, (float4*)d_t);
+    DN_CK(cudaGetLastError());
+    return RL_OK;
+}
+
+extern "C" int rl_denoiser_train_step(rl_denoiser* d, const void* d_x, const float* d_t, int batch, int patch,
+                                      float lr, float* d_loss, void* stream) {
+    if (!d || !d_x || !d_t || batch <= 0 || patch < 8) return dn_fail(RL_INVALID_CALL, "rl_denoiser_train_step: bad arguments");
+    cudaStream_t st = (cudaStream_t)stream;
+    if (int rc = alloc_shapes(d, batch, patch, patch, true, st)) return rc;
+    const long long P = (long long)batch * patch * patch;
+    DN_CK(cudaMemcpyAsync(d->x, d_x, P * kFeat * sizeof(bf16), cudaMemcpyDeviceToDevice, st));
+    DN_CK(cudaMemcpyAsync(d->tgt, d_t, P * sizeof(float4), cudaMemcpyDeviceToDevice, st));
+    // gradient buffers that are accumulated into start at zero
+    if (int rc = forward(d, batch, patch, patch, st)) return rc;
+    k_dn_loss<<<grid_of(P, 256), 256, 0, st>>>(d->y, d->x, d->tgt, P, 1.0f / (float)(P * 3), d->gy, d_loss);
+    if (int rc = backward(d, batch, patch, patch, st)) return rc;
+    if (lr < 0.f) return RL_OK;  // gradients only (rl_denoiser_get_grads)
+    d->step++;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float bc1 = 1.f - powf(b1, (float)d->step), bc2 = 1.f - powf(b2, (float)d->step);
+    for (int l = 0; l < 8; l++) {
+        Conv& c = d->conv[l];
+        k_dn_adam<<<grid_of(c.nw(), 256), 256, 0, st>>>(c.w, c.gw, c.mw, c.vw, c.nw(), lr, b1, b2, 1e-8f, bc1, bc2);
+        k_dn_adam<<<1, 128, 0, st>>>(c.b, c.gb, c.mb, c.vb, c.cout, lr, b1, b2, 1e-8f, bc1, bc2);
+    }
+    return pack_all(d, st);
+}
+
+extern "C" int rl_denoiser_apply(rl_denoiser* d, const rl_scene* scene, rl_map* map, const float* d_base,
+                                 void* stream) {
+    const rl::DevMap* m = rl_internal_map(map);
+    const rl::DevScene* s = rl_internal_scene(scene);
+    if (!d || !m || !s) return dn_fail(RL_INVALID_CALL, "rl_denoiser_apply: null argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    if (int rc = alloc_shapes(d, 1, m->height, m->width, false, st)) return rc;
+    long long n = (long long)m->width * m->height;
+    k_dn_features<<<grid_of(n, 256), 256, 0, st>>>(*s, *m, d->x);
+    if (int rc = forward(d, 1, m->height, m->width, st)) return rc;
+    k_dn_apply<<<grid_of(n, 256), 256, 0, st>>>(d->y, d->x, *m, d_base);
+    DN_CK(cudaGetLastError());
+    return RL_OK;
+}
+
+extern "C" int rl_denoiser_forward(rl_denoiser* d, const void* d_x, int images, int height, int width, void* d_y,
+                                   void* stream) {
+    if (!d || !d_x || !d_y) return dn_fail(RL_INVALID_CALL, "rl_denoiser_forward: null argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    if (int rc = alloc_shapes(d, images, height, width, d->btrain != 0, st)) return rc;
+    const long long P = (long long)images * height * width;
+    DN_CK(cudaMemcpyAsync(d->x, d_x, P * kFeat * sizeof(bf16), cudaMemcpyDeviceToDevice, st));
+    if (int rc = forward(d, images, height, width, st)) return rc;
+    DN_CK(cudaMemcpyAsync(d_y, d->y, P * kFeat * sizeof(bf16), cudaMemcpyDeviceToDevice, st));
+    return RL_OK;
+}
+
+extern "C" int rl_denoiser_status(rl_denoiser* d, int* flags) {
+    if (!d || !flags) return dn_fail(RL_INVALID_CALL, "null argument");
+    DN_CK(cudaMemcpy(flags, d->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    return RL_OK;
+}

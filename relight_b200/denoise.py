@@ -35,3 +35,206 @@ def conv3x3_wgrad(grad, cout, inp, cin, dw, ci_off=0, ci_total=None, err=None, s
     ci_total = dw.shape[-1] if ci_total is None else ci_total
     check(lib().rl_dn_conv3x3_wgrad(_p(grad), cout, gcs, _p(inp), cin, inp.shape[-1], w, h, n, _p(dw), ci_off,
                                     ci_total, _p(err), stream))
+
+
+# ------------------------------------------------------------------ network
+
+# (cout, input segment channel counts) per convolution, as built by
+# rl_denoiser_create; k = sum of segments padded to 64.
+LAYERS = [(32, (16,)), (64, (32,)), (96, (64,)), (128, (96,)), (96, (128, 96)), (64, (96, 64)), (32, (64, 32)),
+          (3, (32,))]
+FEATURES = 16
+
+
+def _pad64(c):
+    return (c + 63) // 64 * 64
+
+
+class Denoiser:
+    """rl_denoiser: the BF16 tensor-core encoder-decoder."""
+
+    def __init__(self, seed: int = 1):
+        self.handle = C.c_void_p()
+        check(lib().rl_denoiser_create(seed, C.byref(self.handle)))
+        n = C.c_int64()
+        check(lib().rl_denoiser_param_count(self.handle, C.byref(n)))
+        self.nparam = n.value
+
+    # parameters ------------------------------------------------------
+    def params(self):
+        import numpy as np
+        out = np.zeros(self.nparam, np.float32)
+        check(lib().rl_denoiser_get_params(self.handle, C.c_void_p(out.ctypes.data)))
+        return out
+
+    def set_params(self, arr):
+        import numpy as np
+        arr = np.ascontiguousarray(arr, np.float32)
+        assert arr.size == self.nparam
+        check(lib().rl_denoiser_set_params(self.handle, C.c_void_p(arr.ctypes.data)))
+
+    def grads(self):
+        import numpy as np
+        out = np.zeros(self.nparam, np.float32)
+        check(lib().rl_denoiser_get_grads(self.handle, C.c_void_p(out.ctypes.data)))
+        return out
+
+    @staticmethod
+    def unflatten(flat):
+        """[(w [cout][9][k], b [cout])] per layer from a flat parameter array."""
+        out, o = [], 0
+        for cout, segs in LAYERS:
+            k = sum(_pad64(s) for s in segs)
+            w = flat[o:o + cout * 9 * k].reshape(cout, 9, k)
+            o += cout * 9 * k
+            out.append((w, flat[o:o + cout]))
+            o += cout
+        return out
+
+    def save(self, path):
+        import numpy as np
+        np.save(path, self.params())
+
+    def load(self, path):
+        import numpy as np
+        self.set_params(np.load(path))
+
+    # compute ---------------------------------------------------------
+    def train_step(self, x, t, lr, loss=None, stream=None):
+        """One Adam step on a batch: x BF16 [b][p][p][16], t FP32 [b][p][p][4]."""
+        b, p = x.shape[0], x.shape[1]
+        check(lib().rl_denoiser_train_step(self.handle, _p(x), _p(t), b, p, float(lr), _p(loss), stream))
+
+    def forward(self, x, stream=None):
+        import torch
+        y = torch.empty_like(x)
+        n, h, w, _ = x.shape
+        check(lib().rl_denoiser_forward(self.handle, _p(x), n, h, w, _p(y), stream))
+        return y
+
+    def apply(self, scene, lightmap, base=None, stream=None):
+        """Denoise a baked lightmap (DeviceMap) of a DeviceScene in place."""
+        check(lib().rl_denoiser_apply(self.handle, scene.handle, lightmap.handle, _p(base), stream))
+
+    def status(self) -> int:
+        f = C.c_int()
+        check(lib().rl_denoiser_status(self.handle, C.byref(f)))
+        return f.value
+
+    def close(self):
+        if self.handle:
+            check(lib().rl_denoiser_destroy(self.handle))
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def features(scene, lightmap, stream=None):
+    """BF16 [h][w][16] input features of a baked lightmap (rl_denoiser_features)."""
+    import torch
+    x = torch.empty(lightmap.height, lightmap.width, FEATURES, dtype=torch.bfloat16, device="cuda")
+    check(lib().rl_denoiser_features(scene.handle, lightmap.handle, _p(x), stream))
+    return x
+
+
+def targets(lightmap, stream=None):
+    """FP32 [h][w][4] training targets (log1p rgb, valid) of a baked lightmap."""
+    import torch
+    t = torch.empty(lightmap.height, lightmap.width, 4, dtype=torch.float32, device="cuda")
+    check(lib().rl_denoiser_targets(lightmap.handle, _p(t), stream))
+    return t
+
+
+# ---------------------------------------------------------------- training data
+
+def bake_fg(relight, ds, lightmap, photonmaps, settings, spp, seed, stream=None):
+    """The final-gather component alone at `spp` samples (colours cleared first)."""
+    from .device import _map_array
+    lightmap.clear(colors=True, photons=False, stream=stream)
+    sky = (C.c_float * 3)(*[float(v) for v in settings.sky_color])
+    amb = (C.c_float * 3)(*[float(v) for v in settings.ambient_color])
+    check(lib().rl_bake_indirect(ds.handle, lightmap.handle, _map_array(photonmaps), len(photonmaps), int(spp),
+                                 float(settings.final_gather_distance), sky, amb, int(seed), None, stream))
+
+
+def training_scenes(n, seed=100, sides=(256, 384, 512)):
+    """Seeded terrain-and-boxes scenes (the bench scene's recipe at varied
+    sizes) for (low, high) sample-count pairs."""
+    import numpy as np
+    from . import scenes
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n):
+        verts = int(rng.integers(48, 160))
+        boxes = int(rng.integers(20, 600))
+        side = int(rng.choice(sides))
+        out.append(scenes.terrain_scene(seed=seed * 1000 + k, verts=verts, n_boxes=boxes, size=side, tiles=1,
+                                        passes=2))
+    return out
+
+
+def make_pairs(workloads, spp_lo=16, spp_hi=1024, seed=7, stream=None, builder=0):
+    """Bake each workload's lightmap twice (final gather only, different
+    seeds): features of the low-sample bake and targets of the high-sample
+    one.  Returns [(x [h][w][16], t [h][w][4])] on the device."""
+    from .device import Relight
+    pairs = []
+    for k, wl in enumerate(workloads):
+        rl = Relight(stream, seed=seed + 31 * k, builder=builder)
+        ds = rl.device_scene(wl.scene)
+        rl.emit_photons(wl.scene, wl.settings)
+        lm = wl.lightmap._device
+        pms = [m._device for m in wl.scene.flat.photonmaps]
+        bake_fg(rl, ds, lm, pms, wl.settings, spp_lo, seed * 7 + 2 * k + 1, stream)
+        x = features(ds, lm, stream)
+        bake_fg(rl, ds, lm, pms, wl.settings, spp_hi, seed * 7 + 2 * k + 2, stream)
+        t = targets(lm, stream)
+        pairs.append((x, t))
+    return pairs
+
+
+def make_patches(pairs, count, patch=64, seed=11, min_valid=0.3):
+    """`count` random patch crops (at least `min_valid` valid texels) from
+    the pairs: x BF16 [count][p][p][16], t FP32 [count][p][p][4]."""
+    import numpy as np
+    import torch
+    rng = np.random.default_rng(seed)
+    xs, ts = [], []
+    tries = 0
+    while len(xs) < count and tries < 50 * count:
+        tries += 1
+        x, t = pairs[int(rng.integers(0, len(pairs)))]
+        h, w = x.shape[0], x.shape[1]
+        y0, x0 = int(rng.integers(0, h - patch + 1)), int(rng.integers(0, w - patch + 1))
+        tt = t[y0:y0 + patch, x0:x0 + patch]
+        if float(tt[..., 3].mean()) < min_valid:
+            continue
+        xs.append(x[y0:y0 + patch, x0:x0 + patch])
+        ts.append(tt)
+    return torch.stack(xs).contiguous(), torch.stack(ts).contiguous()
+
+
+def train(dn, xs, ts, steps, batch=16, lr=2e-3, seed=5, stream=None, log_every=0):
+    """Adam on random batches of the patch set with a cosine learning-rate
+    decay; returns the per-step losses (mean L1 in log space)."""
+    import math
+    import torch
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    loss = torch.zeros(steps, dtype=torch.float32, device="cuda")
+    n = xs.shape[0]
+    for s in range(steps):
+        idx = torch.randint(0, n, (batch,), device="cuda", generator=g)
+        rate = lr * 0.5 * (1 + math.cos(math.pi * s / steps))
+        dn.train_step(xs[idx].contiguous(), ts[idx].contiguous(), rate, loss=loss[s:s + 1], stream=stream)
+    return loss.cpu().numpy() * 1.0
+
+
+def rmse(a, b, valid):
+    """Per-texel RMSE over valid lumels (linear colour)."""
+    import numpy as np
+    d = (np.asarray(a, np.float64) - np.asarray(b, np.float64))[valid]
+    return float(np.sqrt((d * d).mean()))

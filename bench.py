@@ -419,28 +419,98 @@ def batch_arm(args):
     }
 
 
-SERVE_METRIC = "bake-serving p99 latency at 100 req/s (Poisson; direct + AO 64 + FG 16 spp per request)"
+DENOISE_METRIC = "lightmaps/s at equal per-texel RMSE vs an 8192 spp bake (final gather 16 spp + denoiser vs plain)"
+
+
+def train_denoiser(small):
+    """Bake (16, 1024) spp final-gather pairs on seeded terrain-and-boxes
+    scenes, cut 64x64 patches and train the denoiser (Adam, BF16 tensor-core
+    kernels).  Returns the network, its loss curve and the timings."""
+    import torch
+    from relight_b200 import denoise as D
+    n_train = 8 if small else 24
+    patches, steps = (4000, 1500) if small else (10000, 4000)
+    t0 = time.perf_counter()
+    pairs = D.make_pairs(D.training_scenes(n_train, seed=100), spp_lo=16, spp_hi=1024, seed=7)
+    xs, ts = D.make_patches(pairs, patches, patch=64, seed=11)
+    del pairs
+    torch.cuda.synchronize()
+    t_data = time.perf_counter() - t0
+    dn = D.Denoiser(seed=1)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    losses = D.train(dn, xs, ts, steps=steps, batch=16, lr=2e-3)
+    e1.record()
+    torch.cuda.synchronize()
+    info = {"scenes": n_train, "patches": patches, "steps": steps, "batch": 16, "lr": 2e-3, "data_s": t_data,
+            "train_ms": e0.elapsed_time(e1), "loss_first50": float(losses[:50].mean()),
+            "loss_last200": float(losses[-200:].mean()), "status": dn.status()}
+    return dn, info
+
+
+def denoise_arm(args):
+    """The denoiser end to end on one GPU: train it (train_denoiser), then on
+    held-out 512^2 scenes compare RMSE and device time of 16 spp + denoiser
+    against plain final gathers of 16-1024 spp, all against an 8192 spp
+    bake."""
+    import torch
+    from relight_b200 import denoise as D
+    torch.cuda.set_device(0)
+    n_eval = 2 if SMALL else 4
+    dn, info = train_denoiser(SMALL)
+    with ClockSampler(0) as clocks:
+        ev = D.evaluate(dn, D.training_scenes(n_eval, seed=900, sides=(512,)), spp_lo=16)
+    dn_ms = ev["denoised"][1]
+    return {
+        "metric": DENOISE_METRIC, "value": 1e3 / dn_ms, "unit": "lightmaps/s", "n_gpus": 1, "steps": n_eval,
+        "warmup": 0, "ms_per_step": dn_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "bf16 (network), f32 (baker)", "data": "synthetic (seeded heightfield + boxes)",
+        "config": {"workload": f"train on {info['patches']} 64x64 patches from {info['scenes']} scenes "
+                               f"(256-512^2 lightmaps), evaluate on {n_eval} held-out 512^2 lightmaps",
+                   "spp_low": 16, "spp_train_target": 1024, "spp_ref": 8192},
+        "plain_at_equal_rmse": {"spp": ev["equal_rmse_spp"], "extrapolated": ev["extrapolated"],
+                                "ms": ev["plain_ms_at_equal_rmse"], "lightmaps_per_s": 1e3 / ev["plain_ms_at_equal_rmse"]},
+        "speedup_at_equal_rmse": ev["speedup"],
+        "rmse": {"denoised_16spp": ev["denoised"][0], **{f"plain_{k}spp": v[0] for k, v in ev["plain"].items()}},
+        "denoised_max_err": ev["denoised_max_err"],
+        "ms": {"denoised_16spp": dn_ms, **{f"plain_{k}spp": v[1] for k, v in ev["plain"].items()}},
+        "train": info, "clocks": clocks.summary(),
+    }
+
+
+SERVE_METRIC = "bake-serving p99 latency at 100 req/s (Poisson; direct + AO 64 + FG 16 spp + denoiser per request)"
 
 
 def serve_arm(args):
-    """Bake serving on one GPU: 32 resident scenes (log-uniform 1k-500k
-    triangles, BVH + gathered photonmap each), requests with log-uniform
-    32^2-1024^2 lightmaps arriving as Poisson streams at 20, 50 and 100
-    requests/s, admitted by a 16 GiB HBM budget and continuously batched.
-    Latency is arrival to colours-in-host-memory on the host clock; a
-    closed-loop run (all requests queued at once) gives the saturated
-    throughput."""
+    """Bake serving on one GPU with the denoiser in the loop: 32 resident
+    scenes (log-uniform 1k-500k triangles, BVH + gathered photonmap each),
+    requests with log-uniform 32^2-1024^2 lightmaps arriving as Poisson
+    streams at 20, 50 and 100 requests/s, admitted by a 16 GiB HBM budget
+    and continuously batched; direct light + AO 64 + final gather 16 spp,
+    the final gather denoised at completion.  Latency is arrival to colours
+    in host memory on the host clock.  A closed-loop run (all requests
+    queued at once) gives the saturated throughput, compared with the plain
+    per-job GPU path at the final-gather sample count whose RMSE (against an
+    8192 spp bake) equals the denoised one."""
     import torch
-    from relight_b200 import batch, scenes, serve
+    from dataclasses import replace
+    from relight_b200 import batch, denoise as D, scenes, serve
+    from relight_b200.device import DeviceMap
     torch.cuda.set_device(0)
     n_scenes = 8 if SMALL else 32
     n_req = 40 if SMALL else 300
+    t0 = time.perf_counter()
+    dn, info = train_denoiser(SMALL)
+    ev = D.evaluate(dn, D.training_scenes(2 if SMALL else 3, seed=900, sides=(512,)), spp_lo=16)
+    t_denoiser = time.perf_counter() - t0
+    # the plain path runs at the equal-RMSE sample count, capped at the largest one measured
+    eq_spp = int(round(min(ev["equal_rmse_spp"], max(ev["plain"]))))
     wl = scenes.batch_workload(n_jobs=1, n_scenes=n_scenes)
-    ts = torch.cuda.Stream()
-    rs = batch.make_resident_scenes(wl, stream=ts.cuda_stream)
-    ts.synchronize()
+    ts_ = torch.cuda.Stream()
+    rs = batch.make_resident_scenes(wl, stream=ts_.cuda_stream)
+    ts_.synchronize()
     budget = 16 << 30
-    srv = serve.BakeServer(rs, budget_bytes=budget, quantum=1 << 18, fg_samples=16, torch_stream=ts)
+    srv = serve.BakeServer(rs, budget_bytes=budget, quantum=1 << 18, fg_samples=16, torch_stream=ts_, denoiser=dn)
     srv.warm()
     srv.run(serve.make_requests(wl, 1000.0, max(args.warmup, 3) * 4, seed=99))  # warm-up
     rates = {}
@@ -448,19 +518,44 @@ def serve_arm(args):
         for rate in (20.0, 50.0, 100.0):
             st = srv.run(serve.make_requests(wl, rate, n_req, seed=int(rate)), keep_results=False)
             rates[str(int(rate))] = st.as_dict()
-        closed = serve.make_requests(wl, 1e9, n_req, seed=7)
-        sat = srv.run(closed, keep_results=False).as_dict()
+        sat = srv.run(serve.make_requests(wl, 1e9, n_req, seed=7), keep_results=False).as_dict()
     srv.close()
+    # the plain per-job GPU path at the equal-RMSE sample count, device time
+    n_plain = 16 if SMALL else 48
+    jobs, maps = [], []
+    for r in serve.make_requests(wl, 1e9, n_plain, seed=7):
+        ds = rs.scenes[r.scene]
+        lm = DeviceMap(0, r.side, r.side)
+        for mi in range(len(ds.flat.mesh_photonmap)):
+            lm.add_mesh(ds, mi)
+        maps.append(lm)
+        fg = replace(wl.scenes[r.scene].settings, final_gather_samples=eq_spp)
+        jobs += [batch.BakeJob.direct(ds, lm), batch.BakeJob.ambient_occlusion(ds, lm, wl.ao, seed=r.seed ^ 0xA0),
+                 batch.BakeJob.indirect(ds, lm, rs.photonmaps[r.scene], fg, seed=r.seed ^ 0xF6)]
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    batch.run_per_job(jobs)
+    e1.record()
+    torch.cuda.synchronize()
+    plain_lps = n_plain / (e0.elapsed_time(e1) / 1e3)
     p99 = rates["100"]["p99_ms"]
     return {
         "metric": SERVE_METRIC, "value": p99, "unit": "ms", "n_gpus": 1, "steps": n_req, "warmup": args.warmup,
         "ms_per_step": rates["100"]["mean_ms"], "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32", "data": "synthetic (seeded heightfield + boxes, Poisson arrivals)",
+        "dtype": "f32 (baker), bf16 (denoiser)", "data": "synthetic (seeded heightfield + boxes, Poisson arrivals)",
         "config": {"workload": f"{n_req} requests per rate over {n_scenes} resident scenes, lightmaps log-uniform "
-                               f"32^2-1024^2, direct + AO 64 + FG 16 spp",
+                               f"32^2-1024^2, direct + AO 64 + FG 16 spp + denoiser",
                    "hbm_budget_bytes": budget, "resident_scene_bytes": rs.nbytes(), "quantum_lumels": 1 << 18,
                    "latency_clock": "host (arrival to colours in pinned host memory)"},
-        "rates": rates, "saturated": sat, "clocks": clocks.summary(),
+        "rates": rates, "saturated": sat,
+        "denoiser": {"rmse_denoised_16spp": ev["denoised"][0], "max_err": ev["denoised_max_err"],
+                     "equal_rmse_spp": ev["equal_rmse_spp"], "extrapolated": ev["extrapolated"], "spp_ref": 8192,
+                     "rmse_plain": {str(k): v[0] for k, v in ev["plain"].items()}, "train": info,
+                     "setup_s": t_denoiser},
+        "plain_per_job_at_equal_rmse": {"fg_spp": eq_spp, "lightmaps_per_s": plain_lps, "requests": n_plain},
+        "speedup_vs_plain_at_equal_rmse": sat["lightmaps_per_s"] / plain_lps,
+        "clocks": clocks.summary(),
     }
 
 
@@ -472,9 +567,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--small", action="store_true", help="512^2 / 64 spp / 2 passes case for ncu captures")
-    ap.add_argument("--workload", default="terrain", choices=["terrain", "batch", "serve"],
+    ap.add_argument("--workload", default="terrain", choices=["terrain", "batch", "serve", "denoise"],
                     help="terrain: the photon + final-gather bake (default); batch: uneven-size batching; "
-                         "serve: the bake-serving loop")
+                         "serve: the bake-serving loop with the denoiser; denoise: the denoiser at equal RMSE")
     args = ap.parse_args()
     global SMALL
     SMALL = args.small
@@ -483,6 +578,9 @@ def main():
         return
     if args.workload == "serve":
         print(json.dumps(serve_arm(args)), flush=True)
+        return
+    if args.workload == "denoise":
+        print(json.dumps(denoise_arm(args)), flush=True)
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

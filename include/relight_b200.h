@@ -290,9 +290,10 @@ int rl_obj_mesh_destroy(rl_obj_mesh* mesh);
    3*(dy+1) + (dx+1), each input segment's channels starting at a multiple
    of 64 (zero-padded).  Accumulator columns
    [outK_c0, outK_c0 + outK_cn) go to outK (channel stride outK_cs), times
-   (maskK > 0) when maskK is given; in1/out1 may be NULL. */
+   (maskK > 0 ? 1 : slope) when maskK is given; relu != 0 applies a leaky
+   ReLU of negative slope `slope` (0: ReLU); in1/out1 may be NULL. */
 int rl_dn_conv3x3(const void* in0, int c0, const void* in1, int c1, int width, int height, int images,
-                  const void* weights, int ncols, const float* bias, int relu, void* out0, int out0_c0,
+                  const void* weights, int ncols, const float* bias, int relu, float slope, void* out0, int out0_c0,
                   int out0_cn, int out0_cs, const void* mask0, void* out1, int out1_c0, int out1_cn, int out1_cs,
                   const void* mask1, int* d_err, void* stream);
 /* dw[co][tap][ci_off + ci] += sum_p grad[p][co] * in[p + offset(tap)][ci]
@@ -301,7 +302,8 @@ int rl_dn_conv3x3_wgrad(const void* grad, int cout, int grad_cs, const void* in,
                         int height, int images, float* dw, int ci_off, int ci_total, int* d_err, void* stream);
 
 /* The denoiser network: 8 convolutions over 4 levels (32, 64, 96, 128
-   channels; 2x2 average pooling, nearest upsampling, skip concatenation),
+   channels, leaky ReLU; 2x2 average pooling, nearest upsampling, skip
+   concatenation),
    input features [h][w][16] = (log1p noisy rgb, normal, albedo, valid, 0),
    output = residual on log1p rgb.  Parameters are FP32 masters updated by
    Adam; the convolutions run in BF16 on the tensor cores. */
@@ -329,6 +331,9 @@ int rl_denoiser_apply(rl_denoiser* dn, const rl_scene* scene, rl_map* lightmap, 
 /* Raw network output (BF16 [n][h][w][16]) for features d_x. */
 int rl_denoiser_forward(rl_denoiser* dn, const void* d_x, int images, int height, int width, void* d_y,
                         void* stream);
+/* Size the working buffers for inputs up to images x height x width (and the
+   training gradients when train != 0), so later calls do not allocate. */
+int rl_denoiser_reserve(rl_denoiser* dn, int images, int height, int width, int train);
 /* Bits set by bounded waits that ran out in the denoiser's kernels (0 = none). */
 int rl_denoiser_status(rl_denoiser* dn, int* flags);
 

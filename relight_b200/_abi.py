@@ -126,8 +126,8 @@ SIGNATURES = {
     "rl_obj_mesh_counts": (_I, [_P, _P, _P, _P]),
     "rl_obj_mesh_arrays": (_I, [_P, _P, _P, _P, _P]),
     "rl_obj_mesh_destroy": (_I, [_P]),
-    "rl_dn_conv3x3": (_I, [_P, _I, _P, _I, _I, _I, _I, _P, _I, _P, _I, _P, _I, _I, _I, _P, _P, _I, _I, _I, _P,
-                           _P, _P]),
+    "rl_dn_conv3x3": (_I, [_P, _I, _P, _I, _I, _I, _I, _P, _I, _P, _I, _F, _P, _I, _I, _I, _P, _P, _I, _I, _I,
+                           _P, _P, _P]),
     "rl_dn_conv3x3_wgrad": (_I, [_P, _I, _I, _P, _I, _I, _I, _I, _I, _P, _I, _I, _P, _P]),
     "rl_denoiser_create": (_I, [_U64, _P]),
     "rl_denoiser_destroy": (_I, [_P]),
@@ -141,6 +141,7 @@ SIGNATURES = {
     "rl_denoiser_apply": (_I, [_P, _P, _P, _P, _P]),
     "rl_denoiser_forward": (_I, [_P, _P, _I, _I, _I, _P, _P]),
     "rl_denoiser_status": (_I, [_P, _P]),
+    "rl_denoiser_reserve": (_I, [_P, _I, _I, _I, _I]),
     "rl_batch_create": (_I, [_P, _I, _P]),
     "rl_batch_update": (_I, [_P, _P, _I, _P]),
     "rl_map_bytes": (_I, [_I, _I, _P]),

@@ -191,11 +191,12 @@ struct ConvArgs {
     int tmem_cols;         // power of two >= max(32, ncols)
     int stages;
     const float* bias;     // [ncols] or null
-    int relu;
+    int relu;              // leaky ReLU with negative slope `slope` (0: ReLU)
+    float slope;
     // output segments: accumulator columns [c0, c0 + cn) -> tensor out (cstride channels)
     bf16* out[2];
     int out_c0[2], out_cn[2], out_cs[2];
-    const bf16* mask[2];   // optional: out *= (mask > 0), same layout as out
+    const bf16* mask[2];   // optional: out *= (mask > 0 ? 1 : slope), same layout as out
     int nout;
     int* err;
 };
@@ -290,7 +291,7 @@ __global__ void __launch_bounds__(128, 2) k_conv3x3(const __grid_constant__ CUte
             for (int i = 0; i < 16; i++) {
                 float x = __uint_as_float(r[i]);
                 if (a.bias) x += a.bias[c + i];
-                if (a.relu) x = fmaxf(x, 0.0f);
+                if (a.relu && !(x > 0.0f)) x *= a.slope;
                 v[i] = x;
             }
             const long long off = pix * a.out_cs[o] + oc;
@@ -301,8 +302,8 @@ __global__ void __launch_bounds__(128, 2) k_conv3x3(const __grid_constant__ CUte
                 const bf16* mb1 = reinterpret_cast<const bf16*>(&m1);
 #pragma unroll
                 for (int i = 0; i < 8; i++) {
-                    if (!(__bfloat162float(mb0[i]) > 0.0f)) v[i] = 0.0f;
-                    if (!(__bfloat162float(mb1[i]) > 0.0f)) v[8 + i] = 0.0f;
+                    if (!(__bfloat162float(mb0[i]) > 0.0f)) v[i] *= a.slope;
+                    if (!(__bfloat162float(mb1[i]) > 0.0f)) v[8 + i] *= a.slope;
                 }
             }
             uint4 w0, w1;
@@ -501,7 +502,8 @@ int conv_smem(int ncols, int stages) { return stages * (int)(kABytes + ncols * 1
 
 // One 3x3 "same" convolution over NHWC BF16 tensors (see the header).
 extern "C" int rl_dn_conv3x3(const void* in0, int c0, const void* in1, int c1, int width, int height, int images,
-                             const void* weights, int ncols, const float* bias, int relu, void* out0, int out0_c0,
+                             const void* weights, int ncols, const float* bias, int relu, float slope, void* out0,
+                             int out0_c0,
                              int out0_cn, int out0_cs, const void* mask0, void* out1, int out1_c0, int out1_cn,
                              int out1_cs, const void* mask1, int* d_err, void* stream) {
     if (!in0 || !weights || !out0 || width <= 0 || height <= 0 || images <= 0)
@@ -528,6 +530,7 @@ extern "C" int rl_dn_conv3x3(const void* in0, int c0, const void* in1, int c1, i
     a.stages = ncols > 128 ? 2 : 3;  // two CTAs per SM
     a.bias = bias;
     a.relu = relu;
+    a.slope = slope;
     a.nout = nout;
     a.out[0] = (bf16*)out0;
     a.out[1] = (bf16*)out1;
@@ -597,6 +600,7 @@ extern "C" int rl_dn_conv3x3_wgrad(const void* grad, int cout, int grad_cs, cons
 
 // ================================================================ network
 //
+// (relu = leaky ReLU, negative slope 0.1)
 //   x (16: log1p noisy rgb, normal, albedo, valid)
 //   e0 = relu(c0(x))            32  full       p0 = pool(e0)
 //   e1 = relu(c1(p0))           64  1/2        p1 = pool(e1)
@@ -612,6 +616,7 @@ extern "C" int rl_dn_conv3x3_wgrad(const void* grad, int cout, int grad_cs, cons
 namespace {
 
 constexpr int kFeat = 16;
+constexpr float kLeak = 0.1f;  // leaky ReLU slope: no unit can die
 
 __device__ __forceinline__ float bf(bf16 v) { return __bfloat162float(v); }
 
@@ -637,8 +642,8 @@ __global__ void k_dn_pool(const bf16* in, bf16* out, int C, int W, int H, int N)
     }
 }
 
-// gin += (gout / children) * (mask > 0), gin and mask at the fine size.
-__global__ void k_dn_pool_bwd(const bf16* gout, const bf16* mask, bf16* gin, int C, int W, int H, int N) {
+// gin += (gout / children) * (mask > 0 ? 1 : slope), gin and mask at the fine size.
+__global__ void k_dn_pool_bwd(const bf16* gout, const bf16* mask, bf16* gin, int C, int W, int H, int N, float slope) {
     const int W2 = (W + 1) / 2, H2 = (H + 1) / 2;
     const long long total = (long long)N * H * W * C;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
@@ -648,7 +653,7 @@ __global__ void k_dn_pool_bwd(const bf16* gout, const bf16* mask, bf16* gin, int
         int x2 = x / 2, y2 = y / 2;
         int cnt = (2 * x2 + 1 < W ? 2 : 1) * (2 * y2 + 1 < H ? 2 : 1);
         float g = bf(gout[(((long long)n * H2 + y2) * W2 + x2) * C + c]) / cnt;
-        if (!(bf(mask[i]) > 0.f)) g = 0.f;
+        if (!(bf(mask[i]) > 0.f)) g *= slope;
         gin[i] = __float2bfloat16(bf(gin[i]) + g);
     }
 }
@@ -924,18 +929,18 @@ int alloc_shapes(rl_denoiser* d, int n, int h, int w, bool train, cudaStream_t s
 int conv_fwd(rl_denoiser* d, int l, const bf16* in0, const bf16* in1, int w, int h, int n, bf16* out, bool relu,
              cudaStream_t st) {
     Conv& c = d->conv[l];
-    return rl_dn_conv3x3(in0, c.segs[0], in1, c.segs[1], w, h, n, c.wp, c.ncols, c.bias, relu ? 1 : 0, out, 0,
+    return rl_dn_conv3x3(in0, c.segs[0], in1, c.segs[1], w, h, n, c.wp, c.ncols, c.bias, relu ? 1 : 0, kLeak, out, 0,
                          c.ncols, c.ncols, nullptr, nullptr, 0, 0, 0, nullptr, d->d_err, st);
 }
 
 // Data gradient of layer l: gout (ncols stored) -> g0 (segment 0) / g1,
-// each masked by the matching forward input (relu outputs; the upsampled
-// inputs carry their source's sign).
+// each scaled by the leaky-ReLU derivative of the matching forward input
+// (the activation keeps the sign; upsampled inputs carry their source's).
 int conv_dgrad(rl_denoiser* d, int l, const bf16* gout, int w, int h, int n, bf16* g0, const bf16* m0, bf16* g1,
                const bf16* m1, cudaStream_t st) {
     Conv& c = d->conv[l];
-    return rl_dn_conv3x3(gout, c.ncols, nullptr, 0, w, h, n, c.wt, c.kpad, nullptr, 0, g0, 0, c.segs[0], c.segs[0],
-                         m0, g1, pad64(c.segs[0]), g1 ? c.segs[1] : 0, g1 ? c.segs[1] : 0, m1, d->d_err, st);
+    return rl_dn_conv3x3(gout, c.ncols, nullptr, 0, w, h, n, c.wt, c.kpad, nullptr, 0, kLeak, g0, 0, c.segs[0],
+                         c.segs[0], m0, g1, pad64(c.segs[0]), g1 ? c.segs[1] : 0, g1 ? c.segs[1] : 0, m1, d->d_err, st);
 }
 
 int conv_wgrad(rl_denoiser* d, int l, const bf16* gout, const bf16* in0, const bf16* in1, int w, int h, int n,
@@ -994,7 +999,7 @@ int backward(rl_denoiser* d, int n, int h, int w, cudaStream_t st) {
     };
     auto pool_bwd = [&](const bf16* gcoarse, const bf16* mask, bf16* gfine, int c, int lvl) {
         long long tot = (long long)n * L[lvl].w * L[lvl].h * c;
-        k_dn_pool_bwd<<<grid_of(tot, 256), 256, 0, st>>>(gcoarse, mask, gfine, c, L[lvl].w, L[lvl].h, n);
+        k_dn_pool_bwd<<<grid_of(tot, 256), 256, 0, st>>>(gcoarse, mask, gfine, c, L[lvl].w, L[lvl].h, n, kLeak);
     };
     int rc;
     const int W0 = L[0].w, H0 = L[0].h;
@@ -1249,6 +1254,13 @@ extern "C" int rl_denoiser_forward(rl_denoiser* d, const void* d_x, int images, 
     DN_CK(cudaMemcpyAsync(d->x, d_x, P * kFeat * sizeof(bf16), cudaMemcpyDeviceToDevice, st));
     if (int rc = forward(d, images, height, width, st)) return rc;
     DN_CK(cudaMemcpyAsync(d_y, d->y, P * kFeat * sizeof(bf16), cudaMemcpyDeviceToDevice, st));
+    return RL_OK;
+}
+
+extern "C" int rl_denoiser_reserve(rl_denoiser* d, int images, int height, int width, int train) {
+    if (!d || images <= 0 || height <= 0 || width <= 0) return dn_fail(RL_INVALID_CALL, "rl_denoiser_reserve: bad arguments");
+    if (int rc = alloc_shapes(d, images, height, width, train != 0, 0)) return rc;
+    DN_CK(cudaDeviceSynchronize());
     return RL_OK;
 }
 

@@ -15,16 +15,21 @@ from ._abi import check, lib
 
 
 def _p(t):
-    return None if t is None else C.c_void_p(t.data_ptr())
+    if t is None:
+        return None
+    if isinstance(t, int):
+        return C.c_void_p(t)
+    return C.c_void_p(t.data_ptr())
 
 
 def conv3x3(in0, weights, ncols, bias=None, relu=False, in1=None, out0=None, out0_c0=0, out0_cn=None,
-            mask0=None, out1=None, out1_c0=0, out1_cn=0, mask1=None, err=None, stream=None):
+            mask0=None, out1=None, out1_c0=0, out1_cn=0, mask1=None, err=None, stream=None, slope=0.0):
     """One 3x3 'same' convolution (rl_dn_conv3x3); in/out [n][h][w][c]."""
     n, h, w, c0 = in0.shape
     c1 = 0 if in1 is None else in1.shape[-1]
     out0_cn = ncols if out0_cn is None else out0_cn
-    check(lib().rl_dn_conv3x3(_p(in0), c0, _p(in1), c1, w, h, n, _p(weights), ncols, _p(bias), int(relu), _p(out0),
+    check(lib().rl_dn_conv3x3(_p(in0), c0, _p(in1), c1, w, h, n, _p(weights), ncols, _p(bias), int(relu),
+                              float(slope), _p(out0),
                               out0_c0, out0_cn, out0.shape[-1], _p(mask0), _p(out1), out1_c0, out1_cn,
                               0 if out1 is None else out1.shape[-1], _p(mask1), _p(err), stream))
 
@@ -115,6 +120,10 @@ class Denoiser:
     def apply(self, scene, lightmap, base=None, stream=None):
         """Denoise a baked lightmap (DeviceMap) of a DeviceScene in place."""
         check(lib().rl_denoiser_apply(self.handle, scene.handle, lightmap.handle, _p(base), stream))
+
+    def reserve(self, images, height, width, train=False):
+        """Pre-size the working buffers (rl_denoiser_reserve)."""
+        check(lib().rl_denoiser_reserve(self.handle, images, height, width, int(train)))
 
     def status(self) -> int:
         f = C.c_int()
@@ -218,9 +227,10 @@ def make_patches(pairs, count, patch=64, seed=11, min_valid=0.3):
     return torch.stack(xs).contiguous(), torch.stack(ts).contiguous()
 
 
-def train(dn, xs, ts, steps, batch=16, lr=2e-3, seed=5, stream=None, log_every=0):
-    """Adam on random batches of the patch set with a cosine learning-rate
-    decay; returns the per-step losses (mean L1 in log space)."""
+def train(dn, xs, ts, steps, batch=16, lr=2e-3, seed=5, stream=None, warmup=200):
+    """Adam on random batches of the patch set: linear learning-rate warmup
+    over `warmup` steps, then cosine decay; returns the per-step losses
+    (mean L1 in log space)."""
     import math
     import torch
     g = torch.Generator(device="cuda").manual_seed(seed)
@@ -228,7 +238,7 @@ def train(dn, xs, ts, steps, batch=16, lr=2e-3, seed=5, stream=None, log_every=0
     n = xs.shape[0]
     for s in range(steps):
         idx = torch.randint(0, n, (batch,), device="cuda", generator=g)
-        rate = lr * 0.5 * (1 + math.cos(math.pi * s / steps))
+        rate = lr * 0.5 * (1 + math.cos(math.pi * s / steps)) * min(1.0, (s + 1) / max(warmup, 1))
         dn.train_step(xs[idx].contiguous(), ts[idx].contiguous(), rate, loss=loss[s:s + 1], stream=stream)
     return loss.cpu().numpy() * 1.0
 
@@ -238,3 +248,87 @@ def rmse(a, b, valid):
     import numpy as np
     d = (np.asarray(a, np.float64) - np.asarray(b, np.float64))[valid]
     return float(np.sqrt((d * d).mean()))
+
+
+def evaluate(dn, workloads, spp_lo=16, spp_ref=8192, plain=(16, 64, 256, 1024), seed=900, stream=None):
+    """Per-texel RMSE against a `spp_ref` bake (valid lumels, linear colour)
+    of the plain final gather at each sample count in `plain` and of the
+    `spp_lo` bake after the denoiser, with the device time of each (bake,
+    and bake + denoise).  The plain bake's sample count of equal RMSE is
+    interpolated (log-log) inside the measured range, or past its end from
+    the fit RMSE^2 = a / spp + c (c: the reference's own noise and any
+    bias).  Returns {"plain": {spp: (rmse, ms)}, "denoised": (rmse, ms),
+    "denoised_max_err", "equal_rmse_spp", "extrapolated",
+    "plain_ms_at_equal_rmse", "speedup"}."""
+    import numpy as np
+    import torch
+    from .device import Relight
+    ev = lambda: torch.cuda.Event(enable_timing=True)
+    st = torch.cuda.current_stream()
+    acc_plain = {k: [0.0, 0.0, 0] for k in plain}
+    acc_dn = [0.0, 0.0, 0]
+    max_err = 0.0
+    # working buffers sized up front, so no timed call allocates
+    dn.reserve(1, max(w.lightmap.height for w in workloads), max(w.lightmap.width for w in workloads))
+    for i, wl in enumerate(workloads):
+        rl = Relight(stream, seed=seed + i)
+        ds = rl.device_scene(wl.scene)
+        rl.emit_photons(wl.scene, wl.settings)
+        lm = wl.lightmap._device
+        pms = [m._device for m in wl.scene.flat.photonmaps]
+        bake_fg(rl, ds, lm, pms, wl.settings, spp_ref, seed * 13 + i, stream)
+        d = lm.download(stream, fields=("flags", "color"))
+        valid = (d["flags"] & 1).astype(bool)
+        ref = d["color"]
+
+        def timed(fn):
+            e0, e1 = ev(), ev()
+            e0.record(st)
+            fn()
+            e1.record(st)
+            e1.synchronize()
+            return e0.elapsed_time(e1)
+
+        for k in plain:
+            ms = timed(lambda: bake_fg(rl, ds, lm, pms, wl.settings, k, seed * 17 + i * 31 + k, stream))
+            c = lm.download(stream, fields=("color",))["color"]
+            acc_plain[k][0] += rmse(c, ref, valid) ** 2
+            acc_plain[k][1] += ms
+            acc_plain[k][2] += 1
+
+        def lo_and_denoise():
+            bake_fg(rl, ds, lm, pms, wl.settings, spp_lo, seed * 19 + i, stream)
+            dn.apply(ds, lm, stream=stream)
+
+        if i == 0:
+            lo_and_denoise()  # untimed warm-up of the denoiser's kernels
+        ms = timed(lo_and_denoise)
+        c = lm.download(stream, fields=("color",))["color"]
+        acc_dn[0] += rmse(c, ref, valid) ** 2
+        acc_dn[1] += ms
+        acc_dn[2] += 1
+        max_err = max(max_err, float(np.abs(c - ref)[valid].max()) if valid.any() else 0.0)
+    res_plain = {k: (float(np.sqrt(v[0] / v[2])), v[1] / v[2]) for k, v in acc_plain.items()}
+    dn_rmse, dn_ms = float(np.sqrt(acc_dn[0] / acc_dn[2])), acc_dn[1] / acc_dn[2]
+    ks = sorted(res_plain)
+    r = np.array([res_plain[k][0] for k in ks])
+    extrapolated = False
+    if dn_rmse >= r[0]:
+        s_eq = float(ks[0])
+    elif dn_rmse >= r[-1]:
+        j = int(np.argmax(r <= dn_rmse))
+        lk0, lk1 = np.log(ks[j - 1]), np.log(ks[j])
+        f = (np.log(dn_rmse) - np.log(r[j - 1])) / (np.log(r[j]) - np.log(r[j - 1]))
+        s_eq = float(np.exp(lk0 + f * (lk1 - lk0)))
+    else:
+        # least squares of RMSE^2 = a / spp + c over the measured counts
+        A = np.stack([1.0 / np.array(ks, float), np.ones(len(ks))], 1)
+        (a, c0), *_ = np.linalg.lstsq(A, r * r, rcond=None)
+        extrapolated = True
+        s_eq = float(a / (dn_rmse ** 2 - c0)) if dn_rmse ** 2 > c0 and a > 0 else float("inf")
+    ms = np.array([res_plain[k][1] for k in ks])
+    a1, b1 = np.polyfit(np.array(ks, float), ms, 1)  # bake time is linear in samples
+    plain_ms_eq = float(a1 * s_eq + b1) if np.isfinite(s_eq) else float("inf")
+    return {"plain": res_plain, "denoised": (dn_rmse, dn_ms), "denoised_max_err": max_err,
+            "equal_rmse_spp": s_eq, "extrapolated": extrapolated, "plain_ms_at_equal_rmse": plain_ms_eq,
+            "speedup": plain_ms_eq / dn_ms}

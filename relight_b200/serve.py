@@ -128,6 +128,7 @@ class _Active:
     total: int
     cursor: int = 0
     host: object = None  # pinned tensor for the colours
+    fg_map: object = None  # with a denoiser: the final gather, denoised on completion
 
 
 @dataclass
@@ -158,7 +159,7 @@ class BakeServer:
     """
 
     def __init__(self, resident: ResidentScenes, budget_bytes: int, quantum: int = 1 << 18,
-                 fg_samples: int = 16, max_active: int = 256, torch_stream=None):
+                 fg_samples: int = 16, max_active: int = 256, torch_stream=None, denoiser=None, max_side: int = 1024):
         import torch
         from .device import DeviceMap
         self.rs = resident
@@ -169,7 +170,11 @@ class BakeServer:
         self.torch_stream = torch_stream or torch.cuda.Stream()
         self.stream = self.torch_stream.cuda_stream
         self.fg = [replace(sc.settings, final_gather_samples=fg_samples) for sc in self.wl.scenes]
-        self._map_bytes = DeviceMap.nbytes
+        self.denoiser = denoiser
+        if denoiser is not None:
+            denoiser.reserve(1, max_side, max_side)
+        maps = 2 if denoiser is not None else 1
+        self._map_bytes = lambda w, h: maps * DeviceMap.nbytes(w, h)
         self.pinned = PinnedPool()
         self.batch = Batch([])
         self.batch.capture(self.stream)
@@ -180,9 +185,10 @@ class BakeServer:
         r = a.req
         ds = self.rs.scenes[r.scene]
         kw = dict(begin=begin, end=end)
+        fg_map = a.fg_map if a.fg_map is not None else a.lightmap
         return [BakeJob.direct(ds, a.lightmap, **kw),
                 BakeJob.ambient_occlusion(ds, a.lightmap, self.wl.ao, seed=r.seed ^ 0xA0, **kw),
-                BakeJob.indirect(ds, a.lightmap, self.rs.photonmaps[r.scene], self.fg[r.scene],
+                BakeJob.indirect(ds, fg_map, self.rs.photonmaps[r.scene], self.fg[r.scene],
                                  seed=r.seed ^ 0xF6, **kw)]
 
     def _admit(self, r: Request, now: float) -> _Active:
@@ -192,9 +198,14 @@ class BakeServer:
         lm = DeviceMap(0, r.side, r.side, stream=self.stream, stream_ordered=True)
         for mi in range(len(ds.flat.mesh_photonmap)):
             lm.add_mesh(ds, mi, self.stream)
+        fg = None
+        if self.denoiser is not None:
+            fg = DeviceMap(0, r.side, r.side, stream=self.stream, stream_ordered=True)
+            for mi in range(len(ds.flat.mesh_photonmap)):
+                fg.add_mesh(ds, mi, self.stream)
         r.t_admit = now
         host = self.pinned.get(r.side * r.side * 12)
-        return _Active(r, lm, r.side * r.side, 0, host)
+        return _Active(r, lm, r.side * r.side, 0, host, fg)
 
     # -------------------------------------------------------------- loop
     def run(self, requests: Sequence[Request], clock: Optional[Callable[[], float]] = None,
@@ -252,8 +263,16 @@ class BakeServer:
                 self.batch.update(jobs, self.stream)
                 self.batch.replay(self.stream)
                 for a in fin:
-                    a.lightmap.download_color_async(a.host.data_ptr(), self.stream)
+                    out = a.lightmap
+                    if a.fg_map is not None:
+                        # final = (direct, AO) + denoised final gather
+                        self.denoiser.apply(self.rs.scenes[a.req.scene], a.fg_map,
+                                            base=a.lightmap.device_arrays()["color"], stream=self.stream)
+                        out = a.fg_map
+                    out.download_color_async(a.host.data_ptr(), self.stream)
                     a.lightmap.close(self.stream)
+                    if a.fg_map is not None:
+                        a.fg_map.close(self.stream)
                 ev = torch.cuda.Event()
                 ev.record(self.torch_stream)
                 inflight.append((ev, fin))
@@ -294,9 +313,11 @@ class BakeServer:
         self.batch.close()
 
 
-def bake_alone(resident: ResidentScenes, r: Request, fg_samples: int = 16, stream=None) -> np.ndarray:
+def bake_alone(resident: ResidentScenes, r: Request, fg_samples: int = 16, stream=None,
+               denoiser=None) -> np.ndarray:
     """The request baked by itself through the single-job calls (the
-    reference for the alone-vs-in-the-mix check)."""
+    reference for the alone-vs-in-the-mix check); with a denoiser, the
+    final gather goes to its own map, denoised onto the direct + AO map."""
     from .batch import run_per_job
     from .device import DeviceMap
     ds = resident.scenes[r.scene]
@@ -304,11 +325,20 @@ def bake_alone(resident: ResidentScenes, r: Request, fg_samples: int = 16, strea
     lm = DeviceMap(0, r.side, r.side)
     for mi in range(len(ds.flat.mesh_photonmap)):
         lm.add_mesh(ds, mi, stream)
+    fgm = lm
+    if denoiser is not None:
+        fgm = DeviceMap(0, r.side, r.side)
+        for mi in range(len(ds.flat.mesh_photonmap)):
+            fgm.add_mesh(ds, mi, stream)
     fg = replace(wl.scenes[r.scene].settings, final_gather_samples=fg_samples)
     jobs = [BakeJob.direct(ds, lm),
             BakeJob.ambient_occlusion(ds, lm, wl.ao, seed=r.seed ^ 0xA0),
-            BakeJob.indirect(ds, lm, resident.photonmaps[r.scene], fg, seed=r.seed ^ 0xF6)]
+            BakeJob.indirect(ds, fgm, resident.photonmaps[r.scene], fg, seed=r.seed ^ 0xF6)]
     run_per_job(jobs, stream)
-    out = lm.download(stream, fields=("color",))["color"]
+    if denoiser is not None:
+        denoiser.apply(ds, fgm, base=lm.device_arrays()["color"], stream=stream)
+    out = fgm.download(stream, fields=("color",))["color"]
     lm.close()
+    if fgm is not lm:
+        fgm.close()
     return out

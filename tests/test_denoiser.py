@@ -28,7 +28,7 @@ def _torch_net(x, layers):
         cout, _, k = w.shape
         wt = w.reshape(cout, 3, 3, k).permute(0, 3, 1, 2)
         o = F.conv2d(z, wt, b, padding=1)
-        return torch.relu(o) if relu else o
+        return F.leaky_relu(o, 0.1) if relu else o
 
     def pool(t):
         return F.avg_pool2d(t, 2, ceil_mode=True, count_include_pad=False)

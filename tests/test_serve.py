@@ -69,3 +69,26 @@ def test_serve_alone_equals_mix(cuda):
         want = serve.bake_alone(rs, r, fg_samples=16)
         assert np.array_equal(r.result.view(np.uint32), want.view(np.uint32)), f"request {r.rid}"
         assert r.t_admit >= r.arrival and r.t_done >= r.t_admit
+
+
+@pytest.mark.gpu
+def test_serve_denoised_alone_equals_mix(cuda):
+    """With the denoiser in the loop (final gather to its own map, denoised
+    onto direct + AO at completion) each result is still the same bits alone
+    and in the mix."""
+    from relight_b200 import batch
+    from relight_b200.denoise import Denoiser
+    from relight_b200.device import DeviceMap
+    wl = scenes.batch_workload(n_jobs=1, n_scenes=2, seed=12, tris=(1_000, 10_000), sides=(24, 96),
+                               ao_samples=8, fg_samples=16, photon_map=64)
+    rs = batch.make_resident_scenes(wl)
+    dn = Denoiser(seed=2)
+    reqs = serve.make_requests(wl, rate=2000.0, n=8, seed=4, sides=(24, 130))
+    srv = serve.BakeServer(rs, budget_bytes=6 * DeviceMap.nbytes(130, 130), quantum=4096, denoiser=dn, max_side=130)
+    stats = srv.run(reqs)
+    srv.close()
+    assert stats.requests == len(reqs) and dn.status() == 0
+    for r in reqs:
+        want = serve.bake_alone(rs, r, fg_samples=16, denoiser=dn)
+        assert np.array_equal(r.result.view(np.uint32), want.view(np.uint32)), f"request {r.rid}"
+    dn.close()

@@ -620,71 +620,101 @@ constexpr float kLeak = 0.1f;  // leaky ReLU slope: no unit can die
 
 __device__ __forceinline__ float bf(bf16 v) { return __bfloat162float(v); }
 
+// The resampling kernels move 8 channels (16 bytes) per thread: C is a
+// multiple of 8, and each thread decodes its pixel once.
+union Pack8 {
+    uint4 u;
+    bf16 h[8];
+};
+
 // 2x2 average pooling; odd edges average the children that exist.
 __global__ void k_dn_pool(const bf16* in, bf16* out, int C, int W, int H, int N) {
-    const int W2 = (W + 1) / 2, H2 = (H + 1) / 2;
-    const long long total = (long long)N * H2 * W2 * C;
+    const int W2 = (W + 1) / 2, H2 = (H + 1) / 2, G = C / 8;
+    const long long total = (long long)N * H2 * W2 * G;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
-        int c = (int)(i % C);
-        long long p = i / C;
+        int g = (int)(i % G);
+        long long p = i / G;
         int x = (int)(p % W2), y = (int)((p / W2) % H2), n = (int)(p / ((long long)W2 * H2));
-        float s = 0.f;
+        float s[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         int cnt = 0;
         for (int dy = 0; dy < 2; dy++)
             for (int dx = 0; dx < 2; dx++) {
                 int xx = 2 * x + dx, yy = 2 * y + dy;
                 if (xx < W && yy < H) {
-                    s += bf(in[(((long long)n * H + yy) * W + xx) * C + c]);
+                    Pack8 v;
+                    v.u = reinterpret_cast<const uint4*>(in + (((long long)n * H + yy) * W + xx) * C)[g];
+#pragma unroll
+                    for (int k = 0; k < 8; k++) s[k] += bf(v.h[k]);
                     cnt++;
                 }
             }
-        out[i] = __float2bfloat16(s / cnt);
+        Pack8 o;
+#pragma unroll
+        for (int k = 0; k < 8; k++) o.h[k] = __float2bfloat16(s[k] / cnt);
+        reinterpret_cast<uint4*>(out)[i] = o.u;
     }
 }
 
 // gin += (gout / children) * (mask > 0 ? 1 : slope), gin and mask at the fine size.
 __global__ void k_dn_pool_bwd(const bf16* gout, const bf16* mask, bf16* gin, int C, int W, int H, int N, float slope) {
-    const int W2 = (W + 1) / 2, H2 = (H + 1) / 2;
-    const long long total = (long long)N * H * W * C;
+    const int W2 = (W + 1) / 2, H2 = (H + 1) / 2, G = C / 8;
+    const long long total = (long long)N * H * W * G;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
-        int c = (int)(i % C);
-        long long p = i / C;
+        int g = (int)(i % G);
+        long long p = i / G;
         int x = (int)(p % W), y = (int)((p / W) % H), n = (int)(p / ((long long)W * H));
         int x2 = x / 2, y2 = y / 2;
-        int cnt = (2 * x2 + 1 < W ? 2 : 1) * (2 * y2 + 1 < H ? 2 : 1);
-        float g = bf(gout[(((long long)n * H2 + y2) * W2 + x2) * C + c]) / cnt;
-        if (!(bf(mask[i]) > 0.f)) g *= slope;
-        gin[i] = __float2bfloat16(bf(gin[i]) + g);
+        float inv = 1.0f / ((2 * x2 + 1 < W ? 2 : 1) * (2 * y2 + 1 < H ? 2 : 1));
+        Pack8 go, m, gi;
+        go.u = reinterpret_cast<const uint4*>(gout + (((long long)n * H2 + y2) * W2 + x2) * C)[g];
+        m.u = reinterpret_cast<const uint4*>(mask)[i];
+        gi.u = reinterpret_cast<const uint4*>(gin)[i];
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            float v = bf(go.h[k]) * inv;
+            if (!(bf(m.h[k]) > 0.f)) v *= slope;
+            gi.h[k] = __float2bfloat16(bf(gi.h[k]) + v);
+        }
+        reinterpret_cast<uint4*>(gin)[i] = gi.u;
     }
 }
 
 // Nearest 2x upsampling to W x H.
 __global__ void k_dn_up(const bf16* in, bf16* out, int C, int W, int H, int N) {
-    const int W2 = (W + 1) / 2, H2 = (H + 1) / 2;
-    const long long total = (long long)N * H * W * C;
+    const int W2 = (W + 1) / 2, H2 = (H + 1) / 2, G = C / 8;
+    const long long total = (long long)N * H * W * G;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
-        int c = (int)(i % C);
-        long long p = i / C;
+        int g = (int)(i % G);
+        long long p = i / G;
         int x = (int)(p % W), y = (int)((p / W) % H), n = (int)(p / ((long long)W * H));
-        out[i] = in[(((long long)n * H2 + y / 2) * W2 + x / 2) * C + c];
+        reinterpret_cast<uint4*>(out)[i] =
+            reinterpret_cast<const uint4*>(in + (((long long)n * H2 + y / 2) * W2 + x / 2) * C)[g];
     }
 }
 
 // gin (coarse) = sum of the gradients of its children.
 __global__ void k_dn_up_bwd(const bf16* gout, bf16* gin, int C, int W, int H, int N) {
-    const int W2 = (W + 1) / 2, H2 = (H + 1) / 2;
-    const long long total = (long long)N * H2 * W2 * C;
+    const int W2 = (W + 1) / 2, H2 = (H + 1) / 2, G = C / 8;
+    const long long total = (long long)N * H2 * W2 * G;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
-        int c = (int)(i % C);
-        long long p = i / C;
+        int g = (int)(i % G);
+        long long p = i / G;
         int x = (int)(p % W2), y = (int)((p / W2) % H2), n = (int)(p / ((long long)W2 * H2));
-        float s = 0.f;
+        float s[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         for (int dy = 0; dy < 2; dy++)
             for (int dx = 0; dx < 2; dx++) {
                 int xx = 2 * x + dx, yy = 2 * y + dy;
-                if (xx < W && yy < H) s += bf(gout[(((long long)n * H + yy) * W + xx) * C + c]);
+                if (xx < W && yy < H) {
+                    Pack8 v;
+                    v.u = reinterpret_cast<const uint4*>(gout + (((long long)n * H + yy) * W + xx) * C)[g];
+#pragma unroll
+                    for (int k = 0; k < 8; k++) s[k] += bf(v.h[k]);
+                }
             }
-        gin[i] = __float2bfloat16(s);
+        Pack8 o;
+#pragma unroll
+        for (int k = 0; k < 8; k++) o.h[k] = __float2bfloat16(s[k]);
+        reinterpret_cast<uint4*>(gin)[i] = o.u;
     }
 }
 
@@ -963,11 +993,11 @@ int forward(rl_denoiser* d, int n, int h, int w, cudaStream_t st) {
     L[0] = {w, h};
     for (int k = 1; k < 4; k++) L[k] = {(L[k - 1].w + 1) / 2, (L[k - 1].h + 1) / 2};
     auto pool = [&](const bf16* in, bf16* out, int c, int lvl) {
-        long long tot = (long long)n * L[lvl + 1].w * L[lvl + 1].h * c;
+        long long tot = (long long)n * L[lvl + 1].w * L[lvl + 1].h * (c / 8);
         k_dn_pool<<<grid_of(tot, 256), 256, 0, st>>>(in, out, c, L[lvl].w, L[lvl].h, n);
     };
     auto up = [&](const bf16* in, bf16* out, int c, int lvl) {
-        long long tot = (long long)n * L[lvl].w * L[lvl].h * c;
+        long long tot = (long long)n * L[lvl].w * L[lvl].h * (c / 8);
         k_dn_up<<<grid_of(tot, 256), 256, 0, st>>>(in, out, c, L[lvl].w, L[lvl].h, n);
     };
     int rc;
@@ -994,11 +1024,11 @@ int backward(rl_denoiser* d, int n, int h, int w, cudaStream_t st) {
     L[0] = {w, h};
     for (int k = 1; k < 4; k++) L[k] = {(L[k - 1].w + 1) / 2, (L[k - 1].h + 1) / 2};
     auto up_bwd = [&](const bf16* gfine, bf16* gcoarse, int c, int lvl) {
-        long long tot = (long long)n * L[lvl + 1].w * L[lvl + 1].h * c;
+        long long tot = (long long)n * L[lvl + 1].w * L[lvl + 1].h * (c / 8);
         k_dn_up_bwd<<<grid_of(tot, 256), 256, 0, st>>>(gfine, gcoarse, c, L[lvl].w, L[lvl].h, n);
     };
     auto pool_bwd = [&](const bf16* gcoarse, const bf16* mask, bf16* gfine, int c, int lvl) {
-        long long tot = (long long)n * L[lvl].w * L[lvl].h * c;
+        long long tot = (long long)n * L[lvl].w * L[lvl].h * (c / 8);
         k_dn_pool_bwd<<<grid_of(tot, 256), 256, 0, st>>>(gcoarse, mask, gfine, c, L[lvl].w, L[lvl].h, n, kLeak);
     };
     int rc;

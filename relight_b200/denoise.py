@@ -332,3 +332,45 @@ def evaluate(dn, workloads, spp_lo=16, spp_ref=8192, plain=(16, 64, 256, 1024), 
     return {"plain": res_plain, "denoised": (dn_rmse, dn_ms), "denoised_max_err": max_err,
             "equal_rmse_spp": s_eq, "extrapolated": extrapolated, "plain_ms_at_equal_rmse": plain_ms_eq,
             "speedup": plain_ms_eq / dn_ms}
+
+
+def _main():
+    """Time the network's forward pass on a synthetic side x side feature map
+    (CUDA events, after one warm-up pass): the inference a bake request
+    pays.  Used as the profiling target of the convolution kernels."""
+    import argparse
+    import json
+    import torch
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--side", type=int, default=1024)
+    ap.add_argument("--reps", type=int, default=3)
+    args = ap.parse_args()
+    torch.cuda.set_device(0)
+    g = torch.Generator(device="cuda").manual_seed(0)
+    x = torch.zeros(1, args.side, args.side, FEATURES, device="cuda")
+    x[..., :10] = torch.rand(1, args.side, args.side, 10, device="cuda", generator=g)
+    x = x.to(torch.bfloat16)
+    dn = Denoiser(seed=1)
+    dn.forward(x)
+    torch.cuda.synchronize()
+    ms = []
+    for _ in range(args.reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        dn.forward(x)
+        e1.record()
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    # multiply-adds of the 8 convolutions (MMA shapes, padding included)
+    flops, s = 0, args.side
+    sizes = [s, (s + 1) // 2, (s + 3) // 4, (s + 7) // 8]
+    levels = [0, 1, 2, 3, 2, 1, 0, 0]
+    for (cout, segs), lv in zip(LAYERS, levels):
+        k = 9 * sum(_pad64(c) for c in segs)
+        flops += 2 * sizes[lv] ** 2 * ((cout + 15) // 16 * 16) * k
+    print(json.dumps({"side": args.side, "forward_ms": min(ms), "mma_tflops": flops / (min(ms) / 1e3) / 1e12,
+                      "status": dn.status()}))
+
+
+if __name__ == "__main__":
+    _main()

@@ -41,6 +41,9 @@ sys.path.insert(0, ROOT)
 # 48 B ray I/O + 32 B x 43.78 box tests + 48 B x 2.80 triangle tests.
 RAY_MODEL = {"n_box": 43.78, "n_tri": 2.80, "bytes_per_ray": 1583.6}
 METRIC = "lightmap texels/s (photons + gather + final gather 256 spp, 1024^2)"
+# --gather knn: the k-nearest-neighbour photon estimate (k = 100 deposits
+# within a radius cap of 2 world units), run after the disc gather.
+KNN_K, KNN_RADIUS = 100, 2.0
 UNIT = "texels/s"
 WORKLOAD = "terrain 256^2 verts + 2000 boxes (154,050 tris), 1M photons x3 bounces, gather r7, FG 256 spp, 1024^2"
 # DRAM bytes (read + write) of one full-size k_indirect launch, from the ncu
@@ -143,13 +146,27 @@ def gpu_arm(args, rank, world, local_rank):
 
     ev = lambda: torch.cuda.Event(enable_timing=True)
 
+    knn = args.gather == "knn"
+    records = None
+    if knn:
+        from relight_b200.device import PhotonRecords
+        records = PhotonRecords(8 << 20)
+        launches_per_step += 4  # k_knn_keys, radix sort (counted as one), k_knn_scatter, k_knn_query
+
     def step(seed, fg_events=None):
         _abi.check(L.rl_map_clear(pmap.handle, 1, 1, sh))
         _abi.check(L.rl_map_clear(lmap.handle, 1, 0, sh))
-        _abi.check(L.rl_emit_photons(ds.handle, maps, 1, lights, len(flat.lights), st.photon_pass_count,
-                                     st.photon_bounce_count, st.photon_energy_threshold, st.photon_max_distance,
-                                     seed, None, sh))
+        if knn:
+            _abi.check(L.rl_emit_photons_records(ds.handle, maps, 1, lights, len(flat.lights), st.photon_pass_count,
+                                                 st.photon_bounce_count, st.photon_energy_threshold,
+                                                 st.photon_max_distance, seed, records.handle, None, sh))
+        else:
+            _abi.check(L.rl_emit_photons(ds.handle, maps, 1, lights, len(flat.lights), st.photon_pass_count,
+                                         st.photon_bounce_count, st.photon_energy_threshold, st.photon_max_distance,
+                                         seed, None, sh))
         _abi.check(L.rl_photonmap_gather(pmap.handle, st.final_gather_radius, sh))
+        if knn:
+            records.gather_knn(pmap, 0, KNN_K, KNN_RADIUS, sh)
         if fg_events:
             fg_events[0].record(stream)
         _abi.check(L.rl_bake_indirect(ds.handle, lmap.handle, maps, 1, st.final_gather_samples,
@@ -239,7 +256,8 @@ def gpu_arm(args, rank, world, local_rank):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded fBm terrain + boxes)",
-        "config": {"workload": WORKLOAD, "lightmap": [lmap.width, lmap.height], "valid_texels": valid,
+        "config": {"workload": WORKLOAD + (f", kNN k={KNN_K} r={KNN_RADIUS}" if knn else ""),
+                   "gather": args.gather, "lightmap": [lmap.width, lmap.height], "valid_texels": valid,
                    "photons": int(st.photon_pass_count * 125000), "fg_samples": st.final_gather_samples, "triangles": flat.ntris,
                    "parallelism": f"replicas x{world}", "l2": "flushed between steps (256 MiB write)"},
         "grays_per_s": rays_per_step * args.steps * world / (total_ms / 1e3) / 1e9,
@@ -567,6 +585,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--small", action="store_true", help="512^2 / 64 spp / 2 passes case for ncu captures")
+    ap.add_argument("--gather", default="disc", choices=["disc", "knn"],
+                    help="photon estimate: Relight's disc gather (default) or the k-nearest-neighbour estimate")
     ap.add_argument("--workload", default="terrain", choices=["terrain", "batch", "serve", "denoise"],
                     help="terrain: the photon + final-gather bake (default); batch: uneven-size batching; "
                          "serve: the bake-serving loop with the denoiser; denoise: the denoiser at equal RMSE")

@@ -248,6 +248,31 @@ int rl_emit_photons_range(const rl_scene* scene, rl_map* const* photonmaps, int 
    scene/Light.cpp:334-337). */
 int rl_photon_count(const rl_light* lights, int nlights, int pass_count, int64_t* total);
 
+/* k-nearest-neighbour photon estimate (no reference counterpart: the
+   reference has only the texel-space disc gather, Photonmap::gather,
+   Lightmap.cpp:376-413).  rl_emit_photons_records is rl_emit_photons that
+   also keeps every deposit Photons::store makes (baker/Photons.cpp:119-126)
+   as a world-space record in `records` (cleared first; deposits beyond its
+   capacity are counted but not kept).  rl_photonmap_gather_knn then sets,
+   at every valid lumel of the photonmap in `slot`, gathered = the mean
+   colour of the k nearest deposits of that photonmap within `radius` world
+   units of the lumel position (ties by photon number and bounce; 0 when
+   none), over a hashed grid of `radius`-wide cells.  Run it after
+   rl_photonmap_gather: lumels that are not valid keep the disc's value. */
+typedef struct rl_photons rl_photons;
+int rl_photons_create(int64_t capacity, rl_photons** out);
+int rl_photons_destroy(rl_photons* records);
+/* Deposits of the last emission (may exceed the capacity). */
+int rl_photons_count(const rl_photons* records, int64_t* deposits);
+/* The kept records, in no particular order: xyzrgb [n][6], photon [n],
+   depth_slot [n][2] (any may be NULL; n = min(count, capacity)). */
+int rl_photons_download(const rl_photons* records, float* xyzrgb, uint32_t* photon, int32_t* depth_slot);
+int rl_emit_photons_records(const rl_scene* scene, rl_map* const* photonmaps, int nmaps, const rl_light* lights,
+                            int nlights, int pass_count, int max_depth, float threshold, float max_distance,
+                            uint64_t seed, rl_photons* records, int64_t* stored, void* stream);
+/* k in [1, 128]; fails with RL_CAPACITY if the records overflowed. */
+int rl_photonmap_gather_knn(rl_map* photonmap, int slot, rl_photons* records, int k, float radius, void* stream);
+
 /* Photonmap::gather(radius) (Lightmap.cpp:376-413), the loop-bound quirk
    of :379 included. */
 int rl_photonmap_gather(rl_map* photonmap, int radius, void* stream);

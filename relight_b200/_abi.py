@@ -142,6 +142,12 @@ SIGNATURES = {
     "rl_denoiser_forward": (_I, [_P, _P, _I, _I, _I, _P, _P]),
     "rl_denoiser_status": (_I, [_P, _P]),
     "rl_denoiser_reserve": (_I, [_P, _I, _I, _I, _I]),
+    "rl_photons_create": (_I, [_I64, _P]),
+    "rl_photons_destroy": (_I, [_P]),
+    "rl_photons_count": (_I, [_P, _P]),
+    "rl_photons_download": (_I, [_P, _P, _P, _P]),
+    "rl_emit_photons_records": (_I, [_P, _P, _I, _P, _I, _I, _I, _F, _F, _U64, _P, _P, _P]),
+    "rl_photonmap_gather_knn": (_I, [_P, _I, _P, _I, _F, _P]),
     "rl_batch_create": (_I, [_P, _I, _P]),
     "rl_batch_update": (_I, [_P, _P, _I, _P]),
     "rl_map_bytes": (_I, [_I, _I, _P]),

@@ -20,9 +20,9 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "librelight_b200.so")
 
-SOURCES = ["rl_capi.cu", "rl_lbvh.cu", "rl_denoise.cu", "rl_bvh.cpp", os.path.join("host", "relight_api.cpp"),
+SOURCES = ["rl_capi.cu", "rl_lbvh.cu", "rl_denoise.cu", "rl_knn.cu", "rl_bvh.cpp", os.path.join("host", "relight_api.cpp"),
            os.path.join("host", "obj_loader.cpp")]
-HEADERS = ["rl_device.cuh", "rl_bvh.h", "rl_lbvh.h", os.path.join("..", "..", "include", "relight_b200.h"),
+HEADERS = ["rl_device.cuh", "rl_bvh.h", "rl_lbvh.h", "rl_photon_records.h", os.path.join("..", "..", "include", "relight_b200.h"),
            os.path.join("..", "..", "include", "relight", "Relight.h")]
 
 NVCC_FLAGS = [

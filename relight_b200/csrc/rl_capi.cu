@@ -27,6 +27,7 @@
 #include "../../include/relight_b200.h"
 #include "rl_bvh.h"
 #include "rl_device.cuh"
+#include "rl_photon_records.h"
 #include "rl_lbvh.h"
 
 using namespace rl;
@@ -989,7 +990,7 @@ struct PhotonTables {
 // pass / light / photon loops.
 __global__ void k_photons(DevScene s, const __grid_constant__ LightTable LT, const __grid_constant__ PhotonTables T,
                           unsigned first, unsigned total, int max_depth, float threshold, float maxd, uint2 key,
-                          unsigned long long* stored, int* status) {
+                          unsigned long long* stored, PhotonSink sink, int* status) {
     unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= total) return;
     unsigned p = first + t;
@@ -1035,6 +1036,12 @@ __global__ void k_photons(DevScene s, const __grid_constant__ LightTable LT, con
                 atomicAdd(P.color + 3 * ti + 2, hc.z);
                 atomicAdd(P.photons + ti, 1);
                 if (stored) atomicAdd(stored, 1ull);
+                if (sink.rec) {  // the same deposit as a world-space record
+                    unsigned long long q = atomicAdd(sink.count, 1ull);
+                    if (q < sink.capacity)
+                        sink.rec[q] = PhotonRecord{h.point.x, h.point.y, h.point.z, hc.x, hc.y, hc.z, p,
+                                                   (uint16_t)depth, (uint16_t)slot};
+                }
             }
         }
         dir = random_hemisphere(h.normal, key, p, (uint32_t)(depth + 1), kTagBounce);
@@ -1045,7 +1052,7 @@ __global__ void k_photons(DevScene s, const __grid_constant__ LightTable LT, con
 
 static int emit_photons(const rl_scene* s, rl_map* const* maps, int nmaps, const rl_light* lights, int nlights,
                         int pass_count, int max_depth, float threshold, float maxd, uint64_t seed, int64_t first_photon,
-                        int64_t photon_count, int64_t* stored, void* stream) {
+                        int64_t photon_count, int64_t* stored, void* stream, rl_photons* records = nullptr) {
     if (!s || (nmaps > 0 && !maps)) return fail(RL_INVALID_CALL, "rl_emit_photons: null argument");
     if (nmaps > kMaxPhotonmaps) return fail(RL_INVALID_CALL, "rl_emit_photons: at most %d photonmaps", kMaxPhotonmaps);
     cudaStream_t st = S(stream);
@@ -1087,8 +1094,14 @@ static int emit_photons(const rl_scene* s, rl_map* const* maps, int nmaps, const
         CK(cudaMemsetAsync(dc, 0, 8, st));
     }
     uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
+    PhotonSink sink{nullptr, nullptr, 0};
+    if (records) {
+        rc = rl_internal_photon_sink(records, &sink, st);
+        if (rc) return rc;
+    }
     k_photons<<<blocks_for((long long)total, 128), 128, 0, st>>>(s->dev, LT, T, (unsigned)first, (unsigned)total,
-                                                                max_depth, threshold, maxd, key, dc, s->d_status);
+                                                                max_depth, threshold, maxd, key, dc, sink,
+                                                                s->d_status);
     CK_LAUNCH("k_photons");
     if (stored) {
         unsigned long long h = 0;
@@ -1104,6 +1117,14 @@ extern "C" int rl_emit_photons(const rl_scene* s, rl_map* const* maps, int nmaps
                                int64_t* stored, void* stream) {
     return emit_photons(s, maps, nmaps, lights, nlights, pass_count, max_depth, threshold, maxd, seed, 0, -1, stored,
                         stream);
+}
+
+extern "C" int rl_emit_photons_records(const rl_scene* s, rl_map* const* maps, int nmaps, const rl_light* lights,
+                                       int nlights, int pass_count, int max_depth, float threshold, float maxd,
+                                       uint64_t seed, rl_photons* records, int64_t* stored, void* stream) {
+    if (!records) return fail(RL_INVALID_CALL, "rl_emit_photons_records: null record buffer");
+    return emit_photons(s, maps, nmaps, lights, nlights, pass_count, max_depth, threshold, maxd, seed, 0, -1, stored,
+                        stream, records);
 }
 
 extern "C" int rl_emit_photons_range(const rl_scene* s, rl_map* const* maps, int nmaps, const rl_light* lights,

@@ -169,6 +169,46 @@ class DeviceMap:
             pass
 
 
+class PhotonRecords:
+    """rl_photons: world-space photon deposits and their hashed grid, for
+    the k-nearest-neighbour estimate."""
+
+    def __init__(self, capacity: int):
+        self.capacity = capacity
+        self.handle = C.c_void_p()
+        check(lib().rl_photons_create(capacity, C.byref(self.handle)))
+
+    def count(self) -> int:
+        n = C.c_int64()
+        check(lib().rl_photons_count(self.handle, C.byref(n)))
+        return n.value
+
+    def download(self):
+        """(xyzrgb [n][6], photon [n], depth [n], slot [n]) in no particular order."""
+        n = min(self.count(), self.capacity)
+        xyz = np.zeros((n, 6), np.float32)
+        ph = np.zeros(n, np.uint32)
+        ds = np.zeros((n, 2), np.int32)
+        check(lib().rl_photons_download(self.handle, C.c_void_p(xyz.ctypes.data), C.c_void_p(ph.ctypes.data),
+                                        C.c_void_p(ds.ctypes.data)))
+        return xyz, ph, ds[:, 0], ds[:, 1]
+
+    def gather_knn(self, photonmap, slot: int, k: int = 100, radius: float = 1.0, stream=None):
+        """rl_photonmap_gather_knn on a DeviceMap (after its disc gather)."""
+        check(lib().rl_photonmap_gather_knn(photonmap.handle, slot, self.handle, k, float(radius), stream))
+
+    def close(self):
+        if self.handle:
+            check(lib().rl_photons_destroy(self.handle))
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def _map_array(maps):
     arr = (C.c_void_p * max(len(maps), 1))()
     for i, m in enumerate(maps):
@@ -264,18 +304,29 @@ class Relight:
                                settings.max_distance, settings.exponent, seed, it, self.stream))
         return RelightStatus.RelightSuccess
 
-    def emit_photons(self, scene: Scene, settings: IndirectLightSettings, seed: Optional[int] = None) -> RelightStatus:
-        """Relight::emitPhotons (Relight.cpp:244-257): trace, then gather every photonmap."""
+    def emit_photons(self, scene: Scene, settings: IndirectLightSettings, seed: Optional[int] = None,
+                     knn: Optional[tuple] = None, records: Optional["PhotonRecords"] = None) -> RelightStatus:
+        """Relight::emitPhotons (Relight.cpp:244-257): trace, then gather every
+        photonmap.  knn = (k, radius): also keep the deposits in `records` and
+        replace the estimate at valid lumels by the k nearest deposits'
+        mean colour (rl_photonmap_gather_knn)."""
         ds = self.device_scene(scene)
         f = scene.flat
         maps = [m._device for m in f.photonmaps]
         seed = self.next_seed() if seed is None else seed
-        check(lib().rl_emit_photons(ds.handle, _map_array(maps), len(maps), C.c_void_p(f.lights.ctypes.data),
-                                    len(f.lights), settings.photon_pass_count, settings.photon_bounce_count,
-                                    settings.photon_energy_threshold, settings.photon_max_distance, seed, None,
-                                    self.stream))
-        for m in maps:
+        args = (ds.handle, _map_array(maps), len(maps), C.c_void_p(f.lights.ctypes.data), len(f.lights),
+                settings.photon_pass_count, settings.photon_bounce_count, settings.photon_energy_threshold,
+                settings.photon_max_distance, seed)
+        if knn is not None:
+            if records is None:
+                raise ValueError("knn needs a PhotonRecords buffer")
+            check(lib().rl_emit_photons_records(*args, records.handle, None, self.stream))
+        else:
+            check(lib().rl_emit_photons(*args, None, self.stream))
+        for slot, m in enumerate(maps):
             check(lib().rl_photonmap_gather(m.handle, settings.final_gather_radius, self.stream))
+            if knn is not None:
+                records.gather_knn(m, slot, knn[0], knn[1], self.stream)
         return RelightStatus.RelightSuccess
 
     def bake_indirect_light(self, scene: Scene, mesh: Mesh, progress, settings: IndirectLightSettings,

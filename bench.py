@@ -121,7 +121,7 @@ def build_workload(seed):
 
 def gpu_arm(args, rank, world, local_rank):
     import torch
-    from relight_b200 import _abi
+    from relight_b200 import _abi, autotune
     from relight_b200.device import Relight, _map_array
 
     torch.cuda.set_device(local_rank)
@@ -257,7 +257,7 @@ def gpu_arm(args, rank, world, local_rank):
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded fBm terrain + boxes)",
         "config": {"workload": WORKLOAD + (f", kNN k={KNN_K} r={KNN_RADIUS}" if knn else ""),
-                   "gather": args.gather, "lightmap": [lmap.width, lmap.height], "valid_texels": valid,
+                   "gather": args.gather, "bvh_width": autotune.get_width(), "lightmap": [lmap.width, lmap.height], "valid_texels": valid,
                    "photons": int(st.photon_pass_count * 125000), "fg_samples": st.final_gather_samples, "triangles": flat.ntris,
                    "parallelism": f"replicas x{world}", "l2": "flushed between steps (256 MiB write)"},
         "grays_per_s": rays_per_step * args.steps * world / (total_ms / 1e3) / 1e9,
@@ -585,6 +585,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--small", action="store_true", help="512^2 / 64 spp / 2 passes case for ncu captures")
+    ap.add_argument("--bvh-width", type=int, default=0, choices=[0, 2, 4, 8],
+                    help="traversal tree for AO / final gather (0: the library's default)")
     ap.add_argument("--gather", default="disc", choices=["disc", "knn"],
                     help="photon estimate: Relight's disc gather (default) or the k-nearest-neighbour estimate")
     ap.add_argument("--workload", default="terrain", choices=["terrain", "batch", "serve", "denoise"],
@@ -593,6 +595,9 @@ def main():
     args = ap.parse_args()
     global SMALL
     SMALL = args.small
+    if args.bvh_width:
+        from relight_b200 import autotune
+        autotune.set_width(args.bvh_width)
     if args.workload == "batch":
         print(json.dumps(batch_arm(args)), flush=True)
         return

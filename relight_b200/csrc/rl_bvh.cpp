@@ -177,6 +177,174 @@ void put_child_box(float* dst, int slot, const Box& b) {
     dst[8 + 2 * slot + 1] = b.hi[2];
 }
 
+// ---------------------------------------------------- compressed 8-wide
+//
+// Node (20 words): p.xyz (float), exponent bytes ex | ey << 8 | ez << 16 |
+// internal-child mask << 24, child base, triangle base, meta[8] (2 words),
+// then the quantised child bounds qlo.x[8] qlo.y[8] qlo.z[8] qhi.x[8]
+// qhi.y[8] qhi.z[8] (one byte each).  Child c's box is
+// p + q * 2^(e - 127) per axis; internal children are stored contiguously
+// from the child base in slot order (rank = internal slots below c); a leaf
+// slot's meta is count << 5 | offset, its triangles at triangle base +
+// offset (count <= 4, offset <= 28); meta 0 on a non-internal slot = empty.
+// Children go to slots by octant (the child lying most towards corner s of
+// the node gets slot s), so a ray that visits slots in the order slot ^
+// (its direction sign bits) meets them roughly front to back.
+
+struct Collapse8 {
+    const std::vector<Node>& bn;
+    const std::vector<float>& tris;   // records in leaf (prims) order
+    std::vector<uint32_t>& n8;
+    std::vector<float>& t8;
+
+    struct Slot {
+        int node = -1;       // binary node id (inner child), or the leaf node
+        int first = 0, count = 0;  // leaf chunk in prims order
+        Box box;
+        bool inner = false;
+    };
+
+    // Smallest exponent e (scale 2^e) with every child's float decode
+    // p + q * 2^e (one rounding) conservative for q in [0, 255].
+    static void quantize(float p, const float* lo, const float* hi, int n, float ext, int& e, uint8_t* qlo,
+                         uint8_t* qhi) {
+        int ee = ext > 0.0f ? (int)std::ceil(std::log2((double)ext / 255.0)) : -126;
+        ee = std::max(-126, std::min(127, ee));
+        for (;; ee++) {
+            float sc = std::ldexp(1.0f, ee);
+            bool ok = true;
+            for (int c = 0; c < n && ok; c++) {
+                float ql = std::floor((lo[c] - p) / sc);
+                ql = std::max(0.0f, std::min(255.0f, ql));
+                while (ql > 0.0f && p + ql * sc > lo[c]) ql -= 1.0f;
+                float qh = std::ceil((hi[c] - p) / sc);
+                qh = std::max(0.0f, qh);
+                while (qh <= 255.0f && p + qh * sc < hi[c]) qh += 1.0f;
+                if (qh > 255.0f || p + ql * sc > lo[c]) {
+                    ok = false;
+                    break;
+                }
+                qlo[c] = (uint8_t)ql;
+                qhi[c] = (uint8_t)qh;
+            }
+            if (ok || ee >= 127) {
+                e = ee;
+                return;
+            }
+        }
+    }
+
+    // Write binary inner node `id` as the 8-wide node at index `at`.
+    void emit(int id, uint32_t at) {
+        std::vector<int> items = {bn[id].child[0], bn[id].child[1]};
+        auto slots_of = [&](int k) { return bn[k].count > 0 ? (bn[k].count + 3) / 4 : 1; };
+        for (;;) {
+            int used = 0, pick = -1;
+            float best = -1.0f;
+            for (int k : items) used += slots_of(k);
+            for (size_t q = 0; q < items.size(); q++) {
+                const Node& c = bn[items[q]];
+                if (c.count == 0 && c.box.area() > best) {
+                    int grow = slots_of(c.child[0]) + slots_of(c.child[1]) - 1;
+                    if (used + grow <= 8) { best = c.box.area(); pick = (int)q; }
+                }
+            }
+            if (pick < 0) break;
+            int opened = items[pick];
+            items[pick] = bn[opened].child[0];
+            items.push_back(bn[opened].child[1]);
+        }
+        std::vector<Slot> sl;
+        for (int k : items) {
+            const Node& c = bn[k];
+            if (c.count == 0) {
+                Slot s;
+                s.node = k; s.inner = true; s.box = c.box;
+                sl.push_back(s);
+            } else {
+                for (int f = 0; f < c.count; f += 4) {
+                    Slot s;
+                    s.node = k; s.first = c.first + f; s.count = std::min(4, c.count - f); s.box = c.box;
+                    sl.push_back(s);
+                }
+            }
+        }
+        // octant slot assignment, greedy on the best remaining (child, slot) score
+        Box nb;
+        for (const Slot& s : sl) nb.grow(s.box);
+        float cen[3];
+        for (int a = 0; a < 3; a++) cen[a] = 0.5f * (nb.lo[a] + nb.hi[a]);
+        int slot_of[8] = {-1, -1, -1, -1, -1, -1, -1, -1};  // slot -> index in sl
+        std::vector<bool> placed(sl.size(), false);
+        for (size_t round = 0; round < sl.size(); round++) {
+            float bs = -FLT_MAX;
+            int bi = -1, bslot = -1;
+            for (size_t i = 0; i < sl.size(); i++) {
+                if (placed[i]) continue;
+                for (int q = 0; q < 8; q++) {
+                    if (slot_of[q] >= 0) continue;
+                    float sc = 0.0f;
+                    for (int a = 0; a < 3; a++) {
+                        float d = 0.5f * (sl[i].box.lo[a] + sl[i].box.hi[a]) - cen[a];
+                        sc += ((q >> a) & 1) ? d : -d;
+                    }
+                    if (sc > bs) { bs = sc; bi = (int)i; bslot = q; }
+                }
+            }
+            placed[bi] = true;
+            slot_of[bslot] = bi;
+        }
+        // children block and triangle run
+        uint32_t imask = 0;
+        int ninner = 0;
+        for (int q = 0; q < 8; q++)
+            if (slot_of[q] >= 0 && sl[slot_of[q]].inner) { imask |= 1u << q; ninner++; }
+        uint32_t child_base = (uint32_t)(n8.size() / 20);
+        n8.resize(n8.size() + 20 * (size_t)ninner, 0u);
+        uint32_t tri_base = (uint32_t)(t8.size() / 12);
+        uint8_t meta[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        int off = 0;
+        for (int q = 0; q < 8; q++) {
+            if (slot_of[q] < 0 || sl[slot_of[q]].inner) continue;
+            const Slot& s = sl[slot_of[q]];
+            for (int i = 0; i < s.count; i++)
+                t8.insert(t8.end(), tris.begin() + 12 * (size_t)(s.first + i), tris.begin() + 12 * (size_t)(s.first + i + 1));
+            meta[q] = (uint8_t)((s.count << 5) | off);
+            off += s.count;
+        }
+        // quantised boxes
+        uint8_t qlo[3][8], qhi[3][8];
+        int ex[3];
+        for (int a = 0; a < 3; a++) {
+            float lo[8], hi[8];
+            int n = 0, map[8];
+            for (int q = 0; q < 8; q++) {
+                qlo[a][q] = 255;
+                qhi[a][q] = 0;
+                if (slot_of[q] < 0) continue;
+                lo[n] = sl[slot_of[q]].box.lo[a];
+                hi[n] = sl[slot_of[q]].box.hi[a];
+                map[n++] = q;
+            }
+            uint8_t l8[8], h8[8];
+            quantize(nb.lo[a], lo, hi, n, nb.hi[a] - nb.lo[a], ex[a], l8, h8);
+            for (int c = 0; c < n; c++) { qlo[a][map[c]] = l8[c]; qhi[a][map[c]] = h8[c]; }
+        }
+        uint32_t* w = &n8[20 * (size_t)at];
+        for (int a = 0; a < 3; a++) std::memcpy(&w[a], &nb.lo[a], 4);
+        w[3] = (uint32_t)(ex[0] + 127) | ((uint32_t)(ex[1] + 127) << 8) | ((uint32_t)(ex[2] + 127) << 16) | (imask << 24);
+        w[4] = child_base;
+        w[5] = tri_base;
+        std::memcpy(&w[6], meta, 8);
+        uint8_t* qb = reinterpret_cast<uint8_t*>(&w[8]);
+        for (int a = 0; a < 3; a++) std::memcpy(qb + 8 * a, qlo[a], 8);
+        for (int a = 0; a < 3; a++) std::memcpy(qb + 24 + 8 * a, qhi[a], 8);
+        int r = 0;
+        for (int q = 0; q < 8; q++)
+            if (imask >> q & 1u) emit(sl[slot_of[q]].node, child_base + r++);
+    }
+};
+
 }  // namespace
 
 bool build_bvh_sah(const float* pos, int nverts, const int32_t* tris, int ntris, BvhBuild& out, const char** err) {
@@ -348,6 +516,14 @@ bool build_bvh_sah(const float* pos, int nverts, const int32_t* tris, int ntris,
         col.emit(0);
     }
     out.nodes4_count = (int64_t)(out.nodes4.size() / 32);
+
+    // Compressed 8-wide tree (a single-leaf tree gets none: the binary walk serves it).
+    if (B.nodes[0].count == 0) {
+        Collapse8 c8{B.nodes, out.tris, out.nodes8, out.tris8};
+        out.nodes8.assign(20, 0u);
+        c8.emit(0, 0);
+        out.nodes8_count = (int64_t)(out.nodes8.size() / 20);
+    }
     return true;
 }
 

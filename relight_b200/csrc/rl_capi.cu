@@ -165,7 +165,7 @@ extern "C" int rl_tune_set(int param, int value) {
     bool width = param == RL_TUNE_BVH_WIDTH;
     bool spec = param == RL_TUNE_SPECULATIVE;
     if ((refill && value >= 1 && value <= 32) || (block && (value == 64 || value == 128 || value == 256)) ||
-        (width && (value == 2 || value == 4)) || (spec && (value == 0 || value == 1)))
+        (width && (value == 2 || value == 4 || value == 8)) || (spec && (value == 0 || value == 1)))
         g_tune[param] = value;
     else
         return fail(RL_INVALID_CALL, "rl_tune_set: bad parameter %d or value %d", param, value);
@@ -246,10 +246,16 @@ extern "C" int rl_scene_create(const rl_scene_desc* d, int builder, void* stream
     long long* tex_off = nullptr;
     unsigned char* tex_px = nullptr;
     float4* nodes4 = nullptr;
+    uint4* nodes8 = nullptr;
+    float4* tris8 = nullptr;
     if (builder == 0) {
         up(&nodes, (const float4*)b.nodes.data(), b.nodes.size() / 4);
         up(&nodes4, (const float4*)b.nodes4.data(), b.nodes4.size() / 4);
         up(&tris, (const float4*)b.tris.data(), b.tris.size() / 4);
+        if (!b.nodes8.empty()) {
+            up(&nodes8, (const uint4*)b.nodes8.data(), b.nodes8.size() / 4);
+            up(&tris8, (const float4*)b.tris8.data(), b.tris8.size() / 4);
+        }
     }
     up(&dvidx, vidx.data(), vidx.size());
     up(&pos, d->pos, 3 * (size_t)d->nverts);
@@ -301,6 +307,7 @@ extern "C" int rl_scene_create(const rl_scene_desc* d, int builder, void* stream
     }
     DevScene& v = s->dev;
     v.nodes = nodes; v.nodes4 = nodes4; v.tris = tris; v.tri_vidx = dvidx;
+    v.nodes8 = nodes8; v.tris8 = tris8;
     v.pos = pos; v.nrm = nrm; v.uv0 = uv0; v.uv1 = uv1; v.vmat = dvmat;
     v.mesh_first_tri = first; v.mesh_photonmap = dpmap;
     v.mat_rgb = mat_rgb; v.mat_tex = dmat_tex; v.tex_dims = tex_dims; v.tex_offset = tex_off; v.tex_pixels = tex_px;
@@ -945,7 +952,8 @@ __global__ void __launch_bounds__(256) k_ao(DevScene s, DevMap m, int samples, f
     g.samples = valid ? samples : 0;
     g.occluded = 0;
     g.maxd = maxd;
-    if (kWidth == 4) ray_loop4<true>(s, g, refill, status);
+    if (kWidth == 8) ray_loop8<true>(s, g, refill, status);
+    else if (kWidth == 4) ray_loop4<true>(s, g, refill, status);
     else if (kWidth == 3) ray_loop_spec<true>(s, g, refill, status);
     else ray_loop<true>(s, g, refill, status);
     if (!valid) return;
@@ -967,7 +975,8 @@ extern "C" int rl_bake_ao(const rl_scene* s, rl_map* lm, int samples, float frac
     uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
     int bs = g_tune[RL_TUNE_AO_BLOCK];
     bool wide = g_tune[RL_TUNE_BVH_WIDTH] == 4 && s->dev.nodes4 != nullptr;
-    auto kern = wide ? k_ao<4> : (g_tune[RL_TUNE_SPECULATIVE] ? k_ao<3> : k_ao<2>);
+    bool wide8 = g_tune[RL_TUNE_BVH_WIDTH] == 8 && s->dev.nodes8 != nullptr;
+    auto kern = wide8 ? k_ao<8> : wide ? k_ao<4> : (g_tune[RL_TUNE_SPECULATIVE] ? k_ao<3> : k_ao<2>);
     kern<<<blocks_for(count, bs), bs, 0, S(stream)>>>(s->dev, lm->dev, samples, fraction, maxd, exponent, key, it,
                                                       count, g_tune[RL_TUNE_AO_REFILL], s->d_status);
     CK_LAUNCH("k_ao");
@@ -1237,8 +1246,11 @@ struct FgGen {
     }
 };
 
+// At most 64 registers (four 256-thread blocks' worth per SM): the ray loop
+// is latency-bound and gains more from resident warps than it loses to the
+// few spills (measured 52.3 -> 50.9 ms on the terrain final gather).
 template <int kWidth>
-__global__ void __launch_bounds__(256) k_indirect(DevScene s, DevMap m, const __grid_constant__ GatherMaps G,
+__global__ void __launch_bounds__(256, 4) k_indirect(DevScene s, DevMap m, const __grid_constant__ GatherMaps G,
                                                   int samples, float maxd, V3 sky, V3 amb, uint2 key, Iter it,
                                                   long long count, int refill, int* status) {
     long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -1260,7 +1272,8 @@ __global__ void __launch_bounds__(256) k_indirect(DevScene s, DevMap m, const __
     g.gr = g.gg = g.gb = 0.f;
     g.influence = 0.f;
     g.dir = mk3(0.f, 0.f, 0.f);
-    if (kWidth == 4) ray_loop4<false>(s, g, refill, status);
+    if (kWidth == 8) ray_loop8<false>(s, g, refill, status);
+    else if (kWidth == 4) ray_loop4<false>(s, g, refill, status);
     else if (kWidth == 3) ray_loop_spec<false>(s, g, refill, status);
     else ray_loop<false>(s, g, refill, status);
     if (!valid) return;
@@ -1292,7 +1305,8 @@ extern "C" int rl_bake_indirect(const rl_scene* s, rl_map* lm, rl_map* const* ma
     uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
     int bs = g_tune[RL_TUNE_FG_BLOCK];
     bool wide = g_tune[RL_TUNE_BVH_WIDTH] == 4 && s->dev.nodes4 != nullptr;
-    auto kern = wide ? k_indirect<4> : (g_tune[RL_TUNE_SPECULATIVE] ? k_indirect<3> : k_indirect<2>);
+    bool wide8 = g_tune[RL_TUNE_BVH_WIDTH] == 8 && s->dev.nodes8 != nullptr;
+    auto kern = wide8 ? k_indirect<8> : wide ? k_indirect<4> : (g_tune[RL_TUNE_SPECULATIVE] ? k_indirect<3> : k_indirect<2>);
     kern<<<blocks_for(count, bs), bs, 0, st>>>(s->dev, lm->dev, G, samples, maxd, skyv, ambv, key, it, count,
                                               g_tune[RL_TUNE_FG_REFILL], s->d_status);
     CK_LAUNCH("k_indirect");
@@ -1928,7 +1942,7 @@ __device__ __forceinline__ int find_job(const long long* prefix, int njobs, long
 // and Philox keys as the single-job calls, so the lumels come out
 // bit-identical to rl_bake_direct / rl_bake_ao / rl_bake_indirect.
 template <int kKind>
-__global__ void __launch_bounds__(kKind == 0 ? 128 : 256, kKind == 0 ? 1 : 3) k_batch(const BatchHeader* __restrict__ hdrs,
+__global__ void __launch_bounds__(kKind == 0 ? 128 : 256, kKind == 0 ? 1 : 4) k_batch(const BatchHeader* __restrict__ hdrs,
                                                                   unsigned long long* counter, int refill) {
     if (hdrs[kKind].total <= 0) return;
     const int lane = threadIdx.x & 31;

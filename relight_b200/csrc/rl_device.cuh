@@ -29,6 +29,8 @@ struct DevScene {
     const float4* nodes4;       // 4-wide nodes, 128 B: lo.x hi.x lo.y hi.y lo.z hi.z (4 children each), codes, pad
     const float4* tris;
     const int4* tri_vidx;       // per global triangle id: a, b, c, mesh
+    const uint4* nodes8;        // compressed 8-wide nodes, 80 B (rl_bvh.cpp), or null
+    const float4* tris8;        // triangle records in 8-wide node order
     const float* pos;
     const float* nrm;
     const float* uv0;
@@ -689,6 +691,158 @@ __device__ __forceinline__ bool segment_blocked(const DevScene& s, V3 start, V3 
     SegHit r;
     trace_segment(s, start, end, flags, r, overflow);
     return r.hit;
+}
+
+
+// ----------------------------------------------------- compressed 8-wide walk
+
+constexpr int kStack8 = 32;
+
+__device__ __forceinline__ float qbyte(uint32_t lo4, uint32_t hi4, int c) {
+    return (float)(((c < 4 ? lo4 : hi4) >> ((c & 3) * 8)) & 0xffu);
+}
+
+// One compressed 8-wide node (rl_bvh.cpp): decode the eight child boxes
+// (p + q * 2^e, exact product, one rounding: the builder's decode) and run
+// slab2's conservative test on each.  Returns the internal children hit as
+// key bits (bit slot ^ oct) and the triangle slots of the leaf children hit.
+__device__ __forceinline__ void visit8(const DevScene& s, int node, V3 idir, V3 ood, float tnear, float tmax,
+                                       uint32_t oct, uint32_t& child_base, uint32_t& keys, uint32_t& imask,
+                                       uint32_t& tri_base, uint32_t& tmask) {
+    const uint4* np = s.nodes8 + 5 * (size_t)node;
+    const uint4 q0 = __ldg(np), q1 = __ldg(np + 1), q2 = __ldg(np + 2), q3 = __ldg(np + 3), q4 = __ldg(np + 4);
+    const float px = __uint_as_float(q0.x), py = __uint_as_float(q0.y), pz = __uint_as_float(q0.z);
+    const float sx = __uint_as_float((q0.w & 0xffu) << 23), sy = __uint_as_float(((q0.w >> 8) & 0xffu) << 23),
+                sz = __uint_as_float(((q0.w >> 16) & 0xffu) << 23);
+    imask = q0.w >> 24;
+    child_base = q1.x;
+    tri_base = q1.y;
+    uint32_t k = 0, t = 0;
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+        const uint32_t meta = ((c < 4 ? q1.z : q1.w) >> ((c & 3) * 8)) & 0xffu;
+        const bool inner = (imask >> c) & 1u;
+        if (!inner && meta == 0u) continue;
+        const float lx = __fmaf_rn(qbyte(q2.x, q2.y, c), sx, px), hx = __fmaf_rn(qbyte(q3.z, q3.w, c), sx, px);
+        const float ly = __fmaf_rn(qbyte(q2.z, q2.w, c), sy, py), hy = __fmaf_rn(qbyte(q4.x, q4.y, c), sy, py);
+        const float lz = __fmaf_rn(qbyte(q3.x, q3.y, c), sz, pz), hz = __fmaf_rn(qbyte(q4.z, q4.w, c), sz, pz);
+        const float a0 = __fmaf_rn(lx, idir.x, -ood.x), a1 = __fmaf_rn(hx, idir.x, -ood.x);
+        const float b0 = __fmaf_rn(ly, idir.y, -ood.y), b1 = __fmaf_rn(hy, idir.y, -ood.y);
+        const float c0 = __fmaf_rn(lz, idir.z, -ood.z), c1 = __fmaf_rn(hz, idir.z, -ood.z);
+        const float lo = fmaxf(fmaxf(fminf(a0, a1), fminf(b0, b1)), fmaxf(fminf(c0, c1), tnear));
+        const float hi = fminf(fminf(fmaxf(a0, a1), fmaxf(b0, b1)), fminf(fmaxf(c0, c1), tmax));
+        if (!(lo <= hi * 1.0000003f)) continue;
+        if (inner) k |= 1u << (c ^ oct);
+        else t |= ((1u << (meta >> 5)) - 1u) << (meta & 31u);
+    }
+    keys = k;
+    tmask = t;
+}
+
+// ray_loop over the compressed 8-wide tree: node groups (a node's internal
+// children hit, as key bits, with its child base) on the stack instead of
+// single nodes, and the triangles of the leaf children hit tested one per
+// step (Ylitie, Karras & Laine, "Efficient incoherent ray traversal on GPUs
+// through compressed wide BVHs", HPG 2017).  Same warp refill and same
+// closest-hit / tie-break rule as ray_loop, so the hits are identical.
+template <bool kAny, typename Gen>
+__device__ __forceinline__ void ray_loop8(const DevScene& s, Gen& g, int refill, int* overflow) {
+    V3 o = mk3(0.f, 0.f, 0.f), d = o, idir = o, ood = o;
+    float tnear = 0.f, tfar = 0.f, best = 0.f;
+    int best_gid = 0x7fffffff;
+    RayHit hit;
+    hit.gid = -1; hit.t = hit.u = hit.v = 0.f;
+    uint2 stack[kStack8];
+    int sp = 0;
+    uint32_t gbase = 0, gkeys = 0, gimask = 0;  // current node group
+    uint32_t tbase = 0, tmask = 0;              // current triangle group
+    uint32_t oct = 0;
+    bool root = false, walking = false, have = false, exhausted = false;
+    const unsigned mask = __activemask();
+    for (;;) {
+        bool need = !walking && !exhausted;
+        unsigned alive = __ballot_sync(mask, !exhausted);
+        if (alive == 0) break;
+        unsigned needm = __ballot_sync(mask, need);
+        if (need && (__popc(needm) >= refill || needm == alive)) {
+            if (have) {
+                g.finish(hit);
+                have = false;
+            }
+            if (g.next(o, d, tnear, tfar)) {
+                have = true;
+                idir = mk3(safe_inv(d.x), safe_inv(d.y), safe_inv(d.z));
+                ood = mk3(o.x * idir.x, o.y * idir.y, o.z * idir.z);
+                oct = (d.x < 0.f ? 1u : 0u) | (d.y < 0.f ? 2u : 0u) | (d.z < 0.f ? 4u : 0u);
+                best = tfar;
+                best_gid = 0x7fffffff;
+                hit.gid = -1;
+                sp = 0;
+                gkeys = 0;
+                tmask = 0;
+                root = s.ntris > 0;
+                walking = root;
+            } else {
+                exhausted = true;
+            }
+        }
+        if (!walking) continue;
+        // nodes until there are triangles to test (or the walk ends)
+        while (tmask == 0u) {
+            int node;
+            if (root) {
+                node = 0;
+                root = false;
+            } else if (gkeys) {
+                const uint32_t key = __ffs(gkeys) - 1;
+                gkeys &= gkeys - 1u;
+                const uint32_t slot = key ^ oct;
+                node = (int)(gbase + __popc(gimask & ((1u << slot) - 1u)));
+            } else if (sp > 0) {
+                const uint2 e = stack[--sp];
+                gbase = e.x;
+                gkeys = e.y & 0xffu;
+                gimask = e.y >> 8;
+                continue;
+            } else {
+                walking = false;
+                break;
+            }
+            uint32_t cb, keys, im, tb, tm;
+            visit8(s, node, idir, ood, tnear, best, oct, cb, keys, im, tb, tm);
+            if (keys) {
+                if (gkeys) {
+                    if (sp < kStack8) stack[sp++] = make_uint2(gbase, gkeys | (gimask << 8));
+                    else if (overflow) *overflow = 1;
+                }
+                gbase = cb;
+                gkeys = keys;
+                gimask = im;
+            }
+            if (tm) {
+                tbase = tb;
+                tmask = tm;
+            }
+        }
+        if (!walking) continue;
+        // one triangle
+        const int i = (int)(tbase + __ffs(tmask) - 1);
+        tmask &= tmask - 1u;
+        const float4* tp = s.tris8 + 3 * (size_t)i;
+        float4 t0 = __ldg(tp), t1 = __ldg(tp + 1), t2 = __ldg(tp + 2);
+        float t, u, v;
+        if (tri_test(t0, t1, t2, o, d, tnear, tfar, t, u, v)) {
+            int gid = __float_as_int(t0.w);
+            if (t < best || (t == best && gid < best_gid)) {
+                best = t; best_gid = gid;
+                hit.t = t; hit.u = u; hit.v = v; hit.gid = gid;
+                if (kAny) {
+                    walking = false;
+                    tmask = 0;
+                }
+            }
+        }
+    }
 }
 
 }  // namespace rl

@@ -292,13 +292,15 @@ def test_radiosity_jacobi_vs_fp64(cuda):
 
 
 def test_launch_tuning_changes_no_result(cuda):
-    """The autotuner's knobs (refill threshold, block size) reschedule rays
-    only: every setting bakes the same bits."""
+    """The autotuner's knobs (refill threshold, block size, BVH width 2 / 4 /
+    compressed 8, speculative walk) reschedule rays only: every setting
+    bakes the same bits."""
     from relight_b200 import autotune
     saved = autotune.get("ao"), autotune.get("indirect"), autotune.get_width(), autotune.get_speculative()
     colors, fg = [], []
     try:
-        for refill, block, width, spec in ((1, 64, 2, 0), (13, 128, 4, 0), (32, 256, 2, 1), (24, 64, 2, 1)):
+        for refill, block, width, spec in ((1, 64, 2, 0), (13, 128, 4, 0), (32, 256, 2, 1), (24, 64, 2, 1),
+                                           (16, 64, 8, 0), (32, 128, 8, 0)):
             autotune.set_width(width)
             autotune.set_speculative(spec)
             autotune.set(refill, block, "ao")

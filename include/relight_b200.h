@@ -481,7 +481,9 @@ int rl_radiosity_solve_noalloc(int n, const int64_t* d_row_ptr, const int32_t* d
      *_REFILL: a warp restarts finished lanes' rays once this many of its
                live lanes (1..32) have finished;
      *_BLOCK:  threads per block (64, 128 or 256);
-     RL_TUNE_BVH_WIDTH: 2 (binary nodes) or 4 (4-wide nodes);
+     RL_TUNE_BVH_WIDTH: 2 (binary nodes), 4 (4-wide nodes) or 8 (compressed
+                        8-wide nodes, built for scenes created while it is
+                        selected);
      RL_TUNE_SPECULATIVE: 1 = binary traversal parks leaves until the whole
                           warp has one (speculative traversal), 0 = off. */
 enum {

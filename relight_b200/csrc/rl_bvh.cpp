@@ -347,7 +347,8 @@ struct Collapse8 {
 
 }  // namespace
 
-bool build_bvh_sah(const float* pos, int nverts, const int32_t* tris, int ntris, BvhBuild& out, const char** err) {
+bool build_bvh_sah(const float* pos, int nverts, const int32_t* tris, int ntris, BvhBuild& out, const char** err,
+                   bool wide8) {
     out = BvhBuild();
     if (ntris <= 0) return true;
     if ((int64_t)ntris >= (1ll << 28)) {
@@ -518,7 +519,7 @@ bool build_bvh_sah(const float* pos, int nverts, const int32_t* tris, int ntris,
     out.nodes4_count = (int64_t)(out.nodes4.size() / 32);
 
     // Compressed 8-wide tree (a single-leaf tree gets none: the binary walk serves it).
-    if (B.nodes[0].count == 0) {
+    if (wide8 && B.nodes[0].count == 0) {
         Collapse8 c8{B.nodes, out.tris, out.nodes8, out.tris8};
         out.nodes8.assign(20, 0u);
         c8.emit(0, 0);

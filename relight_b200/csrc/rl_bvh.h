@@ -21,6 +21,8 @@ struct BvhBuild {
 
 // Binned-SAH build over `ntris` triangles given as three vertex ids into
 // `pos` ([nverts][3]); triangle ids are the global ids (position in `tris`).
-bool build_bvh_sah(const float* pos, int nverts, const int32_t* tris, int ntris, BvhBuild& out, const char** err);
+// wide8: also emit the compressed 8-wide tree (nodes8 / tris8).
+bool build_bvh_sah(const float* pos, int nverts, const int32_t* tris, int ntris, BvhBuild& out, const char** err,
+                   bool wide8 = false);
 
 }  // namespace rl

@@ -199,7 +199,8 @@ extern "C" int rl_scene_create(const rl_scene_desc* d, int builder, void* stream
             delete s;
             return fail(RL_INVALID_CALL, "triangle vertex index out of range");
         }
-    if (builder == 0 && !build_bvh_sah(d->pos, d->nverts, d->tris, d->ntris, b, &err)) {
+    // the compressed 8-wide tree is built only while width 8 is selected
+    if (builder == 0 && !build_bvh_sah(d->pos, d->nverts, d->tris, d->ntris, b, &err, g_tune[RL_TUNE_BVH_WIDTH] == 8)) {
         delete s;
         return fail(RL_INVALID_CALL, "BVH build: %s", err);
     }

@@ -741,10 +741,13 @@ __device__ __forceinline__ void visit8(const DevScene& s, int node, V3 idir, V3 
 
 // ray_loop over the compressed 8-wide tree: node groups (a node's internal
 // children hit, as key bits, with its child base) on the stack instead of
-// single nodes, and the triangles of the leaf children hit tested one per
-// step (Ylitie, Karras & Laine, "Efficient incoherent ray traversal on GPUs
-// through compressed wide BVHs", HPG 2017).  Same warp refill and same
-// closest-hit / tie-break rule as ray_loop, so the hits are identical.
+// single nodes, and the triangles of the leaf children hit tested in the
+// following step (Ylitie, Karras & Laine, "Efficient incoherent ray traversal
+// on GPUs through compressed wide BVHs", HPG 2017).  Same warp refill and
+// same closest-hit / tie-break rule as ray_loop, so the hits are identical.
+// On the terrain final gather it measured 2.3x slower than the binary walk
+// (116 vs 51 ms): each visit decodes and tests eight boxes and the octant
+// order culls less than ray_loop's distance order, so it is opt-in.
 template <bool kAny, typename Gen>
 __device__ __forceinline__ void ray_loop8(const DevScene& s, Gen& g, int refill, int* overflow) {
     V3 o = mk3(0.f, 0.f, 0.f), d = o, idir = o, ood = o;
@@ -825,7 +828,8 @@ __device__ __forceinline__ void ray_loop8(const DevScene& s, Gen& g, int refill,
             }
         }
         if (!walking) continue;
-        // one triangle
+        // every triangle of the group
+        while (tmask) {
         const int i = (int)(tbase + __ffs(tmask) - 1);
         tmask &= tmask - 1u;
         const float4* tp = s.tris8 + 3 * (size_t)i;
@@ -841,6 +845,7 @@ __device__ __forceinline__ void ray_loop8(const DevScene& s, Gen& g, int refill,
                     tmask = 0;
                 }
             }
+        }
         }
     }
 }

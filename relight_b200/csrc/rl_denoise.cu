@@ -78,6 +78,10 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
                  : "memory");
 }
 
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     uint32_t ok;
     asm volatile(
@@ -202,86 +206,15 @@ struct ConvArgs {
 };
 
 // Implicit-GEMM 3x3 convolution (forward, or data gradient with flipped
-// transposed weights).  Warp 0 lane 0 issues TMA, warp 1 lane 0 issues the
-// MMAs, all four warps run the epilogue (warp w reads TMEM lanes 32w..32w+31,
-// i.e. output pixels 32w..32w+31 of the tile).
-__global__ void __launch_bounds__(128, 2) k_conv3x3(const __grid_constant__ CUtensorMap tmA0,
-                                                   const __grid_constant__ CUtensorMap tmA1,
-                                                   const __grid_constant__ CUtensorMap tmB, const ConvArgs a) {
-    extern __shared__ uint8_t smem_raw[];
-    uint8_t* smem = align1024(smem_raw);
-    const int S = a.stages;
-    const uint32_t b_bytes = (uint32_t)a.ncols * 128;
-    uint8_t* sa = smem;
-    uint8_t* sb = smem + S * kABytes;
-    uint64_t* full = (uint64_t*)(sb + S * b_bytes);
-    uint64_t* empty = full + S;
-    uint64_t* done = empty + S;
-    uint32_t* tmem_slot = (uint32_t*)(done + 1);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int x0 = blockIdx.x * kTileW, y0 = blockIdx.y * kTileH, img = blockIdx.z;
+// transposed weights): see k_conv3x3_p below.
 
-    if (threadIdx.x == 0) {
-        for (int s = 0; s < S; s++) {
-            mbar_init(full + s, 1);
-            mbar_init(empty + s, 1);
-        }
-        mbar_init(done, 1);
-        fence_barrier_init();
-    }
-    if (warp == 0) {
-        tmem_alloc(tmem_slot, a.tmem_cols);
-        tmem_relinquish();
-    }
-    tc_fence_before();
-    __syncthreads();
-    tc_fence_after();
-    const uint32_t tmem = *tmem_slot;
-    const int per_tap = a.nblk[0] + a.nblk[1];
-    const int total = 9 * per_tap;
-
-    if (warp == 0 && lane == 0) {
-        int issued = 0;
-        for (int kb = 0; kb < total; kb++) {
-            const int s = kb % S, round = kb / S;
-            if (!mbar_wait(empty + s, (round & 1) ^ 1, a.err, 1)) break;
-            const int tap = kb / per_tap, j = kb % per_tap;
-            const int seg = j < a.nblk[0] ? 0 : 1, cb = seg ? j - a.nblk[0] : j;
-            mbar_expect_tx(full + s, kABytes + b_bytes);
-            tma_load_4d(sa + s * kABytes, seg ? &tmA1 : &tmA0, full + s, cb * 64, x0 + tap % 3 - 1, y0 + tap / 3 - 1,
-                        img);
-            tma_load_3d(sb + s * b_bytes, &tmB, full + s, j * 64, tap, 0);
-            issued = kb + 1;
-        }
-        // no copy may still be landing when the block exits
-        for (int kb = issued > S ? issued - S : 0; kb < issued; kb++) mbar_wait(full + kb % S, (kb / S) & 1, a.err, 64);
-    } else if (warp == 1 && lane == 0) {
-        const uint32_t idesc = idesc_bf16(a.ncols, false, false);
-        for (int kb = 0; kb < total; kb++) {
-            const int s = kb % S, round = kb / S;
-            if (!mbar_wait(full + s, round & 1, a.err, 2)) break;
-            tc_fence_after();
-            const uint64_t ad = desc_sw128(smem_u32(sa + s * kABytes), 16, 1024);
-            const uint64_t bd = desc_sw128(smem_u32(sb + s * b_bytes), 16, 1024);
-#pragma unroll
-            for (int kk = 0; kk < 4; kk++)  // K = 16 per MMA: 32 bytes along the swizzled row
-                umma_bf16(tmem, ad + 2 * kk, bd + 2 * kk, idesc, (kb | kk) != 0);
-            umma_commit(empty + s);
-        }
-        umma_commit(done);  // also on a timeout: tensor memory is freed only after the issued MMAs
-    }
-    __syncwarp();
-
-    // epilogue
-    const bool finished = mbar_wait(done, 0, a.err, 4);
-    tc_fence_after();
-    const int row = warp * 32 + lane;
-    const int px = x0 + (row % kTileW), py = y0 + (row / kTileW);
-    const bool inb = finished && px < a.W && py < a.H;
-    const long long pix = ((long long)img * a.H + py) * a.W + px;
+// Epilogue of one output row of a tile: TMEM columns -> bias, activation,
+// mask -> BF16 stores into the output segments.  taddr addresses this
+// thread's TMEM lane at column 0 of the tile's accumulator.
+__device__ __forceinline__ void conv_epilogue_row(const ConvArgs& a, uint32_t taddr, bool inb, long long pix) {
     for (int c = 0; c < a.ncols; c += 16) {
         uint32_t r[16];
-        tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, r);
+        tmem_ld16(taddr + (uint32_t)c, r);
         if (!inb) continue;
         for (int o = 0; o < a.nout; o++) {
             if (c < a.out_c0[o] || c >= a.out_c0[o] + a.out_cn[o]) continue;
@@ -319,9 +252,125 @@ __global__ void __launch_bounds__(128, 2) k_conv3x3(const __grid_constant__ CUte
             dst[1] = w1;
         }
     }
+}
+
+// Persistent form of k_conv3x3: one CTA per SM walks tiles blockIdx.x,
+// blockIdx.x + gridDim.x, ...  Warp 0 (lane 0) streams A/B boxes through
+// the stage ring without stopping between tiles; warp 1 (lane 0) issues
+// each tile's MMAs into one of two TMEM accumulators; warps 2-5 drain the
+// other accumulator (warp w owns TMEM lanes 32 (w % 4) .. +31), so the
+// epilogue of tile i overlaps the loads and MMAs of tile i + 1.
+constexpr int kConvPThreads = 192;
+
+__global__ void __launch_bounds__(kConvPThreads, 1) k_conv3x3_p(const __grid_constant__ CUtensorMap tmA0,
+                                                               const __grid_constant__ CUtensorMap tmA1,
+                                                               const __grid_constant__ CUtensorMap tmB,
+                                                               const ConvArgs a, int tiles_x, int tiles_y,
+                                                               int ntiles) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = align1024(smem_raw);
+    const int S = a.stages;
+    const uint32_t b_bytes = (uint32_t)a.ncols * 128;
+    uint8_t* sa = smem;
+    uint8_t* sb = smem + S * kABytes;
+    uint64_t* full = (uint64_t*)(sb + S * b_bytes);
+    uint64_t* empty = full + S;
+    uint64_t* accf = empty + S;  // accumulator k ready for the epilogue
+    uint64_t* acce = accf + 2;   // accumulator k drained
+    uint32_t* tmem_slot = (uint32_t*)(acce + 2);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < S; s++) {
+            mbar_init(full + s, 1);
+            mbar_init(empty + s, 1);
+        }
+        for (int k = 0; k < 2; k++) {
+            mbar_init(accf + k, 1);
+            mbar_init(acce + k, 128);
+        }
+        fence_barrier_init();
+    }
+    if (warp == 0) {
+        tmem_alloc(tmem_slot, 2 * a.tmem_cols);
+        tmem_relinquish();
+    }
     tc_fence_before();
     __syncthreads();
-    if (warp == 0) tmem_dealloc(tmem, a.tmem_cols);
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+    const int per_tap = a.nblk[0] + a.nblk[1];
+    const int total = 9 * per_tap;
+
+    if (warp == 0 && lane == 0) {
+        long long g = 0;  // K-blocks issued by this CTA, over all its tiles
+        bool ok = true;
+        for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+            const int x0 = (tile % tiles_x) * kTileW, y0 = ((tile / tiles_x) % tiles_y) * kTileH;
+            const int img = tile / (tiles_x * tiles_y);
+            for (int kb = 0; kb < total; kb++, g++) {
+                const int s = (int)(g % S);
+                const uint32_t round = (uint32_t)(g / S);
+                if (!mbar_wait(empty + s, (round & 1) ^ 1, a.err, 1)) {
+                    ok = false;
+                    break;
+                }
+                const int tap = kb / per_tap, j = kb % per_tap;
+                const int seg = j < a.nblk[0] ? 0 : 1, cb = seg ? j - a.nblk[0] : j;
+                mbar_expect_tx(full + s, kABytes + b_bytes);
+                tma_load_4d(sa + s * kABytes, seg ? &tmA1 : &tmA0, full + s, cb * 64, x0 + tap % 3 - 1,
+                            y0 + tap / 3 - 1, img);
+                tma_load_3d(sb + s * b_bytes, &tmB, full + s, j * 64, tap, 0);
+            }
+        }
+        for (long long k = g > S ? g - S : 0; k < g; k++) mbar_wait(full + k % S, (uint32_t)((k / S) & 1), a.err, 64);
+    } else if (warp == 1 && lane == 0) {
+        const uint32_t idesc = idesc_bf16(a.ncols, false, false);
+        long long g = 0;
+        int i = 0;
+        bool ok = true;
+        for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, i++) {
+            const int buf = i & 1;
+            if (!mbar_wait(acce + buf, ((uint32_t)(i >> 1) & 1) ^ 1, a.err, 128)) break;
+            tc_fence_after();
+            const uint32_t d = tmem + (uint32_t)(buf * a.tmem_cols);
+            for (int kb = 0; kb < total; kb++, g++) {
+                const int s = (int)(g % S);
+                if (!mbar_wait(full + s, (uint32_t)((g / S) & 1), a.err, 2)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const uint64_t ad = desc_sw128(smem_u32(sa + s * kABytes), 16, 1024);
+                const uint64_t bd = desc_sw128(smem_u32(sb + s * b_bytes), 16, 1024);
+#pragma unroll
+                for (int kk = 0; kk < 4; kk++) umma_bf16(d, ad + 2 * kk, bd + 2 * kk, idesc, (kb | kk) != 0);
+                umma_commit(empty + s);
+            }
+            umma_commit(accf + buf);  // also after a timeout: the epilogue then waits for the issued MMAs
+        }
+    } else if (warp >= 2) {
+        const uint32_t quarter = (uint32_t)(warp & 3);
+        const int row = (int)quarter * 32 + lane;
+        int i = 0;
+        for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, i++) {
+            const int buf = i & 1;
+            const bool ready = mbar_wait(accf + buf, (uint32_t)(i >> 1) & 1, a.err, 4);
+            tc_fence_after();
+            const int x0 = (tile % tiles_x) * kTileW, y0 = ((tile / tiles_x) % tiles_y) * kTileH;
+            const int img = tile / (tiles_x * tiles_y);
+            const int px = x0 + (row % kTileW), py = y0 + (row / kTileW);
+            const bool inb = ready && px < a.W && py < a.H;
+            const long long pix = ((long long)img * a.H + py) * a.W + px;
+            conv_epilogue_row(a, tmem + (quarter * 32u << 16) + (uint32_t)(buf * a.tmem_cols), inb, pix);
+            tc_fence_before();
+            mbar_arrive(acce + buf);
+            if (!ready) break;
+        }
+    }
+    __syncwarp();
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tmem, 2 * a.tmem_cols);
 }
 
 // ------------------------------------------------- the weight gradient
@@ -494,7 +543,7 @@ int weight_map(CUtensorMap* tm, const void* base, int k, int rows) {
 
 int pow2_cols(int n) { return n <= 32 ? 32 : n <= 64 ? 64 : n <= 128 ? 128 : 256; }
 
-int conv_smem(int ncols, int stages) { return stages * (int)(kABytes + ncols * 128) + 2 * stages * 8 + 16 + 1024; }
+int conv_smem(int ncols, int stages) { return stages * (int)(kABytes + ncols * 128) + (2 * stages + 4) * 8 + 16 + 1024; }
 
 }  // namespace
 
@@ -527,7 +576,12 @@ extern "C" int rl_dn_conv3x3(const void* in0, int c0, const void* in1, int c1, i
     a.nblk[1] = nb1;
     a.ncols = ncols;
     a.tmem_cols = pow2_cols(ncols);
-    a.stages = ncols > 128 ? 2 : 3;  // two CTAs per SM
+    // ring depth: two CTAs per SM while both fit in TMEM (2 x 2 accumulators of
+    // <= 128 columns), each with up to ~100 KB of stages; otherwise one CTA
+    // with up to ~200 KB
+    const int per_sm = pow2_cols(ncols) <= 128 ? 2 : 1;
+    const int stage_bytes = (int)(kABytes + ncols * 128);
+    a.stages = std::max(2, std::min(8, (per_sm == 2 ? 100 : 200) * 1024 / stage_bytes));
     a.bias = bias;
     a.relu = relu;
     a.slope = slope;
@@ -543,14 +597,24 @@ extern "C" int rl_dn_conv3x3(const void* in0, int c0, const void* in1, int c1, i
     a.mask[1] = (const bf16*)mask1;
     a.err = d_err;
     const int smem = conv_smem(ncols, a.stages);
+    static int sms = 0;
     static std::once_flag attr;
     cudaError_t ae = cudaSuccess;
-    std::call_once(attr, [&] { ae = cudaFuncSetAttribute(k_conv3x3, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024); });
-    if (ae != cudaSuccess) return dn_fail(RL_CUDA_ERROR, "conv smem attribute: %s", cudaGetErrorString(ae));
-    dim3 grid((width + kTileW - 1) / kTileW, (height + kTileH - 1) / kTileH, images);
-    k_conv3x3<<<grid, 128, smem, (cudaStream_t)stream>>>(tA0, tA1, tB, a);
+    std::call_once(attr, [&] {
+        ae = cudaFuncSetAttribute(k_conv3x3_p, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        int dev = 0;
+        if (ae == cudaSuccess) ae = cudaGetDevice(&dev);
+        if (ae == cudaSuccess) ae = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    });
+    if (ae != cudaSuccess) return dn_fail(RL_CUDA_ERROR, "conv set-up: %s", cudaGetErrorString(ae));
+    const int tiles_x = (width + kTileW - 1) / kTileW, tiles_y = (height + kTileH - 1) / kTileH;
+    const long long ntiles = (long long)tiles_x * tiles_y * images;
+    if (ntiles > INT32_MAX) return dn_fail(RL_INVALID_CALL, "rl_dn_conv3x3: too many tiles");
+    const int grid = (int)std::min<long long>(ntiles, (long long)per_sm * std::max(sms, 1));
+    k_conv3x3_p<<<grid, kConvPThreads, smem, (cudaStream_t)stream>>>(tA0, tA1, tB, a, tiles_x, tiles_y,
+                                                                    (int)ntiles);
     cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return dn_fail(RL_CUDA_ERROR, "k_conv3x3: %s", cudaGetErrorString(e));
+    if (e != cudaSuccess) return dn_fail(RL_CUDA_ERROR, "k_conv3x3_p: %s", cudaGetErrorString(e));
     return RL_OK;
 }
 

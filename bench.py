@@ -151,9 +151,10 @@ def gpu_arm(args, rank, world, local_rank):
     if knn:
         from relight_b200.device import PhotonRecords
         records = PhotonRecords(8 << 20)
-        launches_per_step += 4  # k_knn_keys, radix sort (counted as one), k_knn_scatter, k_knn_query
+        # k_knn_bounds, k_knn_grid, k_knn_keys, radix sort (counted as one), k_knn_scatter, k_knn_start, k_knn_query
+        launches_per_step += 7
 
-    def step(seed, fg_events=None):
+    def step(seed, fg_events=None, knn_events=None):
         _abi.check(L.rl_map_clear(pmap.handle, 1, 1, sh))
         _abi.check(L.rl_map_clear(lmap.handle, 1, 0, sh))
         if knn:
@@ -166,7 +167,11 @@ def gpu_arm(args, rank, world, local_rank):
                                          seed, None, sh))
         _abi.check(L.rl_photonmap_gather(pmap.handle, st.final_gather_radius, sh))
         if knn:
+            if knn_events:
+                knn_events[0].record(stream)
             records.gather_knn(pmap, 0, KNN_K, KNN_RADIUS, sh)
+            if knn_events:
+                knn_events[1].record(stream)
         if fg_events:
             fg_events[0].record(stream)
         _abi.check(L.rl_bake_indirect(ds.handle, lmap.handle, maps, 1, st.final_gather_samples,
@@ -180,20 +185,22 @@ def gpu_arm(args, rank, world, local_rank):
     torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
-    step_ms, fg_ms = [], []
+    step_ms, fg_ms, knn_ms = [], [], []
     with ClockSampler(local_rank) as clocks:
         torch.cuda.synchronize()
         if world > 1:
             torch.distributed.barrier()
         for i in range(args.steps):
             flush.zero_()
-            e0, e1, f0, f1 = ev(), ev(), ev(), ev()
+            e0, e1, f0, f1, k0, k1 = ev(), ev(), ev(), ev(), ev(), ev()
             e0.record(stream)
-            step(1001 + 2 * i, (f0, f1))
+            step(1001 + 2 * i, (f0, f1), (k0, k1))
             e1.record(stream)
             torch.cuda.synchronize()
             step_ms.append(e0.elapsed_time(e1))
             fg_ms.append(f0.elapsed_time(f1))
+            if knn:
+                knn_ms.append(k0.elapsed_time(k1))
         torch.cuda.synchronize()
         if world > 1:
             torch.distributed.barrier()
@@ -257,11 +264,13 @@ def gpu_arm(args, rank, world, local_rank):
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded fBm terrain + boxes)",
         "config": {"workload": WORKLOAD + (f", kNN k={KNN_K} r={KNN_RADIUS}" if knn else ""),
-                   "gather": args.gather, "bvh_width": autotune.get_width(), "lightmap": [lmap.width, lmap.height], "valid_texels": valid,
+                   "gather": args.gather, "bvh_width": autotune.get_width(),
+                   **({"knn_cell_64ths": autotune.get_knn_cell()} if knn else {}), "lightmap": [lmap.width, lmap.height], "valid_texels": valid,
                    "photons": int(st.photon_pass_count * 125000), "fg_samples": st.final_gather_samples, "triangles": flat.ntris,
                    "parallelism": f"replicas x{world}", "l2": "flushed between steps (256 MiB write)"},
         "grays_per_s": rays_per_step * args.steps * world / (total_ms / 1e3) / 1e9,
         "fg_ms": sum(fg_ms) / len(fg_ms),
+        **({"knn_ms": sum(knn_ms) / len(knn_ms)} if knn else {}),
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": e2e_total / args.steps},
         "roofline": {"kernel": "k_indirect (final gather)", "bound": "hbm", "achieved": achieved, "peak": peak,
@@ -589,6 +598,8 @@ def main():
                     help="traversal tree for AO / final gather (0: the library's default)")
     ap.add_argument("--gather", default="disc", choices=["disc", "knn"],
                     help="photon estimate: Relight's disc gather (default) or the k-nearest-neighbour estimate")
+    ap.add_argument("--knn-cell", type=int, default=0,
+                    help="kNN grid cell width in 64ths of the radius (0: the library's default)")
     ap.add_argument("--workload", default="terrain", choices=["terrain", "batch", "serve", "denoise"],
                     help="terrain: the photon + final-gather bake (default); batch: uneven-size batching; "
                          "serve: the bake-serving loop with the denoiser; denoise: the denoiser at equal RMSE")
@@ -598,6 +609,9 @@ def main():
     if args.bvh_width:
         from relight_b200 import autotune
         autotune.set_width(args.bvh_width)
+    if args.knn_cell:
+        from relight_b200 import autotune
+        autotune.set_knn_cell(args.knn_cell)
     if args.workload == "batch":
         print(json.dumps(batch_arm(args)), flush=True)
         return

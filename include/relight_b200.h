@@ -257,7 +257,8 @@ int rl_photon_count(const rl_light* lights, int nlights, int pass_count, int64_t
    at every valid lumel of the photonmap in `slot`, gathered = the mean
    colour of the k nearest deposits of that photonmap within `radius` world
    units of the lumel position (ties by photon number and bounce; 0 when
-   none), over a hashed grid of `radius`-wide cells.  Run it after
+   none), over a uniform grid of cells RL_TUNE_KNN_CELL / 64 of the radius
+   wide (half by default).  Run it after
    rl_photonmap_gather: lumels that are not valid keep the disc's value. */
 typedef struct rl_photons rl_photons;
 int rl_photons_create(int64_t capacity, rl_photons** out);
@@ -267,6 +268,11 @@ int rl_photons_count(const rl_photons* records, int64_t* deposits);
 /* The kept records, in no particular order: xyzrgb [n][6], photon [n],
    depth_slot [n][2] (any may be NULL; n = min(count, capacity)). */
 int rl_photons_download(const rl_photons* records, float* xyzrgb, uint32_t* photon, int32_t* depth_slot);
+/* Replaces the records with n given ones (same layout as the download;
+   depth and slot in [0, 65535]), as if an emission had kept them: records
+   from another emitter, or planted cases.  No reference counterpart. */
+int rl_photons_upload(rl_photons* records, int64_t n, const float* xyzrgb, const uint32_t* photon,
+                      const int32_t* depth_slot);
 int rl_emit_photons_records(const rl_scene* scene, rl_map* const* photonmaps, int nmaps, const rl_light* lights,
                             int nlights, int pass_count, int max_depth, float threshold, float max_distance,
                             uint64_t seed, rl_photons* records, int64_t* stored, void* stream);
@@ -485,14 +491,17 @@ int rl_radiosity_solve_noalloc(int n, const int64_t* d_row_ptr, const int32_t* d
                         8-wide nodes, built for scenes created while it is
                         selected);
      RL_TUNE_SPECULATIVE: 1 = binary traversal parks leaves until the whole
-                          warp has one (speculative traversal), 0 = off. */
+                          warp has one (speculative traversal), 0 = off;
+     RL_TUNE_KNN_CELL: cell width of rl_photonmap_gather_knn's grid in 64ths
+                       of its radius (8..128, default 32). */
 enum {
     RL_TUNE_FG_REFILL = 0,
     RL_TUNE_FG_BLOCK = 1,
     RL_TUNE_AO_REFILL = 2,
     RL_TUNE_AO_BLOCK = 3,
     RL_TUNE_BVH_WIDTH = 4,
-    RL_TUNE_SPECULATIVE = 5
+    RL_TUNE_SPECULATIVE = 5,
+    RL_TUNE_KNN_CELL = 6
 };
 int rl_tune_set(int param, int value);
 int rl_tune_get(int param, int* value);

@@ -17,6 +17,7 @@ RL_OK, RL_INVALID_CALL, RL_NOT_IMPLEMENTED, RL_OUT_OF_MEMORY, RL_CUDA_ERROR, RL_
 HIT_POINT, HIT_UV, HIT_COLOR, HIT_NORMAL, HIT_USE_ALPHA = 1, 2, 4, 8, 16
 HIT_ALL = 15
 TUNE_FG_REFILL, TUNE_FG_BLOCK, TUNE_AO_REFILL, TUNE_AO_BLOCK, TUNE_BVH_WIDTH, TUNE_SPECULATIVE = 0, 1, 2, 3, 4, 5
+TUNE_KNN_CELL = 6
 SOLVE_NOALLOC_MAX_PATCHES = 65536
 
 
@@ -146,6 +147,7 @@ SIGNATURES = {
     "rl_photons_destroy": (_I, [_P]),
     "rl_photons_count": (_I, [_P, _P]),
     "rl_photons_download": (_I, [_P, _P, _P, _P]),
+    "rl_photons_upload": (_I, [_P, _I64, _P, _P, _P]),
     "rl_emit_photons_records": (_I, [_P, _P, _I, _P, _I, _I, _I, _F, _F, _U64, _P, _P, _P]),
     "rl_photonmap_gather_knn": (_I, [_P, _I, _P, _I, _F, _P]),
     "rl_batch_create": (_I, [_P, _I, _P]),

@@ -56,6 +56,17 @@ def set_speculative(on):
     _abi.check(_abi.lib().rl_tune_set(_abi.TUNE_SPECULATIVE, int(bool(on))))
 
 
+def get_knn_cell():
+    v = C.c_int()
+    _abi.check(_abi.lib().rl_tune_get(_abi.TUNE_KNN_CELL, C.byref(v)))
+    return v.value
+
+
+def set_knn_cell(sixty_fourths):
+    """kNN grid cell width in 64ths of the search radius (8..128)."""
+    _abi.check(_abi.lib().rl_tune_set(_abi.TUNE_KNN_CELL, int(sixty_fourths)))
+
+
 def tune(run, kernel="indirect", refills=REFILLS, blocks=BLOCKS, widths=(2,), speculative=(0, 1), reps=2,
          stream=None):
     """`run()` enqueues one call of `kernel` ("indirect" or "ao") on `stream`

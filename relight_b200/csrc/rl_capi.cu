@@ -68,7 +68,9 @@ inline cudaStream_t S(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 // Launch tuning (rl_tune_set): per ray-stream kernel, the number of lanes a
 // warp waits for before refilling rays and the threads per block.  Defaults
 // are the autotuner's picks on the terrain final-gather / room AO workloads.
-int g_tune[6] = {24, 64, 32, 128, 2, 0};  // + BVH width, speculative traversal
+// Then the BVH width, speculative traversal, and the kNN grid's cell width
+// in 64ths of the search radius.
+int g_tune[7] = {24, 64, 32, 128, 2, 0, 32};
 
 inline unsigned blocks_for(long long n, int threads) { return (unsigned)((n + threads - 1) / threads); }
 
@@ -164,8 +166,10 @@ extern "C" int rl_tune_set(int param, int value) {
     bool block = param == RL_TUNE_FG_BLOCK || param == RL_TUNE_AO_BLOCK;
     bool width = param == RL_TUNE_BVH_WIDTH;
     bool spec = param == RL_TUNE_SPECULATIVE;
+    bool cell = param == RL_TUNE_KNN_CELL;
     if ((refill && value >= 1 && value <= 32) || (block && (value == 64 || value == 128 || value == 256)) ||
-        (width && (value == 2 || value == 4 || value == 8)) || (spec && (value == 0 || value == 1)))
+        (width && (value == 2 || value == 4 || value == 8)) || (spec && (value == 0 || value == 1)) ||
+        (cell && value >= 8 && value <= 128))
         g_tune[param] = value;
     else
         return fail(RL_INVALID_CALL, "rl_tune_set: bad parameter %d or value %d", param, value);
@@ -173,10 +177,12 @@ extern "C" int rl_tune_set(int param, int value) {
 }
 
 extern "C" int rl_tune_get(int param, int* value) {
-    if (!value || param < 0 || param > 5) return fail(RL_INVALID_CALL, "rl_tune_get: bad parameter");
+    if (!value || param < 0 || param > RL_TUNE_KNN_CELL) return fail(RL_INVALID_CALL, "rl_tune_get: bad parameter");
     *value = g_tune[param];
     return RL_OK;
 }
+
+int rl_internal_tune(int param) { return g_tune[param]; }
 
 // ------------------------------------------------------------- scene
 

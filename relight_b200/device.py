@@ -170,7 +170,7 @@ class DeviceMap:
 
 
 class PhotonRecords:
-    """rl_photons: world-space photon deposits and their hashed grid, for
+    """rl_photons: world-space photon deposits and their grid, for
     the k-nearest-neighbour estimate."""
 
     def __init__(self, capacity: int):
@@ -192,6 +192,15 @@ class PhotonRecords:
         check(lib().rl_photons_download(self.handle, C.c_void_p(xyz.ctypes.data), C.c_void_p(ph.ctypes.data),
                                         C.c_void_p(ds.ctypes.data)))
         return xyz, ph, ds[:, 0], ds[:, 1]
+
+    def upload(self, xyzrgb, photon, depth, slot):
+        """Replace the records (rl_photons_upload): xyzrgb [n][6], photon [n],
+        depth [n], slot [n]."""
+        xyz = np.ascontiguousarray(xyzrgb, np.float32).reshape(-1, 6)
+        ph = np.ascontiguousarray(photon, np.uint32)
+        ds = np.ascontiguousarray(np.stack([np.asarray(depth), np.asarray(slot)], 1), np.int32)
+        check(lib().rl_photons_upload(self.handle, len(xyz), C.c_void_p(xyz.ctypes.data), C.c_void_p(ph.ctypes.data),
+                                      C.c_void_p(ds.ctypes.data)))
 
     def gather_knn(self, photonmap, slot: int, k: int = 100, radius: float = 1.0, stream=None):
         """rl_photonmap_gather_knn on a DeviceMap (after its disc gather)."""

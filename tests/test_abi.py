@@ -40,3 +40,19 @@ def test_version_and_error_text_without_gpu():
     assert b"sm_100a" in lib.rl_version()
     buf = C.create_string_buffer(64)
     assert lib.rl_last_error(buf, 64) >= 0
+
+
+def test_tune_parameters_are_checked_without_gpu():
+    """rl_tune_set keeps each parameter within its documented range and
+    changes nothing on a refusal."""
+    lib = _abi.load()
+    v = C.c_int()
+    assert lib.rl_tune_get(_abi.TUNE_KNN_CELL, C.byref(v)) == 0 and v.value == 32
+    for bad in (7, 129, 0, -1):
+        assert lib.rl_tune_set(_abi.TUNE_KNN_CELL, bad) != 0
+    assert lib.rl_tune_get(_abi.TUNE_KNN_CELL, C.byref(v)) == 0 and v.value == 32
+    assert lib.rl_tune_set(_abi.TUNE_KNN_CELL, 48) == 0
+    assert lib.rl_tune_get(_abi.TUNE_KNN_CELL, C.byref(v)) == 0 and v.value == 48
+    assert lib.rl_tune_set(_abi.TUNE_KNN_CELL, 32) == 0
+    assert lib.rl_tune_get(_abi.TUNE_KNN_CELL + 1, C.byref(v)) != 0
+    assert lib.rl_tune_set(_abi.TUNE_BVH_WIDTH, 3) != 0

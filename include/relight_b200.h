@@ -258,8 +258,11 @@ int rl_photon_count(const rl_light* lights, int nlights, int pass_count, int64_t
    colour of the k nearest deposits of that photonmap within `radius` world
    units of the lumel position (ties by photon number and bounce; 0 when
    none), over a uniform grid of cells RL_TUNE_KNN_CELL / 64 of the radius
-   wide (half by default).  Run it after
-   rl_photonmap_gather: lumels that are not valid keep the disc's value. */
+   wide.  The colours are summed exactly in 64-bit fixed point (2^s per unit,
+   2^53 <= s-scaled largest colour < 2^54) and the mean is taken in double
+   precision, so the value depends only on which deposits are nearest.  Run
+   it after rl_photonmap_gather: lumels that are not valid keep the disc's
+   value. */
 typedef struct rl_photons rl_photons;
 int rl_photons_create(int64_t capacity, rl_photons** out);
 int rl_photons_destroy(rl_photons* records);
@@ -493,7 +496,7 @@ int rl_radiosity_solve_noalloc(int n, const int64_t* d_row_ptr, const int32_t* d
      RL_TUNE_SPECULATIVE: 1 = binary traversal parks leaves until the whole
                           warp has one (speculative traversal), 0 = off;
      RL_TUNE_KNN_CELL: cell width of rl_photonmap_gather_knn's grid in 64ths
-                       of its radius (8..128, default 32). */
+                       of its radius (8..256, default 80). */
 enum {
     RL_TUNE_FG_REFILL = 0,
     RL_TUNE_FG_BLOCK = 1,

@@ -63,7 +63,7 @@ def get_knn_cell():
 
 
 def set_knn_cell(sixty_fourths):
-    """kNN grid cell width in 64ths of the search radius (8..128)."""
+    """kNN grid cell width in 64ths of the search radius (8..256)."""
     _abi.check(_abi.lib().rl_tune_set(_abi.TUNE_KNN_CELL, int(sixty_fourths)))
 
 

@@ -69,8 +69,8 @@ inline cudaStream_t S(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 // warp waits for before refilling rays and the threads per block.  Defaults
 // are the autotuner's picks on the terrain final-gather / room AO workloads.
 // Then the BVH width, speculative traversal, and the kNN grid's cell width
-// in 64ths of the search radius.
-int g_tune[7] = {24, 64, 32, 128, 2, 0, 32};
+// in 64ths of the search radius (the fastest on the terrain kNN bench).
+int g_tune[7] = {24, 64, 32, 128, 2, 0, 80};
 
 inline unsigned blocks_for(long long n, int threads) { return (unsigned)((n + threads - 1) / threads); }
 
@@ -169,7 +169,7 @@ extern "C" int rl_tune_set(int param, int value) {
     bool cell = param == RL_TUNE_KNN_CELL;
     if ((refill && value >= 1 && value <= 32) || (block && (value == 64 || value == 128 || value == 256)) ||
         (width && (value == 2 || value == 4 || value == 8)) || (spec && (value == 0 || value == 1)) ||
-        (cell && value >= 8 && value <= 128))
+        (cell && value >= 8 && value <= 256))
         g_tune[param] = value;
     else
         return fail(RL_INVALID_CALL, "rl_tune_set: bad parameter %d or value %d", param, value);

@@ -9,19 +9,25 @@
 // photonmap (rl_emit_photons_records keeps each one as a record).
 //
 //   build:  the records of the requested slot span a box; a dense grid of
-//           cells (half the radius wide by default, RL_TUNE_KNN_CELL) covers
-//           it; cells grow when the box would need more than 2^24 of them.  One radix sort orders the
+//           cells (1.25 radii wide by default, RL_TUNE_KNN_CELL) covers it;
+//           cells grow when the box would need more than 2^24 of them.  One radix sort orders the
 //           records by cell, x fastest, so that every row of cells along x
 //           is one contiguous range; start[c] = first record of cell c.
-//   query:  one thread per lumel, 8x8 lumel tiles per block.  Pass 1 scans
-//           the cells within one cell of the lumel and keeps the k nearest
-//           records in a max-heap in shared memory ordered by (squared
-//           distance, record id).  Every record it skipped is farther than
-//           one cell, so when the heap is full and its largest distance is
-//           below one cell the selection is final.  Otherwise pass 2 scans
-//           the rest of the cells within the radius.  The k records are
-//           summed in ascending (distance, id) order, so the result does
-//           not depend on emission order, sort order or thread timing.
+//   query:  one warp per lumel (8x8 lumel tiles per block, a tile row per
+//           warp).  The warp visits shells of cells at growing distance,
+//           32 records at a time, and appends those within the radius to a
+//           buffer in shared memory; when the buffer fills it is sorted and
+//           cut to the k nearest, which then bound admission.  After each
+//           shell every record not yet seen is provably farther than the
+//           shell's half-width, so the search stops once that passes the
+//           admission bound.  The k nearest by (squared distance, record
+//           id) come from binary searches over the buffer's distance bits
+//           (and record ids on exact ties).  Their colours are summed in
+//           64-bit fixed point (2^s per unit, s set per gather from the
+//           largest colour so that no sum can overflow) and the mean taken
+//           in double precision, so the result depends only on which
+//           records are selected: not on emission order, sort order, cell
+//           width or thread timing.
 // Lumels that are not valid keep the disc gather's value.
 #include <cuda_runtime.h>
 
@@ -51,6 +57,8 @@ struct KnnGrid {
     int nx, ny, nz;
     int n;
     unsigned long long count;
+    float scale;     // 2^s: colour -> fixed point
+    double unscale;  // 2^-s
 };
 
 // Box of one slot's records: ordered-integer images of the floats, so that
@@ -58,6 +66,7 @@ struct KnnGrid {
 struct KnnBounds {
     uint32_t lo[3];  // ~max(~key)
     uint32_t hi[3];
+    uint32_t cmax;   // bits of the largest |colour component|
 };
 
 }  // namespace
@@ -111,7 +120,6 @@ int kfail(int code, const char* fmt, ...) {
 
 constexpr int kMaxK = 128;
 constexpr int kKnnTile = 8;  // lumels per block: kKnnTile x kKnnTile
-constexpr int kKnnBlock = kKnnTile * kKnnTile;
 constexpr long long kMaxCells = (1ll << 24) - 1;
 
 __device__ __forceinline__ uint32_t ordered(float f) {
@@ -122,8 +130,11 @@ __device__ __forceinline__ float unordered(uint32_t u) {
     return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
 }
 
-__device__ __forceinline__ bool finite3(const PhotonRecord& r) {
-    return isfinite(r.x) && isfinite(r.y) && isfinite(r.z);
+// The records a gather of `slot` uses: that slot's, with finite position
+// and colour.
+__device__ __forceinline__ bool eligible(const PhotonRecord& r, int slot) {
+    return r.slot == slot && isfinite(r.x) && isfinite(r.y) && isfinite(r.z) && isfinite(r.r) && isfinite(r.g) &&
+           isfinite(r.b);
 }
 
 __device__ __forceinline__ long long kept(const unsigned long long* count, long long capacity) {
@@ -134,26 +145,31 @@ __device__ __forceinline__ long long kept(const unsigned long long* count, long 
 __global__ void k_knn_bounds(const PhotonRecord* rec, const unsigned long long* count, long long capacity, int slot,
                              KnnBounds* b) {
     const long long n = kept(count, capacity);
-    uint32_t lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+    uint32_t lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0}, cmax = 0;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         const PhotonRecord r = rec[i];
-        if (r.slot != slot || !finite3(r)) continue;
+        if (!eligible(r, slot)) continue;
         const uint32_t k[3] = {ordered(r.x), ordered(r.y), ordered(r.z)};
         for (int a = 0; a < 3; a++) {
             lo[a] = max(lo[a], ~k[a]);
             hi[a] = max(hi[a], k[a]);
         }
+        // non-negative float bits order like the floats
+        cmax = max(cmax, max(__float_as_uint(fabsf(r.r)), max(__float_as_uint(fabsf(r.g)), __float_as_uint(fabsf(r.b)))));
     }
     for (int a = 0; a < 3; a++)
         for (int o = 16; o > 0; o >>= 1) {
             lo[a] = max(lo[a], __shfl_xor_sync(0xffffffffu, lo[a], o));
             hi[a] = max(hi[a], __shfl_xor_sync(0xffffffffu, hi[a], o));
         }
-    if ((threadIdx.x & 31) == 0)
+    for (int o = 16; o > 0; o >>= 1) cmax = max(cmax, __shfl_xor_sync(0xffffffffu, cmax, o));
+    if ((threadIdx.x & 31) == 0) {
         for (int a = 0; a < 3; a++) {
             if (lo[a]) atomicMax(&b->lo[a], lo[a]);
             if (hi[a]) atomicMax(&b->hi[a], hi[a]);
         }
+        if (cmax) atomicMax(&b->cmax, cmax);
+    }
 }
 
 // One thread: the grid of the box.  No records -> zero cells.
@@ -163,6 +179,16 @@ __global__ void k_knn_grid(const KnnBounds* b, const unsigned long long* count, 
     o.count = *count;
     o.n = (int)kept(count, capacity);
     o.nx = o.ny = o.nz = 0;
+    // Fixed point for the colour sums: 2^s with |colour| * 2^s < 2^54, so
+    // that kMaxK terms stay below 2^61.  s in [-100, 100] (2^s a normal float).
+    int s = 0;
+    if (b->cmax) {
+        int e;
+        frexp((double)__uint_as_float(b->cmax), &e);  // cmax < 2^e
+        s = min(100, max(-100, 54 - e));
+    }
+    o.scale = ldexpf(1.0f, s);
+    o.unscale = ldexp(1.0, -s);
     if (b->hi[0] != 0) {
         const float lo[3] = {unordered(~b->lo[0]), unordered(~b->lo[1]), unordered(~b->lo[2])};
         const float hi[3] = {unordered(b->hi[0]), unordered(b->hi[1]), unordered(b->hi[2])};
@@ -202,7 +228,7 @@ __global__ void k_knn_keys(const PhotonRecord* rec, long long capacity, int slot
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < g.n; i += (long long)gridDim.x * blockDim.x) {
         const PhotonRecord r = rec[i];
         uint32_t key = none;
-        if (r.slot == slot && finite3(r)) {
+        if (eligible(r, slot)) {
             const int ix = cell_axis(r.x, g.ox, g.inv, g.nx), iy = cell_axis(r.y, g.oy, g.inv, g.ny),
                       iz = cell_axis(r.z, g.oz, g.inv, g.nz);
             key = (uint32_t)(((long long)iz * g.ny + iy) * g.nx + ix);
@@ -235,164 +261,256 @@ __global__ void k_knn_start(const uint32_t* keys, int n, uint32_t cells, uint32_
     }
 }
 
-// Per-thread max-heap of (squared distance, sorted position) in shared
-// memory, entry e of thread t at [e * kKnnBlock + t], ordered by
-// (distance, record id); ids are read only on distance ties.
-struct KnnHeap {
-    float* d;
-    uint32_t* j;
-    const PhotonRecord* rec;
-    int t, size, k;
-    float top_d;  // largest entry, valid when size == k
-    uint32_t top_j;
+// A box of cells, bounds inclusive (empty when lx > hx).
+struct KnnBox {
+    int lx, hx, ly, hy, lz, hz;
+};
 
-    __device__ __forceinline__ bool less(float da, uint32_t ja, float db, uint32_t jb) const {
-        if (da != db) return da < db;
-        return record_id(rec[ja]) < record_id(rec[jb]);
-    }
-    __device__ __forceinline__ float& D(int e) { return d[e * kKnnBlock + t]; }
-    __device__ __forceinline__ uint32_t& J(int e) { return j[e * kKnnBlock + t]; }
+// The cells holding the records within h of (px, py, pz) along every axis.
+// cell_axis is monotone, so the box only grows with h, and a record outside
+// it lies below px - h or above px + h as rounded (or likewise along y, z).
+__device__ __forceinline__ KnnBox box_around(const KnnGrid& g, float px, float py, float pz, float h) {
+    return {cell_axis(px - h, g.ox, g.inv, g.nx), cell_axis(px + h, g.ox, g.inv, g.nx),
+            cell_axis(py - h, g.oy, g.inv, g.ny), cell_axis(py + h, g.oy, g.inv, g.ny),
+            cell_axis(pz - h, g.oz, g.inv, g.nz), cell_axis(pz + h, g.oz, g.inv, g.nz)};
+}
 
-    __device__ __forceinline__ void push(float dd, uint32_t jj) {
-        int c = size++;
-        while (c > 0) {
-            const int p = (c - 1) >> 1;
-            const float pd = D(p);
-            const uint32_t pj = J(p);
-            if (!less(pd, pj, dd, jj)) break;
-            D(c) = pd;
-            J(c) = pj;
-            c = p;
-        }
-        D(c) = dd;
-        J(c) = jj;
-        if (size == k) {
-            top_d = D(0);
-            top_j = J(0);
-        }
+constexpr int kKnnWarps = 8;              // warps per block: one row of an 8x8 lumel tile each
+constexpr int kKnnBuf = 256;              // candidate entries per warp
+constexpr int kKnnPer = kKnnBuf / 32;     // buffer entries per lane (entry lane + 32 q)
+constexpr uint32_t kNoEntry = 0xffffffffu;  // distance bits above every real squared distance
+
+__device__ __forceinline__ uint64_t warp_max64(uint64_t v) {
+    for (int o = 16; o > 0; o >>= 1) {
+        const uint64_t w = __shfl_xor_sync(0xffffffffu, (unsigned long long)v, o);
+        v = w > v ? w : v;
     }
-    // Put (dd, jj) at the root of a heap of n entries and sift it down.
-    __device__ __forceinline__ void sift_root(float dd, uint32_t jj, int n) {
+    return v;
+}
+
+// The k nearest of the n > k buffer entries, by (squared distance, record
+// id): each lane's entries lane + 32 q get sel[q].  Distances are
+// non-negative, so their bits order like them; a binary search on the bits
+// finds the k-th distance v, then one on record ids settles ties at v.
+// Returns the largest selected key in (*tau_d, *tau_id).
+__device__ __forceinline__ void warp_select(const uint32_t (&bits)[kKnnPer], const uint32_t (&jj)[kKnnPer], int k,
+                                            const PhotonRecord* __restrict__ rec, bool (&sel)[kKnnPer],
+                                            float* tau_d, uint64_t* tau_id) {
+    uint32_t v = 0;
+    for (int bit = 30; bit >= 0; bit--) {
+        const uint32_t t = v + (1u << bit) - 1u;
         int c = 0;
-        for (;;) {
-            const int l = 2 * c + 1;
-            if (l >= n) break;
-            int g = l;
-            if (l + 1 < n && less(D(l), J(l), D(l + 1), J(l + 1))) g = l + 1;
-            if (!less(dd, jj, D(g), J(g))) break;
-            D(c) = D(g);
-            J(c) = J(g);
-            c = g;
-        }
-        D(c) = dd;
-        J(c) = jj;
+#pragma unroll
+        for (int q = 0; q < kKnnPer; q++) c += bits[q] <= t;
+        if ((int)__reduce_add_sync(0xffffffffu, (unsigned)c) < k) v += 1u << bit;
     }
-    __device__ __forceinline__ void offer(float dd, uint32_t jj, float r2) {
-        if (!(dd <= r2)) return;
-        if (size < k) {
-            push(dd, jj);
-        } else if (dd < top_d || (dd == top_d && record_id(rec[jj]) < record_id(rec[top_j]))) {
-            sift_root(dd, jj, size);
-            top_d = D(0);
-            top_j = J(0);
+    int cl = 0, ce = 0;
+#pragma unroll
+    for (int q = 0; q < kKnnPer; q++) {
+        cl += bits[q] < v;
+        ce += bits[q] == v;
+    }
+    cl = (int)__reduce_add_sync(0xffffffffu, (unsigned)cl);
+    ce = (int)__reduce_add_sync(0xffffffffu, (unsigned)ce);
+    const int slots = k - cl;  // 1 <= slots <= ce
+    uint64_t ids[kKnnPer];
+#pragma unroll
+    for (int q = 0; q < kKnnPer; q++) ids[q] = bits[q] == v ? record_id(rec[jj[q]]) : ~0ull;
+    uint64_t idmax;
+    if (slots == ce) {
+        uint64_t m = 0;
+#pragma unroll
+        for (int q = 0; q < kKnnPer; q++)
+            if (bits[q] == v && ids[q] > m) m = ids[q];
+        idmax = warp_max64(m);
+    } else {
+        // the slots-th smallest id at distance v (ids have 36 bits)
+        uint64_t u = 0;
+        for (int bit = 35; bit >= 0; bit--) {
+            const uint64_t t = u + (1ull << bit) - 1ull;
+            int c = 0;
+#pragma unroll
+            for (int q = 0; q < kKnnPer; q++) c += ids[q] <= t;
+            if ((int)__reduce_add_sync(0xffffffffu, (unsigned)c) < slots) u += 1ull << bit;
+        }
+        idmax = u;
+    }
+#pragma unroll
+    for (int q = 0; q < kKnnPer; q++) sel[q] = bits[q] < v || (bits[q] == v && ids[q] <= idmax);
+    *tau_d = __uint_as_float(v);
+    *tau_id = idmax;
+}
+
+// One warp per lumel, all lanes on the same lumel.
+struct KnnWarp {
+    float* bd;       // [kKnnBuf] squared distances
+    uint32_t* bj;    // [kKnnBuf] grid positions
+    const float4* __restrict__ pos;
+    const PhotonRecord* __restrict__ rec;
+    int lane, k, cnt;
+    float r2;
+    bool limited;    // the buffer was cut to k: admit only keys below (tau_d, tau_id)
+    float tau_d;
+    uint64_t tau_id;
+
+    __device__ __forceinline__ void load(uint32_t (&bits)[kKnnPer], uint32_t (&jj)[kKnnPer]) const {
+#pragma unroll
+        for (int q = 0; q < kKnnPer; q++) {
+            const int e = lane + 32 * q;
+            bits[q] = e < cnt ? __float_as_uint(bd[e]) : kNoEntry;
+            jj[q] = e < cnt ? bj[e] : 0u;
+        }
+    }
+
+    // Cut the buffer to its k nearest entries.
+    __device__ __forceinline__ void cut() {
+        uint32_t bits[kKnnPer], jj[kKnnPer];
+        bool sel[kKnnPer];
+        __syncwarp();
+        load(bits, jj);
+        warp_select(bits, jj, k, rec, sel, &tau_d, &tau_id);
+        __syncwarp();
+        int at = 0;
+#pragma unroll
+        for (int q = 0; q < kKnnPer; q++) {
+            const unsigned vote = __ballot_sync(0xffffffffu, sel[q]);
+            if (sel[q]) {
+                const int e = at + __popc(vote & ((1u << lane) - 1u));
+                bd[e] = __uint_as_float(bits[q]);
+                bj[e] = jj[q];
+            }
+            at += __popc(vote);
+        }
+        cnt = k;
+        limited = true;
+    }
+
+    // The records of [a, b), 32 at a time; admitted ones join the buffer.
+    __device__ __forceinline__ void scan(uint32_t a, uint32_t b, float px, float py, float pz) {
+        for (uint32_t base = a; base < b; base += 32) {
+            if (cnt + 32 > kKnnBuf) cut();
+            const uint32_t j = base + lane;
+            bool take = false;
+            float d2 = 0.f;
+            if (j < b) {
+                const float4 q = __ldg(pos + j);
+                const float ex = q.x - px, ey = q.y - py, ez = q.z - pz;
+                d2 = ex * ex + ey * ey + ez * ez;
+                take = d2 <= r2 && (!limited || d2 < tau_d || (d2 == tau_d && record_id(rec[j]) < tau_id));
+            }
+            const unsigned vote = __ballot_sync(0xffffffffu, take);
+            if (take) {
+                const int at = cnt + __popc(vote & ((1u << lane) - 1u));
+                bd[at] = d2;
+                bj[at] = j;
+            }
+            cnt += __popc(vote);
         }
     }
 };
 
-__device__ __forceinline__ void scan_range(KnnHeap& h, const float4* __restrict__ pos, uint32_t a, uint32_t b,
-                                           float px, float py, float pz, float r2) {
-    uint32_t jj = a;
-    for (; jj + 4 <= b; jj += 4) {
-        float4 q[4];
-#pragma unroll
-        for (int u = 0; u < 4; u++) q[u] = __ldg(pos + jj + u);
-#pragma unroll
-        for (int u = 0; u < 4; u++) {
-            const float ex = q[u].x - px, ey = q[u].y - py, ez = q[u].z - pz;
-            h.offer(ex * ex + ey * ey + ez * ez, jj + u, r2);
-        }
-    }
-    for (; jj < b; jj++) {
-        const float4 q = __ldg(pos + jj);
-        const float ex = q.x - px, ey = q.y - py, ez = q.z - pz;
-        h.offer(ex * ex + ey * ey + ez * ez, jj, r2);
-    }
+__device__ __forceinline__ long long fixed(float c, float scale) { return __float2ll_rn(c * scale); }
+
+__device__ __forceinline__ long long warp_sum64(long long v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
 }
 
-__global__ void __launch_bounds__(kKnnBlock) k_knn_query(rl::DevMap m, const float4* __restrict__ pos,
-                                                         const PhotonRecord* __restrict__ rec,
-                                                         const uint32_t* __restrict__ start, KnnGrid g, float r2,
-                                                         float radius, int k) {
-    extern __shared__ float smem[];
-    const int t = threadIdx.x;
-    const int x = blockIdx.x * kKnnTile + (t % kKnnTile), y = blockIdx.y * kKnnTile + (t / kKnnTile);
-    if (x >= m.width || y >= m.height) return;
-    const long long i = (long long)y * m.width + x;
-    if (!(m.flags[i] & 1)) return;
-    const float px = m.position[3 * i], py = m.position[3 * i + 1], pz = m.position[3 * i + 2];
-    KnnHeap h{smem, reinterpret_cast<uint32_t*>(smem + (size_t)k * kKnnBlock), rec, t, 0, k, 0.f, 0u};
-    if (g.nx > 0) {
-        // pass 1: the cells within one cell of the lumel
-        const float h1 = g.cell;
-        // covers the rounding of px - h1 (and of g1 below), many times over
-        const float margin = (fabsf(px) + fabsf(py) + fabsf(pz) + h1) * (1.0f / (1 << 20)) + 1e-30f;
-        const int lx = cell_axis(px - h1, g.ox, g.inv, g.nx), hx = cell_axis(px + h1, g.ox, g.inv, g.nx);
-        const int ly = cell_axis(py - h1, g.oy, g.inv, g.ny), hy = cell_axis(py + h1, g.oy, g.inv, g.ny);
-        const int lz = cell_axis(pz - h1, g.oz, g.inv, g.nz), hz = cell_axis(pz + h1, g.oz, g.inv, g.nz);
-        for (int cz = lz; cz <= hz; cz++)
-            for (int cy = ly; cy <= hy; cy++) {
-                const long long row = ((long long)cz * g.ny + cy) * g.nx;
-                scan_range(h, pos, start[row + lx], start[row + hx + 1], px, py, pz, r2);
-            }
-        // cell_axis is monotone, so a record in a cell below lx lies below
-        // px - h1 as rounded (above hx: above px + h1; the same along y and
-        // z): it is farther than g1 along that axis, and its squared
-        // distance, rounded, is at least g1 * g1.
-        const float g1 = h1 - margin;
-        const float t1 = g1 > 0.f ? g1 * g1 : 0.f;
-        const bool done = t1 > r2 || (h.size == k && t1 > h.top_d);
-        if (!done) {
-            // pass 2: the cells within the radius, minus those of pass 1.  A
-            // record with a rounded squared distance <= r2 lies within
-            // radius * (1 + 2^-22) along each axis, well inside h2.
-            const float h2 = radius * (1.0f + 1.0f / 65536) + 4.f * margin;
-            const int Lx = min(lx, cell_axis(px - h2, g.ox, g.inv, g.nx)), Hx = max(hx, cell_axis(px + h2, g.ox, g.inv, g.nx));
-            const int Ly = min(ly, cell_axis(py - h2, g.oy, g.inv, g.ny)), Hy = max(hy, cell_axis(py + h2, g.oy, g.inv, g.ny));
-            const int Lz = min(lz, cell_axis(pz - h2, g.oz, g.inv, g.nz)), Hz = max(hz, cell_axis(pz + h2, g.oz, g.inv, g.nz));
-            for (int cz = Lz; cz <= Hz; cz++)
-                for (int cy = Ly; cy <= Hy; cy++) {
-                    const long long row = ((long long)cz * g.ny + cy) * g.nx;
-                    if (cz >= lz && cz <= hz && cy >= ly && cy <= hy) {
-                        scan_range(h, pos, start[row + Lx], start[row + lx], px, py, pz, r2);
-                        scan_range(h, pos, start[row + hx + 1], start[row + Hx + 1], px, py, pz, r2);
-                    } else {
-                        scan_range(h, pos, start[row + Lx], start[row + Hx + 1], px, py, pz, r2);
+// 80 registers: 24 resident warps, no spills (launch bounds alone spill).
+__global__ void __maxnreg__(80) k_knn_query(rl::DevMap m, const float4* __restrict__ pos,
+                                                              const PhotonRecord* __restrict__ rec,
+                                                              const uint32_t* __restrict__ start, KnnGrid g, float r2,
+                                                              float radius, int k) {
+    __shared__ float s_d[kKnnWarps][kKnnBuf];
+    __shared__ uint32_t s_j[kKnnWarps][kKnnBuf];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int y = blockIdx.y * kKnnTile + w;
+    if (y >= m.height) return;
+    KnnWarp q{s_d[w], s_j[w], pos, rec, lane, k, 0, r2, false, 0.f, 0};
+    for (int tx = 0; tx < kKnnTile; tx++) {
+        const int x = blockIdx.x * kKnnTile + tx;
+        if (x >= m.width) break;
+        const long long i = (long long)y * m.width + x;
+        if (!(m.flags[i] & 1)) continue;
+        const float px = m.position[3 * i], py = m.position[3 * i + 1], pz = m.position[3 * i + 2];
+        q.cnt = 0;
+        q.limited = false;
+        if (g.nx > 0) {
+            // Shells of cells at growing distance: after the box of
+            // half-width hl, every record not yet seen is farther than
+            // gl = hl - margin along some axis, so its squared distance,
+            // rounded, is at least gl * gl (margin covers the rounding of
+            // px +- hl, many times over).  Stop once that bound passes the
+            // admission bound (the radius, or the k-th key once the buffer
+            // has been cut).  hmax: a record with a rounded squared distance
+            // <= r2 lies within radius * (1 + 2^-22) along each axis, well
+            // inside it.
+            const float margin =
+                (fabsf(px) + fabsf(py) + fabsf(pz) + radius + g.cell) * (1.0f / (1 << 20)) + 1e-30f;
+            const float hmax = radius * (1.0f + 1.0f / 65536) + 4.f * margin;
+            KnnBox in{1, 0, 1, 0, 1, 0};
+            for (int l = 1;; l++) {
+                float hl = g.cell * (float)l;
+                const bool last = !(hl < hmax) || l >= 4096;
+                if (last) hl = hmax;
+                const KnnBox b = box_around(g, px, py, pz, hl);
+                for (int cz = b.lz; cz <= b.hz; cz++)
+                    for (int cy = b.ly; cy <= b.hy; cy++) {
+                        const long long row = ((long long)cz * g.ny + cy) * g.nx;
+                        if (cz >= in.lz && cz <= in.hz && cy >= in.ly && cy <= in.hy) {
+                            q.scan(start[row + b.lx], start[row + in.lx], px, py, pz);
+                            q.scan(start[row + in.hx + 1], start[row + b.hx + 1], px, py, pz);
+                        } else {
+                            q.scan(start[row + b.lx], start[row + b.hx + 1], px, py, pz);
+                        }
                     }
-                }
+                if (last) break;
+                const float gl = hl - margin;
+                const float tl = gl > 0.f ? gl * gl : 0.f;
+                if (tl > (q.limited ? q.tau_d : r2)) break;
+                in = b;
+            }
         }
-    }
-    // heapsort: ascending (d2, id)
-    for (int e = h.size - 1; e > 0; e--) {
-        const float td = h.D(e);
-        const uint32_t tj = h.J(e);
-        h.D(e) = h.D(0);
-        h.J(e) = h.J(0);
-        h.sift_root(td, tj, e);
-    }
-    float sr = 0.f, sg = 0.f, sb = 0.f;
-    for (int e = 0; e < h.size; e++) {
-        const PhotonRecord& r = rec[h.J(e)];
-        sr += r.r;
-        sg += r.g;
-        sb += r.b;
-    }
-    if (h.size > 0) {
-        const float n = (float)h.size;
-        m.gathered[3 * i] = sr / n;
-        m.gathered[3 * i + 1] = sg / n;
-        m.gathered[3 * i + 2] = sb / n;
-    } else {
-        m.gathered[3 * i] = m.gathered[3 * i + 1] = m.gathered[3 * i + 2] = 0.f;
+        // the k nearest (all, when there are no more than k), summed in
+        // fixed point: exact, so the order of the terms does not matter
+        __syncwarp();
+        uint32_t bits[kKnnPer], jj[kKnnPer];
+        bool sel[kKnnPer];
+        q.load(bits, jj);
+        const int n = q.cnt;
+        if (n > k) {
+            float td;
+            uint64_t ti;
+            warp_select(bits, jj, k, rec, sel, &td, &ti);
+        } else {
+#pragma unroll
+            for (int e = 0; e < kKnnPer; e++) sel[e] = bits[e] != kNoEntry;
+        }
+        long long sr = 0, sg = 0, sb = 0;
+#pragma unroll
+        for (int e = 0; e < kKnnPer; e++)
+            if (sel[e]) {
+                const PhotonRecord& r = rec[jj[e]];
+                sr += fixed(r.r, g.scale);
+                sg += fixed(r.g, g.scale);
+                sb += fixed(r.b, g.scale);
+            }
+        sr = warp_sum64(sr);
+        sg = warp_sum64(sg);
+        sb = warp_sum64(sb);
+        if (lane == 0) {
+            const int c = min(n, k);
+            float* out = m.gathered + 3 * i;
+            if (c > 0) {
+                const double dc = (double)c;
+                out[0] = __double2float_rn(__ll2double_rn(sr) * g.unscale / dc);
+                out[1] = __double2float_rn(__ll2double_rn(sg) * g.unscale / dc);
+                out[2] = __double2float_rn(__ll2double_rn(sb) * g.unscale / dc);
+            } else {
+                out[0] = out[1] = out[2] = 0.f;
+            }
+        }
+        __syncwarp();
     }
 }
 
@@ -559,14 +677,8 @@ extern "C" int rl_photonmap_gather_knn(rl_map* map, int slot, rl_photons* p, int
                                                            p->sorted, p->pos);
         k_knn_start<<<grid_blocks(cells + 1, 256), 256, 0, st>>>(p->keys_out, n, (uint32_t)cells, p->start);
     }
-    const size_t smem = (size_t)k * kKnnBlock * 8;
-    static bool attr = false;
-    if (!attr) {
-        KCK(cudaFuncSetAttribute(k_knn_query, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxK * kKnnBlock * 8));
-        attr = true;
-    }
     const dim3 grid((unsigned)((m->width + kKnnTile - 1) / kKnnTile), (unsigned)((m->height + kKnnTile - 1) / kKnnTile));
-    k_knn_query<<<grid, kKnnBlock, smem, st>>>(*m, p->pos, p->sorted, p->start, g, radius * radius, radius, k);
+    k_knn_query<<<grid, kKnnWarps * 32, 0, st>>>(*m, p->pos, p->sorted, p->start, g, radius * radius, radius, k);
     KCK(cudaGetLastError());
     return RL_OK;
 }

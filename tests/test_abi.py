@@ -47,12 +47,12 @@ def test_tune_parameters_are_checked_without_gpu():
     changes nothing on a refusal."""
     lib = _abi.load()
     v = C.c_int()
-    assert lib.rl_tune_get(_abi.TUNE_KNN_CELL, C.byref(v)) == 0 and v.value == 32
-    for bad in (7, 129, 0, -1):
+    assert lib.rl_tune_get(_abi.TUNE_KNN_CELL, C.byref(v)) == 0 and v.value == 80
+    for bad in (7, 257, 0, -1):
         assert lib.rl_tune_set(_abi.TUNE_KNN_CELL, bad) != 0
-    assert lib.rl_tune_get(_abi.TUNE_KNN_CELL, C.byref(v)) == 0 and v.value == 32
+    assert lib.rl_tune_get(_abi.TUNE_KNN_CELL, C.byref(v)) == 0 and v.value == 80
     assert lib.rl_tune_set(_abi.TUNE_KNN_CELL, 48) == 0
     assert lib.rl_tune_get(_abi.TUNE_KNN_CELL, C.byref(v)) == 0 and v.value == 48
-    assert lib.rl_tune_set(_abi.TUNE_KNN_CELL, 32) == 0
+    assert lib.rl_tune_set(_abi.TUNE_KNN_CELL, 80) == 0
     assert lib.rl_tune_get(_abi.TUNE_KNN_CELL + 1, C.byref(v)) != 0
     assert lib.rl_tune_set(_abi.TUNE_BVH_WIDTH, 3) != 0

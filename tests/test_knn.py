@@ -2,9 +2,10 @@
 rl_photonmap_gather_knn) against the brute-force checker in
 oracle/knn_ref.py, on the deposits the GPU kept.
 
-Tolerances: the float32 checker repeats the kernel's operation order, so
-valid lumels agree bit for bit; the FP64 checker within 1e-5 relative (of
-the largest gathered value).  Lumels that are not valid keep the disc
+Tolerances: the exact checker repeats the kernel's arithmetic (float32
+distances, the fixed-point colour sum, the double-precision mean), so valid
+lumels agree bit for bit; the FP64 checker within 1e-5 relative (of the
+largest gathered value).  Lumels that are not valid keep the disc
 gather's value exactly.  The records are the photonmap's deposits: their
 number equals the stored count and their colour sum the accumulators' sum
 (float atomics in arbitrary order: 1e-5 relative).
@@ -76,7 +77,9 @@ def test_knn_final_gather_runs(cuda):
 def _planted(seed, n=20_000, slots=3, outlier=False):
     """Synthetic records: a plane, points on a 0.25 lattice (exact distance
     ties and points on cell edges), repeated positions, non-finite
-    coordinates, several slots; ids unique (photon number x16 + bounce)."""
+    coordinates and colours, a colour that sets the fixed-point scale and
+    one below its resolution, several slots; ids unique (photon number x16
+    + bounce)."""
     rng = np.random.default_rng(seed)
     xyz = rng.uniform(-5, 5, (n, 3)).astype(np.float32)
     xyz[: n // 4, 1] = 0.0
@@ -88,6 +91,9 @@ def _planted(seed, n=20_000, slots=3, outlier=False):
     if outlier:
         xyz[10] = (1.0e6, -3.0e5, 2.0e5)
     rgb = rng.uniform(0, 1, (n, 3)).astype(np.float32)
+    rgb[11, 1] = np.nan
+    rgb[12, 2] = np.inf
+    rgb[13] = (3.0, 0.0, 5e-30)
     photon = rng.permutation(n * 3)[:n].astype(np.uint32)
     depth = rng.integers(0, 16, n).astype(np.int32)
     slot = rng.integers(0, slots, n).astype(np.int32)

@@ -70,8 +70,22 @@ struct Iter {
     int kind, first, step, mesh;
 };
 
-// Thread k's lumel i under `it`, and whether it is to be baked.
+// Thread k's lumel i under `it`, and whether it is to be baked.  Kind 2 is
+// the whole map in 8x8 lumel tiles (it.first tiles per row): 64 consecutive
+// threads cover one tile and a warp an 8x4 half, so a warp's rays start
+// close together; threads past the map's edge bake nothing.
 __device__ __forceinline__ bool iter_lumel(const DevMap& m, const Iter& it, long long k, long long& i) {
+    if (it.kind == 2) {
+        const long long tile = k >> 6;
+        const int t = (int)(k & 63);
+        const int x = (int)(tile % it.first) * 8 + (t & 7), y = (int)(tile / it.first) * 8 + (t >> 3);
+        if (x >= m.width || y >= m.height) {
+            i = 0;
+            return false;
+        }
+        i = (long long)y * m.width + x;
+        return (m.flags[i] & 1) != 0;
+    }
     if (it.kind == 0) {
         i = it.first + k * it.step;
         return (m.flags[i] & 1) != 0;

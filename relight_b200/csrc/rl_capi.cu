@@ -70,7 +70,7 @@ inline cudaStream_t S(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 // are the autotuner's picks on the terrain final-gather / room AO workloads.
 // Then the BVH width, speculative traversal, and the kNN grid's cell width
 // in 64ths of the search radius (the fastest on the terrain kNN bench).
-int g_tune[7] = {24, 64, 32, 128, 2, 0, 80};
+int g_tune[7] = {24, 256, 32, 128, 2, 0, 80};
 
 inline unsigned blocks_for(long long n, int threads) { return (unsigned)((n + threads - 1) / threads); }
 

@@ -45,6 +45,13 @@ struct Node {
 
 constexpr int kBins = 32;
 constexpr int kMaxLeaf = 4;
+// SAH cost of visiting a node, in triangle tests: a split is worth
+// kTraversalCost * area(node) + area(L) * n(L) + area(R) * n(R) against
+// area(node) * n for a leaf.  Without the term every pair of triangles is
+// split into one-triangle leaves; with it (any value in 0.25..1 builds nearly
+// the same tree) the terrain tree has 77k instead of 114k nodes and the
+// final gather runs 11% faster (48.0 -> 42.8 ms).  Hits do not depend on it.
+constexpr float kTraversalCost = 1.0f;
 constexpr int kHardLeaf = 8;
 constexpr int kDepthLimit = 40;
 
@@ -112,7 +119,7 @@ struct Builder {
                 rcnt += bc[k];
                 int lc = left_count[k - 1];
                 if (lc == 0 || rcnt == 0) continue;
-                float cost = left_area[k - 1] * lc + racc.area() * rcnt;
+                float cost = kTraversalCost * bx.area() + left_area[k - 1] * lc + racc.area() * rcnt;
                 if (cost < best_cost) {
                     best_cost = cost;
                     best_axis = ax;

@@ -586,6 +586,309 @@ def serve_arm(args):
     }
 
 
+ROOM_METRIC = "lightmap texels/s (room: direct light from a point, a spot and a 16-sample area light + AO 64 spp, 256^2)"
+ROOM_AO_BYTES_PER_RAY = 633.0  # room AO rays on the canonical SAH tree: 17.7 box + 0.39 triangle tests (oracle/ray_bytes.py)
+
+
+def _timed_steps(stream, steps, step, flush):
+    """Device time of each of `steps` calls of step(i), L2 flushed before each."""
+    import torch
+    ms = []
+    for i in range(steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step(i)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    return ms
+
+
+def room_cpu_baseline(w, budget_s=15.0, nthreads=None):
+    """Relight's own direct light + AO (oracle/_ref/librelight_ref_fast.so,
+    project CPU BVH in place of Embree) over every k-th lumel on all host
+    threads, scaled by k."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_bind as ob
+    if not os.path.exists(ob.REF_FAST_LIB):
+        return None
+    nthreads = nthreads or os.cpu_count() or 1
+    ref = ob.RefScene(w.scene, fast=True)
+    L = ref.lib
+    L.ref_set_rand(0, 1)
+    lm = ref.lumels(w.lightmap)
+    valid = int((lm.flags & 1).sum())
+    npix = w.lightmap.width * w.lightmap.height
+    zero = np.zeros(3, np.float32)
+    ao = w.ao
+
+    def run(div):
+        t0 = time.perf_counter()
+        L.ref_bake_sampled(ref.h, 0, ref.mesh(w.mesh), nthreads, div, 0, 0.8, 1.0, 1.0, 1, 1.0, 1, ob.ptr(zero), ob.ptr(zero))
+        L.ref_bake_sampled(ref.h, 1, ref.mesh(w.mesh), nthreads, div, ao.samples, ao.occluded_fraction, ao.max_distance,
+                           ao.exponent, 1, 1.0, 1, ob.ptr(zero), ob.ptr(zero))
+        return time.perf_counter() - t0
+
+    probe_div = 256
+    per_lumel = run(probe_div) / max(npix / probe_div, 1)
+    div = int(max(1, min(4096, per_lumel * npix / budget_s)))
+    step_s = run(div) * div
+    return {"value": valid / step_s, "unit": UNIT, "cores": nthreads, "kind": "reference",
+            "sample": (f"reference C++ (Embree unavailable: project CPU BVH): Relight::bakeDirectLight + "
+                       f"bakeAmbientOcclusion on every {div}th lumel over {nthreads} threads (x{div})"),
+            "est_step_s": step_s}
+
+
+def room_arm(args):
+    """BASELINE config 1 on one GPU: the closed 10^3 room with 8 boxes (108
+    triangles), one 256^2 lightmap, direct light from a point light, a 45
+    degree spot and a 1x1 area light sampled at its 16 triangle centroids,
+    then AO with 64 hemisphere rays of length 2."""
+    import torch
+    from relight_b200 import _abi, scenes
+    from relight_b200.device import Relight
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.current_stream(dev)
+    sh = stream.cuda_stream
+    w = scenes.room_scene()
+    rl = Relight(stream=sh, seed=1000)
+    ds = rl.device_scene(w.scene)
+    torch.cuda.synchronize()
+    lmap = w.lightmap._device
+    L = _abi.lib()
+    f = w.scene.flat
+    lights = C.c_void_p(f.lights.ctypes.data)
+    lverts = C.c_void_p(f.light_vertices.ctypes.data)
+    nlv = int(sum(int(l["vertex_count"]) for l in f.lights))
+    shadow_per_lumel = int(sum(max(1, int(l["vertex_count"])) for l in f.lights))
+    ao = w.ao
+    valid = lmap.valid_count()
+    ev = lambda: torch.cuda.Event(enable_timing=True)
+    ao_ms = []
+
+    def step(i, timed=False):
+        _abi.check(L.rl_map_clear(lmap.handle, 1, 0, sh))
+        _abi.check(L.rl_bake_direct(ds.handle, lmap.handle, lights, len(f.lights), lverts, nlv, None, sh))
+        a0, a1 = ev(), ev()
+        a0.record(stream)
+        _abi.check(L.rl_bake_ao(ds.handle, lmap.handle, ao.samples, ao.occluded_fraction, ao.max_distance,
+                                ao.exponent, 7 + 2 * i, None, sh))
+        a1.record(stream)
+        if timed:
+            ao_ms.append((a0, a1))
+
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize()
+    with ClockSampler(0) as clocks:
+        step_ms = _timed_steps(stream, args.steps, lambda i: step(100 + i, True), flush)
+    ao_avg_ms = sum(a.elapsed_time(b) for a, b in ao_ms) / len(ao_ms)
+    total_ms = sum(step_ms)
+    value = valid * args.steps / (total_ms / 1e3)
+
+    host = lmap.download(sh, fields=("flags", "position", "normal"))
+    pin = {k: torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for k, a in host.items()}
+    out_color = torch.empty((lmap.width * lmap.height, 3), dtype=torch.float32).pin_memory()
+    h2d = sum(t.numel() * t.element_size() for t in pin.values())
+    d2h = out_color.numel() * 4
+
+    def e2e_step(i):
+        _abi.check(L.rl_map_upload(lmap.handle, C.c_void_p(pin["flags"].data_ptr()), None,
+                                   C.c_void_p(pin["position"].data_ptr()), C.c_void_p(pin["normal"].data_ptr()),
+                                   None, None, None, sh))
+        step(300 + i)
+        _abi.check(L.rl_map_download(lmap.handle, None, None, None, None, C.c_void_p(out_color.data_ptr()), None,
+                                     None, sh))
+
+    e2e_step(0)
+    torch.cuda.synchronize()
+    e2e_ms = _timed_steps(stream, args.steps, lambda i: e2e_step(1 + i), flush)
+    e2e_value = valid * args.steps / (sum(e2e_ms) / 1e3)
+
+    peak, peak_kind = load_peaks()
+    l2 = C.c_double()
+    _abi.check(L.rl_measure_read_bandwidth(48 << 20, 50, C.byref(l2)))
+    ao_rays = valid * ao.samples
+    achieved = ao_rays * ROOM_AO_BYTES_PER_RAY / (ao_avg_ms / 1e3) / 1e9
+    result = {
+        "metric": ROOM_METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded room, BASELINE config 1 shapes)",
+        "config": {"workload": "room 10^3 + 8 boxes (108 tris), 256^2 lightmap, point + 45 deg spot + area "
+                               "(16 samples) lights, AO 64 spp r2", "valid_texels": valid,
+                   "shadow_rays_per_lumel_max": shadow_per_lumel, "ao_samples": ao.samples,
+                   "l2": "flushed between steps (256 MiB write)"},
+        "ao_ms": ao_avg_ms, "direct_ms": total_ms / args.steps - ao_avg_ms,
+        "ao_grays_per_s": ao_rays / (ao_avg_ms / 1e3) / 1e9,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "ms_per_step": sum(e2e_ms) / args.steps},
+        "roofline": {"kernel": "k_ao (AO 64 spp)", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+                     "bytes_per_ray": ROOM_AO_BYTES_PER_RAY, "l2_read_gbs_measured": l2.value,
+                     "note": "the 108-triangle tree is L1-resident: the kernel is bound by issue, not memory"},
+        "gpu_launches": 3 * args.steps,
+        "clocks": clocks.summary(),
+    }
+    if not args.no_cpu_baseline:
+        cb = room_cpu_baseline(w)
+        if cb:
+            result["cpu_baseline"] = cb
+    return result
+
+
+RAD_METRIC = "form-factor Grays/s (16,384 patches x 512 cosine rays) + 50 Jacobi gather iterations"
+
+
+def radiosity_arm(args):
+    """BASELINE config 3 on one GPU: a 10 x 5 x 10 room whose 128^2
+    radiancemap texels are 16,384 patches; form factors from 512
+    cosine-distributed rays per patch (rl_ff_hemisphere), then 50 fp32 Jacobi
+    iterations of B = E + rho F B (rl_radiosity_solve), checked against the
+    same iterations and the converged solve in float64."""
+    import torch
+    import scipy.sparse as sp
+    from relight_b200 import _abi, scenes
+    from relight_b200.device import Relight
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.current_stream(dev)
+    sh = stream.cuda_stream
+    rays, maxd, iters = 512, 100.0, 50
+    w = scenes.radiosity_room(size=128)
+    rl = Relight(stream=sh, seed=1000)
+    ds = rl.device_scene(w.scene)
+    torch.cuda.synchronize()
+    g = w.radiancemap._device.download(sh, fields=("flags", "position", "normal"))
+    valid = np.nonzero(g["flags"] & 1)[0]
+    n = len(valid)
+    pos = np.ascontiguousarray(g["position"][valid], np.float32)
+    nrm = np.ascontiguousarray(g["normal"][valid], np.float32)
+    W, H = w.radiancemap.width, w.radiancemap.height
+    pot = np.full(W * H, -1, np.int32)
+    pot[valid] = np.arange(n, dtype=np.int32)
+    mesh_map, dims, base = np.array([0], np.int32), np.array([[W, H]], np.int32), np.array([0], np.int64)
+    rng = np.random.default_rng(w.albedo_seed)
+    rho = rng.uniform(0.3, 0.9, (n, 3)).astype(np.float32)
+    E = np.zeros((n, 3), np.float32)
+    E[rng.choice(n, 16, replace=False)] = 1.0
+    L = _abi.lib()
+    cap = n * rays
+    pin_pos = torch.from_numpy(pos).pin_memory()
+    pin_nrm = torch.from_numpy(nrm).pin_memory()
+    pin_E = torch.from_numpy(E).pin_memory()
+    pin_rho = torch.from_numpy(rho).pin_memory()
+    out_B = torch.empty((n, 3), dtype=torch.float32).pin_memory()
+    dpos = torch.empty((n, 3), dtype=torch.float32, device=dev)
+    dnrm = torch.empty_like(dpos)
+    dE = torch.empty_like(dpos)
+    drho = torch.empty_like(dpos)
+    dB = torch.empty_like(dpos)
+    drow = torch.empty(n + 1, dtype=torch.int64, device=dev)
+    dcols = torch.empty(cap, dtype=torch.int32, device=dev)
+    dvals = torch.empty(cap, dtype=torch.float32, device=dev)
+    nnz = C.c_int64()
+    ev = lambda: torch.cuda.Event(enable_timing=True)
+    parts = {"ff": [], "solve": []}
+
+    def upload():
+        dpos.copy_(pin_pos, non_blocking=True)
+        dnrm.copy_(pin_nrm, non_blocking=True)
+        dE.copy_(pin_E, non_blocking=True)
+        drho.copy_(pin_rho, non_blocking=True)
+
+    def step(i, timed=False):
+        """Form factors into device memory (rl_ff_hemisphere_device), then 50 iterations."""
+        f0, f1, s0, s1 = ev(), ev(), ev(), ev()
+        f0.record(stream)
+        _abi.check(L.rl_ff_hemisphere_device(ds.handle, n, C.c_void_p(dpos.data_ptr()), C.c_void_p(dnrm.data_ptr()),
+                                             rays, maxd, 11 + i, C.c_void_p(mesh_map.ctypes.data), 1,
+                                             C.c_void_p(dims.ctypes.data), C.c_void_p(base.ctypes.data),
+                                             C.c_void_p(pot.ctypes.data), pot.size, C.c_void_p(drow.data_ptr()),
+                                             C.c_void_p(dcols.data_ptr()), C.c_void_p(dvals.data_ptr()), cap,
+                                             C.byref(nnz), sh))
+        f1.record(stream)
+        s0.record(stream)
+        _abi.check(L.rl_radiosity_solve(n, C.c_void_p(drow.data_ptr()), C.c_void_p(dcols.data_ptr()),
+                                        C.c_void_p(dvals.data_ptr()), C.c_void_p(dE.data_ptr()),
+                                        C.c_void_p(drho.data_ptr()), iters, C.c_void_p(dB.data_ptr()), sh))
+        s1.record(stream)
+        if timed:
+            parts["ff"].append((f0, f1))
+            parts["solve"].append((s0, s1))
+
+    def e2e_step(i):
+        """Patches, E and rho up from pinned host memory, the step, B down."""
+        upload()
+        step(i)
+        out_B.copy_(dB, non_blocking=True)
+
+    upload()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize()
+    with ClockSampler(0) as clocks:
+        step_ms = _timed_steps(stream, args.steps, lambda i: step(100 + i, True), flush)
+    ff_ms = sum(a.elapsed_time(b) for a, b in parts["ff"]) / args.steps
+    solve_ms = sum(a.elapsed_time(b) for a, b in parts["solve"]) / args.steps
+    e2e_step(0)
+    torch.cuda.synchronize()
+    e2e_ms = _timed_steps(stream, args.steps, lambda i: e2e_step(200 + i), flush)
+    k = nnz.value
+    # float64 checks on the last step's matrix
+    F = sp.csr_matrix((dvals[:k].cpu().numpy().astype(np.float64), dcols[:k].cpu().numpy(), drow.cpu().numpy()),
+                      shape=(n, n))
+    E64, rho64 = E.astype(np.float64), rho.astype(np.float64)
+    B64 = E64.copy()
+    for _ in range(iters):
+        B64 = E64 + rho64 * (F @ B64)
+    Bc = B64.copy()
+    conv_iters = iters
+    for conv_iters in range(iters + 1, 20000):
+        Bn = E64 + rho64 * (F @ Bc)
+        if np.abs(Bn - Bc).max() <= 1e-13 * np.abs(Bn).max():
+            Bc = Bn
+            break
+        Bc = Bn
+    B32 = dB.cpu().numpy().astype(np.float64)
+    scale = np.abs(B64).max()
+    peak, peak_kind = load_peaks()
+    l2 = C.c_double()
+    _abi.check(L.rl_measure_read_bandwidth(48 << 20, 50, C.byref(l2)))
+    jac_bytes = iters * (8.0 * k + 44.0 * n)
+    achieved = jac_bytes / (solve_ms / 1e3) / 1e9
+    h2d = 4 * n * 12
+    d2h = 12 * n
+    value = n * rays / (ff_ms / 1e3) / 1e9
+    e2e_value = n * rays * args.steps / (sum(e2e_ms) / 1e3) / 1e9
+    result = {
+        "metric": RAD_METRIC, "value": value, "unit": "Grays/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": sum(step_ms) / args.steps, "higher_is_better": True,
+        "step_grays_per_s": n * rays * args.steps / (sum(step_ms) / 1e3) / 1e9,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (room of 16,384 patches, seeded albedo)",
+        "config": {"workload": "radiosity room 10x5x10, 16,384 patches, 512 cosine rays per patch, 50 Jacobi "
+                               "iterations over RGB", "patches": n, "rays_per_patch": rays, "nnz": k,
+                   "l2": "flushed between steps (256 MiB write)"},
+        "ff_ms": ff_ms, "solve_ms": solve_ms,
+        "jacobi_vs_fp64_50_iters_max_rel": float(np.abs(B32 - B64).max() / scale),
+        "jacobi_50_vs_converged_fp64_max_rel": float(np.abs(B64 - Bc).max() / np.abs(Bc).max()),
+        "converged_after_iters": conv_iters,
+        "e2e": {"value": e2e_value, "unit": "Grays/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "ms_per_step": sum(e2e_ms) / args.steps,
+                "note": "patch positions and normals, E and rho up from pinned memory; form factors and solve; B down"},
+        "roofline": {"kernel": "k_jacobi (50 iterations)", "bound": "hbm", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+                     "algorithmic_bytes": jac_bytes, "bytes_per_iteration": "8 B per nonzero + 44 B per row",
+                     "l2_read_gbs_measured": l2.value, "frac_of_l2": achieved / l2.value},
+        "gpu_launches": (3 + iters) * args.steps,  # k_ff_hemi_rays / _rle / _compact, then k_jacobi per iteration
+        "clocks": clocks.summary(),
+    }
+    return result
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -600,9 +903,11 @@ def main():
                     help="photon estimate: Relight's disc gather (default) or the k-nearest-neighbour estimate")
     ap.add_argument("--knn-cell", type=int, default=0,
                     help="kNN grid cell width in 64ths of the radius (0: the library's default)")
-    ap.add_argument("--workload", default="terrain", choices=["terrain", "batch", "serve", "denoise"],
-                    help="terrain: the photon + final-gather bake (default); batch: uneven-size batching; "
-                         "serve: the bake-serving loop with the denoiser; denoise: the denoiser at equal RMSE")
+    ap.add_argument("--workload", default="terrain",
+                    choices=["terrain", "room", "radiosity", "batch", "serve", "denoise"],
+                    help="terrain: the photon + final-gather bake (default); room: direct light + AO; radiosity: "
+                         "hemisphere form factors + Jacobi; batch: uneven-size batching; serve: the bake-serving "
+                         "loop with the denoiser; denoise: the denoiser at equal RMSE")
     args = ap.parse_args()
     global SMALL
     SMALL = args.small
@@ -614,6 +919,12 @@ def main():
         autotune.set_knn_cell(args.knn_cell)
     if args.workload == "batch":
         print(json.dumps(batch_arm(args)), flush=True)
+        return
+    if args.workload == "room":
+        print(json.dumps(room_arm(args)), flush=True)
+        return
+    if args.workload == "radiosity":
+        print(json.dumps(radiosity_arm(args)), flush=True)
         return
     if args.workload == "serve":
         print(json.dumps(serve_arm(args)), flush=True)

@@ -449,6 +449,16 @@ int rl_ff_hemisphere(const rl_scene* scene, int n, const float* d_pos, const flo
                      float max_distance, uint64_t seed, const int32_t* mesh_map, int nmaps, const int32_t* map_dims,
                      const int64_t* map_base, const int32_t* patch_of_texel, int64_t ntexels, int64_t* row_ptr,
                      int32_t* cols, float* vals, int64_t capacity, int64_t* nnz, void* stream);
+/* The same form factors with the CSR left in device memory (d_row_ptr
+   [n + 1], d_cols and d_vals of `capacity` entries), ready for
+   rl_radiosity_solve without a trip through host memory.  With d_cols NULL
+   it only reports *nnz.  The CSR is written in stream order; n * rays is
+   always enough capacity.  No reference counterpart. */
+int rl_ff_hemisphere_device(const rl_scene* scene, int n, const float* d_pos, const float* d_nrm, int rays,
+                            float max_distance, uint64_t seed, const int32_t* mesh_map, int nmaps,
+                            const int32_t* map_dims, const int64_t* map_base, const int32_t* patch_of_texel,
+                            int64_t ntexels, int64_t* d_row_ptr, int32_t* d_cols, float* d_vals, int64_t capacity,
+                            int64_t* nnz, void* stream);
 
 /* Radiosity gather iterations (RadiositySolver::solve is an empty stub,
    radiosity/RadiositySolver.cpp:34-36; the gather math is the legacy

@@ -120,6 +120,7 @@ SIGNATURES = {
     "rl_bake_indirect": (_I, [_P, _P, _P, _I, _I, _F, _P, _P, _U64, _P, _P]),
     "rl_ff_pairwise": (_I, [_P, _I, _P, _P, _F, _P, _P, _P, _I64, _P, _P]),
     "rl_ff_hemisphere": (_I, [_P, _I, _P, _P, _I, _F, _U64, _P, _I, _P, _P, _P, _I64, _P, _P, _P, _I64, _P, _P]),
+    "rl_ff_hemisphere_device": (_I, [_P, _I, _P, _P, _I, _F, _U64, _P, _I, _P, _P, _P, _I64, _P, _P, _P, _I64, _P, _P]),
     "rl_radiosity_solve": (_I, [_I, _P, _P, _P, _P, _P, _I, _P, _P]),
     "rl_radiosity_solve_noalloc": (_I, [_I, _P, _P, _P, _P, _P, _I, _P, _P]),
     "rl_radiosity_step": (_I, [_I, _I, _P, _P, _P, _P, _P, _P, _P, _P]),

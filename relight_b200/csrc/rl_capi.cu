@@ -1538,17 +1538,28 @@ __global__ void k_ff_hemi_compact(int n, int rays, const int2* runs, const long 
     }
 }
 
-extern "C" int rl_ff_hemisphere(const rl_scene* s, int n, const float* d_pos, const float* d_nrm, int rays,
-                                float maxd, uint64_t seed, const int32_t* mesh_map, int nmaps, const int32_t* map_dims,
-                                const int64_t* map_base, const int32_t* patch_of_texel, int64_t ntexels,
-                                int64_t* row_ptr, int32_t* cols, float* vals, int64_t capacity, int64_t* nnz,
-                                void* stream) {
+// Hemisphere form factors; the CSR goes to host arrays (device_out false,
+// stream synchronised on return) or to the caller's device arrays
+// (device_out true, stream-ordered; only the per-row counts come back for
+// the row offsets and the capacity check).
+static int ff_hemisphere(const rl_scene* s, int n, const float* d_pos, const float* d_nrm, int rays, float maxd,
+                         uint64_t seed, const int32_t* mesh_map, int nmaps, const int32_t* map_dims,
+                         const int64_t* map_base, const int32_t* patch_of_texel, int64_t ntexels, int64_t* row_ptr,
+                         int32_t* cols, float* vals, int64_t capacity, int64_t* nnz, void* stream, bool device_out) {
     if (!s || n < 0 || rays <= 0 || rays > 1024 || !mesh_map || !map_dims || !map_base || !patch_of_texel)
         return fail(RL_INVALID_CALL, "rl_ff_hemisphere: bad arguments (rays must be 1..1024)");
     cudaStream_t st = S(stream);
     if (n == 0) {
         if (nnz) *nnz = 0;
-        if (row_ptr) row_ptr[0] = 0;
+        if (row_ptr) {
+            if (device_out) {
+                const int64_t zero = 0;
+                CK(cudaMemcpyAsync(row_ptr, &zero, sizeof zero, cudaMemcpyHostToDevice, st));
+                CK(cudaStreamSynchronize(st));
+            } else {
+                row_ptr[0] = 0;
+            }
+        }
         return RL_OK;
     }
     for (int m = 0; m < nmaps; m++)
@@ -1596,6 +1607,12 @@ extern "C" int rl_ff_hemisphere(const rl_scene* s, int n, const float* d_pos, co
     if (!row_ptr || !vals) return fail(RL_INVALID_CALL, "rl_ff_hemisphere: row_ptr/vals missing");
     if (capacity < total_nnz) return fail(RL_CAPACITY, "rl_ff_hemisphere: capacity %lld < nnz %lld",
                                           (long long)capacity, (long long)total_nnz);
+    if (device_out) {
+        CK(cudaMemcpyAsync(row_ptr, rp.data(), 8 * ((size_t)n + 1), cudaMemcpyHostToDevice, st));
+        k_ff_hemi_compact<<<n, 128, 0, st>>>(n, rays, druns, (const long long*)row_ptr, cols, vals);
+        CK_LAUNCH("k_ff_hemi_compact");
+        return RL_OK;
+    }
     std::memcpy(row_ptr, rp.data(), sizeof(int64_t) * ((size_t)n + 1));
     rc = scratch(s8, &drow, (size_t)n + 1, st);
     if (rc) return rc;
@@ -1614,27 +1631,75 @@ extern "C" int rl_ff_hemisphere(const rl_scene* s, int n, const float* d_pos, co
     return RL_OK;
 }
 
+extern "C" int rl_ff_hemisphere(const rl_scene* s, int n, const float* d_pos, const float* d_nrm, int rays,
+                                float maxd, uint64_t seed, const int32_t* mesh_map, int nmaps, const int32_t* map_dims,
+                                const int64_t* map_base, const int32_t* patch_of_texel, int64_t ntexels,
+                                int64_t* row_ptr, int32_t* cols, float* vals, int64_t capacity, int64_t* nnz,
+                                void* stream) {
+    return ff_hemisphere(s, n, d_pos, d_nrm, rays, maxd, seed, mesh_map, nmaps, map_dims, map_base, patch_of_texel,
+                         ntexels, row_ptr, cols, vals, capacity, nnz, stream, false);
+}
+
+extern "C" int rl_ff_hemisphere_device(const rl_scene* s, int n, const float* d_pos, const float* d_nrm, int rays,
+                                       float maxd, uint64_t seed, const int32_t* mesh_map, int nmaps,
+                                       const int32_t* map_dims, const int64_t* map_base, const int32_t* patch_of_texel,
+                                       int64_t ntexels, int64_t* d_row_ptr, int32_t* d_cols, float* d_vals,
+                                       int64_t capacity, int64_t* nnz, void* stream) {
+    return ff_hemisphere(s, n, d_pos, d_nrm, rays, maxd, seed, mesh_map, nmaps, map_dims, map_base, patch_of_texel,
+                         ntexels, d_row_ptr, d_cols, d_vals, capacity, nnz, stream, true);
+}
+
+// sum_k F_ik B_k (RGB) over row i's nonzeros [b, e), by one warp: four
+// 32-wide chunks in flight (their columns, then their B gathers), each into
+// its own partial sums, so a row costs two memory latencies per four chunks
+// rather than per chunk.  The result is reduced across the warp.
+__device__ __forceinline__ void row_dot3(int64_t b, int64_t e, int lane, const int32_t* __restrict__ cols,
+                                         const float* __restrict__ vals, const float* __restrict__ B, float& r0,
+                                         float& r1, float& r2) {
+    float s[4][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
+    int64_t k = b + lane;
+    for (; k + 96 < e; k += 128) {
+        int c[4];
+        float w[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            c[u] = __ldg(cols + k + 32 * u);
+            w[u] = __ldg(vals + k + 32 * u);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const float* x = B + 3 * (size_t)c[u];
+            s[u][0] = __fmaf_rn(w[u], __ldg(x), s[u][0]);
+            s[u][1] = __fmaf_rn(w[u], __ldg(x + 1), s[u][1]);
+            s[u][2] = __fmaf_rn(w[u], __ldg(x + 2), s[u][2]);
+        }
+    }
+    for (; k < e; k += 32) {
+        const float w = __ldg(vals + k);
+        const float* x = B + 3 * (size_t)__ldg(cols + k);
+        s[0][0] = __fmaf_rn(w, __ldg(x), s[0][0]);
+        s[0][1] = __fmaf_rn(w, __ldg(x + 1), s[0][1]);
+        s[0][2] = __fmaf_rn(w, __ldg(x + 2), s[0][2]);
+    }
+    r0 = (s[0][0] + s[1][0]) + (s[2][0] + s[3][0]);
+    r1 = (s[0][1] + s[1][1]) + (s[2][1] + s[3][1]);
+    r2 = (s[0][2] + s[1][2]) + (s[2][2] + s[3][2]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        r0 += __shfl_xor_sync(0xffffffffu, r0, o);
+        r1 += __shfl_xor_sync(0xffffffffu, r1, o);
+        r2 += __shfl_xor_sync(0xffffffffu, r2, o);
+    }
+}
+
 // One warp per patch row: B'_i = E_i + rho_i * sum_k F_ik B_k (RGB).
 __global__ void k_jacobi(int n, const int64_t* row_ptr, const int32_t* cols, const float* vals, const float* E,
                          const float* rho, const float* B, float* Bn) {
     int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     int lane = threadIdx.x & 31;
     if (warp >= n) return;
-    int64_t b = row_ptr[warp], e = row_ptr[warp + 1];
-    float s0 = 0.f, s1 = 0.f, s2 = 0.f;
-    for (int64_t k = b + lane; k < e; k += 32) {
-        float w = vals[k];
-        const float* x = B + 3 * (size_t)cols[k];
-        s0 = __fmaf_rn(w, x[0], s0);
-        s1 = __fmaf_rn(w, x[1], s1);
-        s2 = __fmaf_rn(w, x[2], s2);
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        s0 += __shfl_xor_sync(0xffffffffu, s0, o);
-        s1 += __shfl_xor_sync(0xffffffffu, s1, o);
-        s2 += __shfl_xor_sync(0xffffffffu, s2, o);
-    }
+    float s0, s1, s2;
+    row_dot3(row_ptr[warp], row_ptr[warp + 1], lane, cols, vals, B, s0, s1, s2);
     if (lane == 0) {
         size_t i = 3 * (size_t)warp;
         Bn[i] = __fmaf_rn(rho[i], s0, E[i]);
@@ -1650,21 +1715,8 @@ __global__ void k_jacobi_rows(int row_begin, int row_end, const int64_t* row_ptr
     int lane = threadIdx.x & 31;
     int row = row_begin + warp;
     if (row >= row_end) return;
-    int64_t b = row_ptr[row], e = row_ptr[row + 1];
-    float s0 = 0.f, s1 = 0.f, s2 = 0.f;
-    for (int64_t k = b + lane; k < e; k += 32) {
-        float w = vals[k];
-        const float* x = B + 3 * (size_t)cols[k];
-        s0 = __fmaf_rn(w, x[0], s0);
-        s1 = __fmaf_rn(w, x[1], s1);
-        s2 = __fmaf_rn(w, x[2], s2);
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        s0 += __shfl_xor_sync(0xffffffffu, s0, o);
-        s1 += __shfl_xor_sync(0xffffffffu, s1, o);
-        s2 += __shfl_xor_sync(0xffffffffu, s2, o);
-    }
+    float s0, s1, s2;
+    row_dot3(row_ptr[row], row_ptr[row + 1], lane, cols, vals, B, s0, s1, s2);
     if (lane == 0) {
         size_t i = 3 * (size_t)row;
         Bn[i] = __fmaf_rn(rho[i], s0, E[i]);

@@ -270,6 +270,41 @@ def test_hemisphere_form_factors_bit_exact(cuda):
     assert np.array_equal(row, r2) and np.array_equal(cols, c2) and np.array_equal(vals, v2)
 
 
+def test_hemisphere_form_factors_device_output(cuda):
+    """rl_ff_hemisphere_device leaves the same CSR in device memory that
+    rl_ff_hemisphere copies to the host, and reports nnz alone without d_cols."""
+    import torch
+    from relight_b200 import _abi
+    w, rl, valid, pos, nrm = _radiosity_inputs(32)
+    ds = rl.device_scene(w.scene)
+    tabs = _patch_tables(w, valid)
+    row, cols, vals = _ff_hemi_gpu(ds, pos, nrm, 64, 100.0, 9, tabs)
+    mesh_map, dims, base, pot = tabs
+    n = pos.shape[0]
+    dp, dn = _dev(pos, torch), _dev(nrm, torch)
+    args = (mesh_map.ctypes.data, len(dims), dims.ctypes.data, base.ctypes.data, pot.ctypes.data, pot.size)
+    nnz = C.c_int64()
+    _abi.check(_abi.lib().rl_ff_hemisphere_device(ds.handle, n, dp.data_ptr(), dn.data_ptr(), 64, 100.0, 9, *args,
+                                                  None, None, None, 0, C.byref(nnz), None))
+    assert nnz.value == len(cols)
+    cap = n * 64
+    drow = torch.zeros(n + 1, dtype=torch.int64, device="cuda")
+    dcols = torch.zeros(cap, dtype=torch.int32, device="cuda")
+    dvals = torch.zeros(cap, dtype=torch.float32, device="cuda")
+    _abi.check(_abi.lib().rl_ff_hemisphere_device(ds.handle, n, dp.data_ptr(), dn.data_ptr(), 64, 100.0, 9, *args,
+                                                  drow.data_ptr(), dcols.data_ptr(), dvals.data_ptr(), cap,
+                                                  C.byref(nnz), None))
+    torch.cuda.synchronize()
+    k = nnz.value
+    assert np.array_equal(drow.cpu().numpy(), row)
+    assert np.array_equal(dcols[:k].cpu().numpy(), cols)
+    assert np.array_equal(dvals[:k].cpu().numpy().view(np.uint32), vals.view(np.uint32))
+    rc = _abi.lib().rl_ff_hemisphere_device(ds.handle, n, dp.data_ptr(), dn.data_ptr(), 64, 100.0, 9, *args,
+                                            drow.data_ptr(), dcols.data_ptr(), dvals.data_ptr(), k - 1,
+                                            C.byref(nnz), None)
+    assert rc == _abi.RL_CAPACITY and nnz.value == k
+
+
 def test_radiosity_jacobi_vs_fp64(cuda):
     import torch
     from relight_b200 import _abi

@@ -1649,10 +1649,24 @@ extern "C" int rl_ff_hemisphere_device(const rl_scene* s, int n, const float* d_
                          ntexels, d_row_ptr, d_cols, d_vals, capacity, nnz, stream, true);
 }
 
+// B_k of one patch: three floats ([n][3], kB = 0) or a float4 whose w is
+// unused ([n][4], one 16-byte gather, kB = 1).
+template <int kB>
+__device__ __forceinline__ float3 patch_b(const float* __restrict__ B, int c) {
+    if (kB == 1) {
+        const float4 v = __ldg(reinterpret_cast<const float4*>(B) + c);
+        return make_float3(v.x, v.y, v.z);
+    }
+    const float* x = B + 3 * (size_t)c;
+    return make_float3(__ldg(x), __ldg(x + 1), __ldg(x + 2));
+}
+
 // sum_k F_ik B_k (RGB) over row i's nonzeros [b, e), by one warp: four
 // 32-wide chunks in flight (their columns, then their B gathers), each into
 // its own partial sums, so a row costs two memory latencies per four chunks
-// rather than per chunk.  The result is reduced across the warp.
+// rather than per chunk.  The result is reduced across the warp.  Both B
+// layouts load the same values, so they give the same bits.
+template <int kB>
 __device__ __forceinline__ void row_dot3(int64_t b, int64_t e, int lane, const int32_t* __restrict__ cols,
                                          const float* __restrict__ vals, const float* __restrict__ B, float& r0,
                                          float& r1, float& r2) {
@@ -1668,18 +1682,18 @@ __device__ __forceinline__ void row_dot3(int64_t b, int64_t e, int lane, const i
         }
 #pragma unroll
         for (int u = 0; u < 4; u++) {
-            const float* x = B + 3 * (size_t)c[u];
-            s[u][0] = __fmaf_rn(w[u], __ldg(x), s[u][0]);
-            s[u][1] = __fmaf_rn(w[u], __ldg(x + 1), s[u][1]);
-            s[u][2] = __fmaf_rn(w[u], __ldg(x + 2), s[u][2]);
+            const float3 x = patch_b<kB>(B, c[u]);
+            s[u][0] = __fmaf_rn(w[u], x.x, s[u][0]);
+            s[u][1] = __fmaf_rn(w[u], x.y, s[u][1]);
+            s[u][2] = __fmaf_rn(w[u], x.z, s[u][2]);
         }
     }
     for (; k < e; k += 32) {
         const float w = __ldg(vals + k);
-        const float* x = B + 3 * (size_t)__ldg(cols + k);
-        s[0][0] = __fmaf_rn(w, __ldg(x), s[0][0]);
-        s[0][1] = __fmaf_rn(w, __ldg(x + 1), s[0][1]);
-        s[0][2] = __fmaf_rn(w, __ldg(x + 2), s[0][2]);
+        const float3 x = patch_b<kB>(B, __ldg(cols + k));
+        s[0][0] = __fmaf_rn(w, x.x, s[0][0]);
+        s[0][1] = __fmaf_rn(w, x.y, s[0][1]);
+        s[0][2] = __fmaf_rn(w, x.z, s[0][2]);
     }
     r0 = (s[0][0] + s[1][0]) + (s[2][0] + s[3][0]);
     r1 = (s[0][1] + s[1][1]) + (s[2][1] + s[3][1]);
@@ -1699,12 +1713,104 @@ __global__ void k_jacobi(int n, const int64_t* row_ptr, const int32_t* cols, con
     int lane = threadIdx.x & 31;
     if (warp >= n) return;
     float s0, s1, s2;
-    row_dot3(row_ptr[warp], row_ptr[warp + 1], lane, cols, vals, B, s0, s1, s2);
+    row_dot3<0>(row_ptr[warp], row_ptr[warp + 1], lane, cols, vals, B, s0, s1, s2);
     if (lane == 0) {
         size_t i = 3 * (size_t)warp;
         Bn[i] = __fmaf_rn(rho[i], s0, E[i]);
         Bn[i + 1] = __fmaf_rn(rho[i + 1], s1, E[i + 1]);
         Bn[i + 2] = __fmaf_rn(rho[i + 2], s2, E[i + 2]);
+    }
+}
+
+// Row dot with 16-byte column and weight loads: lane l takes the aligned
+// quads base + 4 l and base + 128 + 4 l, two per step (256 nonzeros per warp
+// step, about 6 KB in flight with their gathers); elements outside [b, e)
+// are loaded one by one or skipped, so no load leaves the row.  cols and
+// vals must be 16-byte aligned.
+__device__ __forceinline__ void row_dot3_quads(int64_t b, int64_t e, int lane, const int32_t* __restrict__ cols,
+                                               const float* __restrict__ vals, const float4* __restrict__ B,
+                                               float& r0, float& r1, float& r2) {
+    float s[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
+    for (int64_t base = b & ~(int64_t)3; base < e; base += 256) {
+        int c[2][4];
+        float w[2][4];
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+            const int64_t q = base + 128 * u + 4 * lane;
+            if (q >= b && q + 4 <= e) {
+                const int4 cc = __ldg(reinterpret_cast<const int4*>(cols + q));
+                const float4 ww = __ldg(reinterpret_cast<const float4*>(vals + q));
+                c[u][0] = cc.x; c[u][1] = cc.y; c[u][2] = cc.z; c[u][3] = cc.w;
+                w[u][0] = ww.x; w[u][1] = ww.y; w[u][2] = ww.z; w[u][3] = ww.w;
+            } else {
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    const int64_t k = q + j;
+                    c[u][j] = -1;
+                    w[u][j] = 0.f;
+                    if (k >= b && k < e) {
+                        c[u][j] = __ldg(cols + k);
+                        w[u][j] = __ldg(vals + k);
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 2; u++)
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+                if (c[u][j] >= 0) {
+                    const float4 x = __ldg(B + c[u][j]);
+                    s[u][0] = __fmaf_rn(w[u][j], x.x, s[u][0]);
+                    s[u][1] = __fmaf_rn(w[u][j], x.y, s[u][1]);
+                    s[u][2] = __fmaf_rn(w[u][j], x.z, s[u][2]);
+                }
+    }
+    r0 = s[0][0] + s[1][0];
+    r1 = s[0][1] + s[1][1];
+    r2 = s[0][2] + s[1][2];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        r0 += __shfl_xor_sync(0xffffffffu, r0, o);
+        r1 += __shfl_xor_sync(0xffffffffu, r1, o);
+        r2 += __shfl_xor_sync(0xffffffffu, r2, o);
+    }
+}
+
+// k_jacobi on [n][4] iterates (w unused): one 16-byte gather per nonzero
+// instead of three 4-byte ones; with kQuads, 16-byte column and weight
+// loads as well (the accumulation order differs, within the fp32 tolerance).
+template <bool kQuads>
+__global__ void k_jacobi4(int n, const int64_t* row_ptr, const int32_t* cols, const float* vals, const float* E,
+                          const float* rho, const float4* B, float4* Bn) {
+    int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    if (warp >= n) return;
+    float s0, s1, s2;
+    if (kQuads)
+        row_dot3_quads(row_ptr[warp], row_ptr[warp + 1], lane, cols, vals, B, s0, s1, s2);
+    else
+        row_dot3<1>(row_ptr[warp], row_ptr[warp + 1], lane, cols, vals, reinterpret_cast<const float*>(B), s0, s1,
+                    s2);
+    if (lane == 0) {
+        size_t i = 3 * (size_t)warp;
+        Bn[warp] = make_float4(__fmaf_rn(rho[i], s0, E[i]), __fmaf_rn(rho[i + 1], s1, E[i + 1]),
+                               __fmaf_rn(rho[i + 2], s2, E[i + 2]), 0.f);
+    }
+}
+
+// [n][3] <-> [n][4] (w = 0).
+__global__ void k_pack4(int n, const float* src, float4* dst) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = make_float4(src[3 * i], src[3 * i + 1], src[3 * i + 2], 0.f);
+}
+__global__ void k_unpack4(int n, const float4* src, float* dst) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        const float4 v = src[i];
+        dst[3 * i] = v.x;
+        dst[3 * i + 1] = v.y;
+        dst[3 * i + 2] = v.z;
     }
 }
 
@@ -1716,7 +1822,7 @@ __global__ void k_jacobi_rows(int row_begin, int row_end, const int64_t* row_ptr
     int row = row_begin + warp;
     if (row >= row_end) return;
     float s0, s1, s2;
-    row_dot3(row_ptr[row], row_ptr[row + 1], lane, cols, vals, B, s0, s1, s2);
+    row_dot3<0>(row_ptr[row], row_ptr[row + 1], lane, cols, vals, B, s0, s1, s2);
     if (lane == 0) {
         size_t i = 3 * (size_t)row;
         Bn[i] = __fmaf_rn(rho[i], s0, E[i]);
@@ -1743,21 +1849,30 @@ extern "C" int rl_radiosity_solve(int n, const int64_t* d_row_ptr, const int32_t
         return fail(RL_INVALID_CALL, "rl_radiosity_solve: bad arguments");
     cudaStream_t st = S(stream);
     if (n == 0) return RL_OK;
-    CK(cudaMemcpyAsync(d_B, d_E, 12 * (size_t)n, cudaMemcpyDeviceToDevice, st));
-    if (iters == 0) return RL_OK;
-    Scratch sb;
-    float* tmp = nullptr;
-    int rc = scratch(sb, &tmp, 3 * (size_t)n, st);
+    if (iters == 0) {
+        CK(cudaMemcpyAsync(d_B, d_E, 12 * (size_t)n, cudaMemcpyDeviceToDevice, st));
+        return RL_OK;
+    }
+    // iterates in [n][4] ping-pong buffers, B0 = E
+    Scratch sa, sb;
+    float4 *src = nullptr, *dst = nullptr;
+    int rc = scratch(sa, &src, (size_t)n, st);
+    if (!rc) rc = scratch(sb, &dst, (size_t)n, st);
     if (rc) return rc;
-    float* src = d_B;
-    float* dst = tmp;
+    k_pack4<<<blocks_for(n, 256), 256, 0, st>>>(n, d_E, src);
+    CK_LAUNCH("k_pack4");
     unsigned grid = blocks_for((long long)n * 32, 256);
+    const bool quads = ((uintptr_t)d_cols % 16) == 0 && ((uintptr_t)d_vals % 16) == 0;
     for (int it = 0; it < iters; it++) {
-        k_jacobi<<<grid, 256, 0, st>>>(n, d_row_ptr, d_cols, d_vals, d_E, d_rho, src, dst);
-        CK_LAUNCH("k_jacobi");
+        if (quads)
+            k_jacobi4<true><<<grid, 256, 0, st>>>(n, d_row_ptr, d_cols, d_vals, d_E, d_rho, src, dst);
+        else
+            k_jacobi4<false><<<grid, 256, 0, st>>>(n, d_row_ptr, d_cols, d_vals, d_E, d_rho, src, dst);
+        CK_LAUNCH("k_jacobi4");
         std::swap(src, dst);
     }
-    if (src != d_B) CK(cudaMemcpyAsync(d_B, src, 12 * (size_t)n, cudaMemcpyDeviceToDevice, st));
+    k_unpack4<<<blocks_for(n, 256), 256, 0, st>>>(n, src, d_B);
+    CK_LAUNCH("k_unpack4");
     return RL_OK;
 }
 

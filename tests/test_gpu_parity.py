@@ -324,6 +324,41 @@ def test_radiosity_jacobi_vs_fp64(cuda):
     torch.cuda.synchronize()
     ref = jacobi_f64(row, cols, vals, E, rho, 50)
     np.testing.assert_allclose(B.cpu().numpy(), ref, rtol=1e-4, atol=1e-6)
+    # columns and weights 4 bytes past a 16-byte boundary: the scalar-load path
+    dc1 = _dev(np.concatenate([[0], cols]).astype(np.int32), torch)
+    dv1 = _dev(np.concatenate([[0], vals]).astype(np.float32), torch)
+    B1 = torch.zeros((n, 3), dtype=torch.float32, device="cuda")
+    _abi.check(_abi.lib().rl_radiosity_solve(n, dr.data_ptr(), dc1.data_ptr() + 4, dv1.data_ptr() + 4, dE.data_ptr(),
+                                             drho.data_ptr(), 50, B1.data_ptr(), None))
+    torch.cuda.synchronize()
+    np.testing.assert_allclose(B1.cpu().numpy(), ref, rtol=1e-4, atol=1e-6)
+
+
+def test_radiosity_solve_large_aligned_and_not(cuda):
+    """24,000 patches with 40 nonzeros a row: the solve's 16-byte column and
+    weight loads (aligned arrays) and its 4-byte loads (arrays 4 bytes off a
+    16-byte boundary), both within the fp32 tolerance of FP64 Jacobi."""
+    import torch
+    from relight_b200 import _abi
+    n, per_row = 24000, 40
+    rng = np.random.default_rng(21)
+    cols = np.sort(rng.integers(0, n, (n, per_row)), axis=1).astype(np.int32).reshape(-1)
+    vals = rng.random((n, per_row)).astype(np.float32)
+    vals = (vals * (np.float32(0.9) / vals.sum(1, keepdims=True, dtype=np.float32))).astype(np.float32).reshape(-1)
+    row = np.arange(n + 1, dtype=np.int64) * per_row
+    rho = rng.uniform(0.3, 0.9, (n, 3)).astype(np.float32)
+    E = np.zeros((n, 3), np.float32)
+    E[rng.choice(n, 64, replace=False)] = 1.0
+    ref = jacobi_f64(row, cols, vals, E, rho, 30)
+    dr, dE, drho = (_dev(x, torch) for x in (row, E, rho))
+    for off in (0, 1):
+        dc = _dev(np.concatenate([np.zeros(off, np.int32), cols]), torch)
+        dv = _dev(np.concatenate([np.zeros(off, np.float32), vals]), torch)
+        B = torch.zeros((n, 3), dtype=torch.float32, device="cuda")
+        _abi.check(_abi.lib().rl_radiosity_solve(n, dr.data_ptr(), dc.data_ptr() + 4 * off, dv.data_ptr() + 4 * off,
+                                                 dE.data_ptr(), drho.data_ptr(), 30, B.data_ptr(), None))
+        torch.cuda.synchronize()
+        np.testing.assert_allclose(B.cpu().numpy(), ref, rtol=1e-4, atol=1e-6)
 
 
 def test_launch_tuning_changes_no_result(cuda):

@@ -723,7 +723,7 @@ def room_arm(args):
                                "(16 samples) lights, AO 64 spp r2", "valid_texels": valid,
                    "shadow_rays_per_lumel_max": shadow_per_lumel, "ao_samples": ao.samples,
                    "l2": "flushed between steps (256 MiB write)"},
-        "ao_ms": ao_avg_ms, "direct_ms": total_ms / args.steps - ao_avg_ms,
+        "ao_ms": ao_avg_ms, "direct_ms": total_ms / steps - ao_avg_ms,
         "ao_grays_per_s": ao_rays / (ao_avg_ms / 1e3) / 1e9,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": sum(e2e_ms) / args.steps},
@@ -742,6 +742,66 @@ def room_arm(args):
 
 
 RAD_METRIC = "form-factor Grays/s (16,384 patches x 512 cosine rays) + 50 Jacobi gather iterations"
+
+
+def radiosity_pairwise(w, ds, n, pos, nrm, sh, threshold=0.1, reps=3):
+    """Relight's own form factors (RadiosityBuilder::computeFormFactors,
+    point-to-point with segment visibility, rows normalised) over the same
+    patches: rl_ff_pairwise (its count call and its fill call, CSR to host)
+    against the compiled reference on one host thread, and the two CSRs
+    compared bit for bit.  The reference's patch list is used as input when
+    it is available."""
+    import torch
+    from relight_b200 import _abi
+    L = _abi.lib()
+    out = {"patches": n, "pairs": n * (n - 1) // 2, "threshold": threshold}
+    ref_csr = None
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_bind as ob
+    if os.path.exists(ob.REF_FAST_LIB):
+        ref = ob.RefScene(w.scene, fast=True, radiancemaps=(w.radiancemap,))
+        t0 = time.perf_counter()
+        rrow, rcols, rvals, rpos, rnrm = ref.radiosity(threshold)
+        out["reference_s"] = time.perf_counter() - t0
+        out["reference_threads"] = 1
+        out["reference_patches_equal"] = bool(rpos.shape == pos.shape and np.array_equal(rpos, pos)
+                                              and np.array_equal(rnrm, nrm))
+        if rpos.shape[0] == n:
+            pos, nrm = rpos, rnrm
+            ref_csr = (rrow, rcols, rvals)
+    dp = torch.from_numpy(np.ascontiguousarray(pos, np.float32)).cuda()
+    dn = torch.from_numpy(np.ascontiguousarray(nrm, np.float32)).cuda()
+
+    def run():
+        cnt = C.c_int64()
+        _abi.check(L.rl_ff_pairwise(ds.handle, n, C.c_void_p(dp.data_ptr()), C.c_void_p(dn.data_ptr()), threshold,
+                                    None, None, None, 0, C.byref(cnt), sh))
+        k = cnt.value
+        row = np.zeros(n + 1, np.int64)
+        cols = np.zeros(max(k, 1), np.int32)
+        vals = np.zeros(max(k, 1), np.float32)
+        _abi.check(L.rl_ff_pairwise(ds.handle, n, C.c_void_p(dp.data_ptr()), C.c_void_p(dn.data_ptr()), threshold,
+                                    C.c_void_p(row.ctypes.data), C.c_void_p(cols.ctypes.data),
+                                    C.c_void_p(vals.ctypes.data), k, C.byref(cnt), sh))
+        return row, cols[:k], vals[:k]
+
+    run()
+    torch.cuda.synchronize()
+    ms = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        csr = run()
+        torch.cuda.synchronize()
+        ms.append((time.perf_counter() - t0) * 1e3)
+    out["gpu_ms"] = statistics.median(ms)
+    out["gpu_ms_covers"] = "the count call and the fill call (each sweeps all pairs), CSR to host memory"
+    out["nnz"] = int(len(csr[1]))
+    out["gpu_gpairs_per_s"] = out["pairs"] / (out["gpu_ms"] / 1e3) / 1e9
+    if ref_csr is not None:
+        out["matches_reference"] = bool(np.array_equal(csr[0], ref_csr[0]) and np.array_equal(csr[1], ref_csr[1])
+                                        and np.array_equal(csr[2].view(np.uint32), ref_csr[2].view(np.uint32)))
+        out["speedup_vs_reference"] = out["reference_s"] * 1e3 / out["gpu_ms"]
+    return out
 
 
 def radiosity_arm(args):
@@ -866,6 +926,7 @@ def radiosity_arm(args):
     _abi.check(L.rl_measure_read_bandwidth(48 << 20, 50, C.byref(l2)))
     jac_bytes = iters * (8.0 * k + 44.0 * n)
     achieved = jac_bytes / (solve_ms / 1e3) / 1e9
+    pairwise = radiosity_pairwise(w, ds, n, pos, nrm, sh)
     h2d = 4 * n * 12
     d2h = 12 * n
     value = n * rays / (ff_ms / 1e3) / 1e9
@@ -890,6 +951,7 @@ def radiosity_arm(args):
                      "algorithmic_bytes": jac_bytes, "bytes_per_iteration": "8 B per nonzero + 44 B per row",
                      "l2_read_gbs_measured": l2.value, "frac_of_l2": achieved / l2.value},
         # k_ff_hemi_rays / _rle / _compact, k_pack4, k_jacobi4 per iteration, k_unpack4
+        "pairwise_form_factors": pairwise,
         "gpu_launches": (5 + iters) * steps,
         "clocks": clocks.summary(),
     }

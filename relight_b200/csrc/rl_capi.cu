@@ -13,6 +13,8 @@
 //   radiosity gather iterations        k_jacobi
 #include <cuda_runtime.h>
 
+#include <cub/block/block_scan.cuh>
+
 #include <algorithm>
 #include <climits>
 #include <cstdarg>
@@ -1494,6 +1496,8 @@ __global__ void k_ff_hemi_rle(int rays, int pow2, const int* hits, int2* runs, i
     int* key = sh;
     int* start = sh + pow2;
     int i = blockIdx.x;
+    __shared__ int s_end;  // first empty sorted key (pow2 when every ray hit a patch)
+    if (threadIdx.x == 0) s_end = pow2;
     for (int t = threadIdx.x; t < pow2; t += blockDim.x)
         key[t] = t < rays ? (hits[(size_t)i * rays + t] < 0 ? 0x7fffffff : hits[(size_t)i * rays + t]) : 0x7fffffff;
     __syncthreads();
@@ -1509,23 +1513,32 @@ __global__ void k_ff_hemi_rle(int rays, int pow2, const int* hits, int2* runs, i
             }
             __syncthreads();
         }
-    // run starts, compacted in order by a single warp-serial pass over the
-    // sorted keys (<= 1024 entries)
-    if (threadIdx.x == 0) {
-        int nr = 0;
-        for (int t = 0; t < pow2; t++) {
-            int v = key[t];
-            if (v == 0x7fffffff) break;
-            if (t == 0 || key[t - 1] != v) start[nr++] = t;
-        }
-        int end = 0;
-        while (end < pow2 && key[end] != 0x7fffffff) end++;
-        for (int q = 0; q < nr; q++) {
-            int b = start[q], e = q + 1 < nr ? start[q + 1] : end;
-            runs[(size_t)i * rays + q] = make_int2(key[b], e - b);
-        }
-        run_count[i] = nr;
+    // Run starts (a key that differs from its predecessor), ranked by a block
+    // scan over contiguous chunks, so they land in key order; the first empty
+    // key ends the last run.
+    constexpr int kThreads = 256;  // the launch's block size
+    typedef cub::BlockScan<int, kThreads> Scan;
+    __shared__ typename Scan::TempStorage scan_tmp;
+    const int per = (pow2 + kThreads - 1) / kThreads;
+    const int t0 = threadIdx.x * per, t1 = min(t0 + per, pow2);
+    int c = 0;
+    for (int t = t0; t < t1; t++) {
+        const int v = key[t];
+        if (v != 0x7fffffff && (t == 0 || key[t - 1] != v)) c++;
+        if (v == 0x7fffffff && (t == 0 || key[t - 1] != 0x7fffffff)) s_end = t;
     }
+    int at, nr;
+    Scan(scan_tmp).ExclusiveSum(c, at, nr);
+    for (int t = t0; t < t1; t++) {
+        const int v = key[t];
+        if (v != 0x7fffffff && (t == 0 || key[t - 1] != v)) start[at++] = t;
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < nr; q += kThreads) {
+        const int b = start[q], e = q + 1 < nr ? start[q + 1] : s_end;
+        runs[(size_t)i * rays + q] = make_int2(key[b], e - b);
+    }
+    if (threadIdx.x == 0) run_count[i] = nr;
 }
 
 __global__ void k_ff_hemi_compact(int n, int rays, const int2* runs, const long long* row_ptr, int* cols, float* vals) {

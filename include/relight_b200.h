@@ -506,7 +506,9 @@ int rl_radiosity_solve_noalloc(int n, const int64_t* d_row_ptr, const int32_t* d
      RL_TUNE_SPECULATIVE: 1 = binary traversal parks leaves until the whole
                           warp has one (speculative traversal), 0 = off;
      RL_TUNE_KNN_CELL: cell width of rl_photonmap_gather_knn's grid in 64ths
-                       of its radius (8..256, default 80). */
+                       of its radius (8..256, default 80);
+     RL_TUNE_AO_SPLIT: lanes that share one lumel's AO samples (1, 2, 4 or 8;
+                       0 = chosen from the map size, the default). */
 enum {
     RL_TUNE_FG_REFILL = 0,
     RL_TUNE_FG_BLOCK = 1,
@@ -514,7 +516,8 @@ enum {
     RL_TUNE_AO_BLOCK = 3,
     RL_TUNE_BVH_WIDTH = 4,
     RL_TUNE_SPECULATIVE = 5,
-    RL_TUNE_KNN_CELL = 6
+    RL_TUNE_KNN_CELL = 6,
+    RL_TUNE_AO_SPLIT = 7
 };
 int rl_tune_set(int param, int value);
 int rl_tune_get(int param, int* value);

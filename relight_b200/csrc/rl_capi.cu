@@ -72,7 +72,7 @@ inline cudaStream_t S(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 // are the autotuner's picks on the terrain final-gather / room AO workloads.
 // Then the BVH width, speculative traversal, and the kNN grid's cell width
 // in 64ths of the search radius (the fastest on the terrain kNN bench).
-int g_tune[7] = {24, 256, 32, 128, 2, 0, 80};
+int g_tune[8] = {24, 256, 32, 128, 2, 0, 80, 0};
 
 inline unsigned blocks_for(long long n, int threads) { return (unsigned)((n + threads - 1) / threads); }
 
@@ -169,9 +169,11 @@ extern "C" int rl_tune_set(int param, int value) {
     bool width = param == RL_TUNE_BVH_WIDTH;
     bool spec = param == RL_TUNE_SPECULATIVE;
     bool cell = param == RL_TUNE_KNN_CELL;
+    bool split = param == RL_TUNE_AO_SPLIT;
     if ((refill && value >= 1 && value <= 32) || (block && (value == 64 || value == 128 || value == 256)) ||
         (width && (value == 2 || value == 4 || value == 8)) || (spec && (value == 0 || value == 1)) ||
-        (cell && value >= 8 && value <= 256))
+        (cell && value >= 8 && value <= 256) ||
+        (split && (value == 0 || value == 1 || value == 2 || value == 4 || value == 8)))
         g_tune[param] = value;
     else
         return fail(RL_INVALID_CALL, "rl_tune_set: bad parameter %d or value %d", param, value);
@@ -179,7 +181,7 @@ extern "C" int rl_tune_set(int param, int value) {
 }
 
 extern "C" int rl_tune_get(int param, int* value) {
-    if (!value || param < 0 || param > RL_TUNE_KNN_CELL) return fail(RL_INVALID_CALL, "rl_tune_get: bad parameter");
+    if (!value || param < 0 || param > RL_TUNE_AO_SPLIT) return fail(RL_INVALID_CALL, "rl_tune_get: bad parameter");
     *value = g_tune[param];
     return RL_OK;
 }
@@ -944,13 +946,13 @@ struct AoGen {
     V3 pos, nrm;
     uint2 key;
     uint32_t item;
-    int j, samples, occluded;
+    int j, stride, samples, occluded;
     float maxd;
     __device__ bool next(V3& o, V3& d, float& tnear, float& tfar) {
         if (j >= samples) return false;
         V3 dir = random_hemisphere(nrm, key, item, (uint32_t)j, kTagAO);
         segment_ray(pos, dir, maxd, o, d, tnear, tfar);
-        j++;
+        j += stride;
         return true;
     }
     __device__ void finish(const RayHit& h) {
@@ -958,20 +960,27 @@ struct AoGen {
     }
 };
 
+// `split` (a power of two, at most 8) adjacent lanes share one lumel: lane
+// part takes samples part, part + split, ...  The occlusion count is an
+// integer, so adding the lanes' counts gives the same value as one lane's
+// loop.  `count` is lumels x split, so lanes past it leave in whole groups.
 template <int kWidth>
 __global__ void __launch_bounds__(256) k_ao(DevScene s, DevMap m, int samples, float fraction, float maxd,
-                                            float exponent, uint2 key, Iter it, long long count, int refill,
-                                            int* status) {
+                                            float exponent, uint2 key, Iter it, long long count, int split,
+                                            int refill, int* status) {
     long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const unsigned live = __ballot_sync(0xffffffffu, k < count);  // whole groups of `split` lanes
     if (k >= count) return;
+    const int part = (int)(k & (split - 1));
     long long i;
-    bool valid = iter_lumel(m, it, k, i);
+    bool valid = iter_lumel(m, it, k / split, i);
     AoGen g;
     g.pos = ld3(m.position + 3 * i);
     g.nrm = ld3(m.normal + 3 * i);
     g.key = key;
     g.item = (uint32_t)i;
-    g.j = 0;
+    g.j = part;
+    g.stride = split;
     g.samples = valid ? samples : 0;
     g.occluded = 0;
     g.maxd = maxd;
@@ -979,7 +988,9 @@ __global__ void __launch_bounds__(256) k_ao(DevScene s, DevMap m, int samples, f
     else if (kWidth == 4) ray_loop4<true>(s, g, refill, status);
     else if (kWidth == 3) ray_loop_spec<true>(s, g, refill, status);
     else ray_loop<true>(s, g, refill, status);
-    if (!valid) return;
+    if (split > 1)
+        for (int o = 1; o < split; o <<= 1) g.occluded += __shfl_xor_sync(live, g.occluded, o);
+    if (!valid || part != 0) return;
     float value = 1.0f - g.occluded / (samples * fraction);
     if (fabsf(1.0f - exponent) > 0.01f) value = powf(value, exponent);
     float* col = m.color + 3 * i;
@@ -996,13 +1007,28 @@ extern "C" int rl_bake_ao(const rl_scene* s, rl_map* lm, int samples, float frac
     if (rc) return rc;
     if (count == 0) return RL_OK;
     tile_whole_map(it, count, lm->dev);
+    // Small maps leave most of the GPU idle with one lane per lumel: share
+    // each lumel's samples between up to 8 lanes while the launch stays
+    // within about two waves of resident threads (RL_TUNE_AO_SPLIT forces it).
+    int split = g_tune[RL_TUNE_AO_SPLIT];
+    if (split == 0) {
+        static int sms = 0;
+        if (sms == 0) {
+            int dev = 0;
+            CK(cudaGetDevice(&dev));
+            CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        }
+        split = 1;
+        while (split < 8 && split * 2 <= samples && count * split * 2 <= 2LL * sms * 2048) split *= 2;
+    }
     uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
     int bs = g_tune[RL_TUNE_AO_BLOCK];
     bool wide = g_tune[RL_TUNE_BVH_WIDTH] == 4 && s->dev.nodes4 != nullptr;
     bool wide8 = g_tune[RL_TUNE_BVH_WIDTH] == 8 && s->dev.nodes8 != nullptr;
     auto kern = wide8 ? k_ao<8> : wide ? k_ao<4> : (g_tune[RL_TUNE_SPECULATIVE] ? k_ao<3> : k_ao<2>);
-    kern<<<blocks_for(count, bs), bs, 0, S(stream)>>>(s->dev, lm->dev, samples, fraction, maxd, exponent, key, it,
-                                                      count, g_tune[RL_TUNE_AO_REFILL], s->d_status);
+    kern<<<blocks_for(count * split, bs), bs, 0, S(stream)>>>(s->dev, lm->dev, samples, fraction, maxd, exponent,
+                                                              key, it, count * split, split,
+                                                              g_tune[RL_TUNE_AO_REFILL], s->d_status);
     CK_LAUNCH("k_ao");
     return RL_OK;
 }
@@ -2182,6 +2208,7 @@ __global__ void __launch_bounds__(kKind == 0 ? 128 : 256, kKind == 0 ? 1 : 4) k_
             g.key = J.key;
             g.item = (uint32_t)i;
             g.j = 0;
+            g.stride = 1;
             g.samples = valid ? J.samples : 0;
             g.occluded = 0;
             g.maxd = J.maxd;

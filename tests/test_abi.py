@@ -54,5 +54,8 @@ def test_tune_parameters_are_checked_without_gpu():
     assert lib.rl_tune_set(_abi.TUNE_KNN_CELL, 48) == 0
     assert lib.rl_tune_get(_abi.TUNE_KNN_CELL, C.byref(v)) == 0 and v.value == 48
     assert lib.rl_tune_set(_abi.TUNE_KNN_CELL, 80) == 0
-    assert lib.rl_tune_get(_abi.TUNE_KNN_CELL + 1, C.byref(v)) != 0
+    assert lib.rl_tune_get(_abi.TUNE_AO_SPLIT, C.byref(v)) == 0 and v.value == 0
+    for bad in (3, 16, -1):
+        assert lib.rl_tune_set(_abi.TUNE_AO_SPLIT, bad) != 0
+    assert lib.rl_tune_get(_abi.TUNE_AO_SPLIT + 1, C.byref(v)) != 0
     assert lib.rl_tune_set(_abi.TUNE_BVH_WIDTH, 3) != 0

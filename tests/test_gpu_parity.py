@@ -395,6 +395,36 @@ def test_launch_tuning_changes_no_result(cuda):
         np.testing.assert_allclose(c, fg[0], rtol=1e-4, atol=1e-6)
 
 
+def test_ao_split_changes_no_result(cuda):
+    """Lanes sharing one lumel's AO samples (RL_TUNE_AO_SPLIT 1, 2, 4, 8 and
+    the size-based default) add integer occlusion counts: every setting bakes
+    the same bits, for a whole-map bake and for a LumelBakeIterator(1, 3) slice."""
+    import ctypes as C
+    from relight_b200 import _abi
+    from relight_b200.device import LumelBakeIterator
+    L = _abi.lib()
+    old = C.c_int()
+    _abi.check(L.rl_tune_get(_abi.TUNE_AO_SPLIT, C.byref(old)))
+    out = []
+    try:
+        for split in (1, 2, 4, 8, 0):
+            _abi.check(L.rl_tune_set(_abi.TUNE_AO_SPLIT, split))
+            got = []
+            for it in (None, LumelBakeIterator(1, 3)):
+                rl = _relight()
+                ws = scenes.room_scene(size=64)
+                rl.bake_direct_light(ws.scene, ws.mesh, None)  # AO scales the colour already there
+                rl.bake_ambient_occlusion(ws.scene, ws.mesh, None, ws.ao, iterator=it, seed=5)
+                got.append(_lumels(ws.lightmap)["color"])
+            out.append(got)
+    finally:
+        _abi.check(L.rl_tune_set(_abi.TUNE_AO_SPLIT, old.value))
+    assert (out[0][0].sum(1) > 0).sum() > 1000
+    for got in out[1:]:
+        for a, b in zip(out[0], got):
+            assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
 def test_photon_shares_sum_to_the_full_emission(cuda):
     """rl_emit_photons_range: two shares of the photon sequence, deposited into
     two photonmap replicas, sum to the unsplit emission (the multi-GPU split)."""

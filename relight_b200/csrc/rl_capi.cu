@@ -244,6 +244,26 @@ extern "C" int rl_scene_create(const rl_scene_desc* d, int builder, void* stream
     s->mesh_first_tri.assign(d->mesh_first_tri, d->mesh_first_tri + d->nmeshes + 1);
     s->mesh_photonmap = pmap;
     s->nmeshes = d->nmeshes;
+    // Per-triangle shading record for final-gather hits (64 B, one line):
+    // the three vertex normals, each with its lightmap u, then the three
+    // lightmap v and the mesh's photonmap slot (int bits).
+    std::vector<float4> shade(4 * (size_t)d->ntris);
+    {
+        const float* vn = d->nrm ? d->nrm : zeros3.data();
+        const float* vu = d->uv1 ? d->uv1 : zeros2.data();
+        for (int t = 0; t < d->ntris; t++) {
+            const int4 f = vidx[t];
+            const int vs[3] = {f.x, f.y, f.z};
+            for (int q = 0; q < 3; q++)
+                shade[4 * (size_t)t + q] = make_float4(vn[3 * (size_t)vs[q]], vn[3 * (size_t)vs[q] + 1],
+                                                       vn[3 * (size_t)vs[q] + 2], vu[2 * (size_t)vs[q]]);
+            float slot;
+            const int sl = pmap[f.w];
+            std::memcpy(&slot, &sl, 4);
+            shade[4 * (size_t)t + 3] = make_float4(vu[2 * (size_t)f.x + 1], vu[2 * (size_t)f.y + 1],
+                                                   vu[2 * (size_t)f.z + 1], slot);
+        }
+    }
 
     int rc = RL_OK;
     auto up = [&](auto** dst, const auto* src, size_t count) {
@@ -257,6 +277,7 @@ extern "C" int rl_scene_create(const rl_scene_desc* d, int builder, void* stream
     long long* tex_off = nullptr;
     unsigned char* tex_px = nullptr;
     float4* nodes4 = nullptr;
+    float4* dshade = nullptr;
     uint4* nodes8 = nullptr;
     float4* tris8 = nullptr;
     if (builder == 0) {
@@ -269,6 +290,7 @@ extern "C" int rl_scene_create(const rl_scene_desc* d, int builder, void* stream
         }
     }
     up(&dvidx, vidx.data(), vidx.size());
+    up(&dshade, shade.data(), shade.size());
     up(&pos, d->pos, 3 * (size_t)d->nverts);
     up(&nrm, d->nrm ? d->nrm : zeros3.data(), 3 * (size_t)d->nverts);
     up(&uv0, d->uv0 ? d->uv0 : zeros2.data(), 2 * (size_t)d->nverts);
@@ -317,7 +339,7 @@ extern "C" int rl_scene_create(const rl_scene_desc* d, int builder, void* stream
         return rc;
     }
     DevScene& v = s->dev;
-    v.nodes = nodes; v.nodes4 = nodes4; v.tris = tris; v.tri_vidx = dvidx;
+    v.nodes = nodes; v.nodes4 = nodes4; v.tris = tris; v.tri_vidx = dvidx; v.shade = dshade;
     v.nodes8 = nodes8; v.tris8 = tris8;
     v.pos = pos; v.nrm = nrm; v.uv0 = uv0; v.uv1 = uv1; v.vmat = dvmat;
     v.mesh_first_tri = first; v.mesh_photonmap = dpmap;
@@ -1280,13 +1302,19 @@ struct FgGen {
             gb = gb + (sky.z * influence + amb.z);
             return;
         }
-        int4 f = __ldg(s->tri_vidx + h.gid);
-        V3 hn = interp3(s->nrm, f, h.u, h.v);
+        // the hit's shading record: interp3 / interp2 on the same values
+        const float4* rec = s->shade + 4 * (size_t)h.gid;
+        const float4 ra = __ldg(rec), rb = __ldg(rec + 1), rc = __ldg(rec + 2);
+        const float bx = h.u, by = h.v;
+        V3 hn = mk3(ra.x + (rb.x - ra.x) * by + (rc.x - ra.x) * bx, ra.y + (rb.y - ra.y) * by + (rc.y - ra.y) * bx,
+                    ra.z + (rb.z - ra.z) * by + (rc.z - ra.z) * bx);
         if (dot3(dir, hn) >= 0.0f) return;
-        int slot = s->mesh_photonmap[f.w];
+        const float4 rv = __ldg(rec + 3);
+        int slot = __float_as_int(rv.w);
         if (slot >= 0 && slot < G->nmaps) {
             const DevMap& P = G->maps[slot];
-            float2 uv = interp2(s->uv1, f, h.u, h.v);
+            float2 uv = make_float2(ra.w + (rb.w - ra.w) * by + (rc.w - ra.w) * bx,
+                                    rv.x + (rv.y - rv.x) * by + (rv.z - rv.x) * bx);
             int ti = lumel_at_uv(P.width, P.height, uv);
             const float* g = P.gathered + 3 * (size_t)ti;
             gr = gr + (g[0] * influence + amb.x);

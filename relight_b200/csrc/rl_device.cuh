@@ -29,6 +29,7 @@ struct DevScene {
     const float4* nodes4;       // 4-wide nodes, 128 B: lo.x hi.x lo.y hi.y lo.z hi.z (4 children each), codes, pad
     const float4* tris;
     const int4* tri_vidx;       // per global triangle id: a, b, c, mesh
+    const float4* shade;        // per global triangle id: 4 float4, normals + lightmap uv + photonmap slot
     const uint4* nodes8;        // compressed 8-wide nodes, 80 B (rl_bvh.cpp), or null
     const float4* tris8;        // triangle records in 8-wide node order
     const float* pos;

@@ -46,10 +46,11 @@ METRIC = "lightmap texels/s (photons + gather + final gather 256 spp, 1024^2)"
 KNN_K, KNN_RADIUS = 100, 2.0
 UNIT = "texels/s"
 WORKLOAD = "terrain 256^2 verts + 2000 boxes (154,050 tris), 1M photons x3 bounces, gather r7, FG 256 spp, 1024^2"
-# DRAM bytes (read + write) of one full-size k_indirect launch, from the ncu
-# capture summarised in profiles/k_indirect_terrain_launches.md
-# (dram__bytes_read.sum 75,599,104 + dram__bytes_write.sum 4,105,984).
-FG_DRAM_TRAFFIC = 79_705_088
+L2_BYTES = 126 << 20
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one full-size
+# k_indirect launch in one ncu capture, and the build it was captured on.
+FG_DRAM_TRAFFIC = {"bytes": 79_705_088, "captured_on": "k_indirect before per-triangle shading records "
+                   "(56.0 ms launch under ncu); not re-captured on the timed build"}
 
 
 def load_peaks():
@@ -119,6 +120,16 @@ def build_workload(seed):
     return scenes.terrain_scene(seed=2)
 
 
+def terrain_config(st, valid, ntris, world, knn=False, split=False):
+    """The workload description both arms print (the same dict)."""
+    return {"workload": WORKLOAD + (f", kNN k={KNN_K} r={KNN_RADIUS}" if knn else ""),
+            "gather": "knn" if knn else "disc", "lightmap": [1024, 1024] if not SMALL else [512, 512],
+            "valid_texels": valid, "photons": int(st.photon_pass_count * 125000),
+            "fg_samples": st.final_gather_samples, "triangles": ntris,
+            "parallelism": f"one bake split x{world}" if split else f"replicas x{world}",
+            "l2": "flushed between steps (256 MiB write)"}
+
+
 def gpu_arm(args, rank, world, local_rank):
     import torch
     from relight_b200 import _abi, autotune
@@ -147,6 +158,14 @@ def gpu_arm(args, rank, world, local_rank):
     ev = lambda: torch.cuda.Event(enable_timing=True)
 
     knn = args.gather == "knn"
+    split = args.split
+    if split and knn:
+        raise SystemExit("--split runs the disc gather only")
+    if split:
+        from relight_b200 import parallel
+        # photon share, all-reduce (colour + count), gather; final gather over
+        # LumelBakeIterator(rank, world), all-reduce, add
+        launches_per_step = 3
     records = None
     if knn:
         from relight_b200.device import PhotonRecords
@@ -157,6 +176,14 @@ def gpu_arm(args, rank, world, local_rank):
     def step(seed, fg_events=None, knn_events=None):
         _abi.check(L.rl_map_clear(pmap.handle, 1, 1, sh))
         _abi.check(L.rl_map_clear(lmap.handle, 1, 0, sh))
+        if split:
+            parallel.emit_photons_distributed(rl, w.scene, st, seed)
+            if fg_events:
+                fg_events[0].record(stream)
+            parallel.bake_indirect_distributed(rl, w.scene, w.meshes[0], st, seed + 1)
+            if fg_events:
+                fg_events[1].record(stream)
+            return
         if knn:
             _abi.check(L.rl_emit_photons_records(ds.handle, maps, 1, lights, len(flat.lights), st.photon_pass_count,
                                                  st.photon_bounce_count, st.photon_energy_threshold,
@@ -210,7 +237,9 @@ def gpu_arm(args, rank, world, local_rank):
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         total_ms = float(t.item())
     ms_per_step = total_ms / args.steps
-    value = valid * args.steps * world / (total_ms / 1e3)
+    # replicas: every rank bakes the whole job; split: the ranks share one
+    jobs = 1 if split else world
+    value = valid * args.steps * jobs / (total_ms / 1e3)
 
     # e2e: host buffers through the C ABI (lumel inputs up, baked colours down)
     host = lmap.download(sh, fields=("flags", "position", "normal"))
@@ -251,36 +280,47 @@ def gpu_arm(args, rank, world, local_rank):
         t = torch.tensor([e2e_total], device=dev, dtype=torch.float64)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         e2e_total = float(t.item())
-    e2e_value = valid * args.steps * world / (e2e_total / 1e3)
+    e2e_value = valid * args.steps * jobs / (e2e_total / 1e3)
 
     peak, peak_kind = load_peaks()
     l2 = C.c_double()
     _abi.check(L.rl_measure_read_bandwidth(48 << 20, 50, C.byref(l2)))
     fg_avg_s = (sum(fg_ms) / len(fg_ms)) / 1e3
-    alg_bytes = rays_per_step * RAY_MODEL["bytes_per_ray"]
+    # split: this rank traced 1/world of the rays (its interval also holds
+    # the contribution all-reduce)
+    alg_bytes = rays_per_step / (world if split else 1) * RAY_MODEL["bytes_per_ray"]
     achieved = alg_bytes / fg_avg_s / 1e9
+    bvh = ds.bvh_stats()
+    # node + triangle records the walk reads, plus the per-triangle shading records
+    working_set = 64 * bvh["nodes"] + 48 * flat.ntris + 64 * flat.ntris
+    bound = "l2" if working_set < L2_BYTES else "hbm"
     result = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+        "scaling": "strong" if split else "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded fBm terrain + boxes)",
-        "config": {"workload": WORKLOAD + (f", kNN k={KNN_K} r={KNN_RADIUS}" if knn else ""),
-                   "gather": args.gather, "bvh_width": autotune.get_width(),
-                   **({"knn_cell_64ths": autotune.get_knn_cell()} if knn else {}), "lightmap": [lmap.width, lmap.height], "valid_texels": valid,
-                   "photons": int(st.photon_pass_count * 125000), "fg_samples": st.final_gather_samples, "triangles": flat.ntris,
-                   "parallelism": f"replicas x{world}", "l2": "flushed between steps (256 MiB write)"},
-        "grays_per_s": rays_per_step * args.steps * world / (total_ms / 1e3) / 1e9,
+        "config": terrain_config(st, valid, flat.ntris, world, knn, split),
+        "tuning": {"bvh_width": autotune.get_width(), "fg": autotune.get("indirect"),
+                   **({"knn_cell_64ths": autotune.get_knn_cell()} if knn else {})},
+        "grays_per_s": rays_per_step * args.steps * jobs / (total_ms / 1e3) / 1e9,
         "fg_ms": sum(fg_ms) / len(fg_ms),
         **({"knn_ms": sum(knn_ms) / len(knn_ms)} if knn else {}),
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": e2e_total / args.steps},
-        "roofline": {"kernel": "k_indirect (final gather)", "bound": "hbm", "achieved": achieved, "peak": peak,
-                     "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
-                     "traffic": FG_DRAM_TRAFFIC,
+        "roofline": {"kernel": "k_indirect (final gather)", "bound": bound, "achieved": achieved,
+                     "peak": l2.value if bound == "l2" else peak, "unit": "GB/s",
+                     "frac": achieved / (l2.value if bound == "l2" else peak),
+                     "peak_source": ("L2 read bandwidth measured in this run by the library's probe "
+                                     "(rl_measure_read_bandwidth: 48 MiB re-read 50 times with 16-byte loads); "
+                                     "no driver-measured L2 figure exists" if bound == "l2"
+                                     else f"{peak_kind} HBM copy bandwidth"),
+                     "working_set_bytes": working_set, "l2_bytes": L2_BYTES,
+                     "traffic": FG_DRAM_TRAFFIC["bytes"], "traffic_source": FG_DRAM_TRAFFIC["captured_on"],
                      "algorithmic_bytes_per_launch": alg_bytes, "bytes_per_ray": RAY_MODEL["bytes_per_ray"],
-                     "l2_read_gbs_measured": l2.value, "frac_of_l2": achieved / l2.value},
+                     "hbm": {"peak": peak, "source": peak_kind, "frac": achieved / peak}},
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clocks.summary(),
-        "bvh": ds.bvh_stats(),
+        "bvh": bvh,
     }
     return result, w
 
@@ -314,15 +354,16 @@ def cpu_baseline(w, budget_s=20.0, nthreads=None):
     lm = ref.lumels(w.lightmap)
     valid = int((lm.flags & 1).sum())
     npix = w.lightmap.width * w.lightmap.height
-    # size the final-gather sample to the budget: probe with a sparse sample first
-    div = 4096
+    # size the final-gather sample to the budget: probe with a sparse sample
+    # first (odd strides, so samples spread over every column)
+    div = 4095
     t0 = time.perf_counter()
     L.ref_bake_sampled(ref.h, 2, ref.mesh(w.meshes[0]), nthreads, div, 0, 0.8, 1.0, 1.0, st.final_gather_samples,
                        st.final_gather_distance, st.final_gather_radius, ob.ptr(sky), ob.ptr(amb))
     t_probe = time.perf_counter() - t0
     per_lumel = t_probe / max(npix / div, 1)
     target = max(budget_s - t_photons_gather, 2.0)
-    div2 = int(max(16, min(4096, per_lumel * npix / target)))
+    div2 = int(max(17, min(4095, per_lumel * npix / target))) | 1
     t0 = time.perf_counter()
     L.ref_bake_sampled(ref.h, 2, ref.mesh(w.meshes[0]), nthreads, div2, 0, 0.8, 1.0, 1.0, st.final_gather_samples,
                        st.final_gather_distance, st.final_gather_radius, ob.ptr(sky), ob.ptr(amb))
@@ -336,6 +377,21 @@ def cpu_baseline(w, budget_s=20.0, nthreads=None):
 
 
 def reference_arm(args, rank, world):
+    """Relight itself (oracle/_ref/librelight_ref_fast.so: the reference's
+    own sources, project CPU BVH in place of Embree) on this host's cores,
+    through its own API: Relight::emitPhotons (single-threaded, as the
+    reference is), then Relight::bakeIndirectLight over LumelBakeIterator(j,
+    threads) on one std::thread per core.
+
+      value     one full, unsampled step, timed once per run;
+      steps     K sampled steps (each: 1 of 8 photon passes, the gather, and
+                the final gather on every `div`-th lumel), the time of what
+                ran as ms_per_step, and their extrapolation (x8 photons,
+                x div final gather) beside the full step's value;
+      as_is     one sampled step with the C library's global rand() (the
+                reference as shipped, lock-contended across threads); the
+                headline uses a per-thread rand() (fair to the reference).
+    Under torchrun only rank 0 runs."""
     if rank != 0:
         return None
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -343,23 +399,88 @@ def reference_arm(args, rank, world):
     if not os.path.exists(ob.REF_FAST_LIB):
         return {"impl": "reference", "unavailable": "oracle/_ref/librelight_ref_fast.so was not built"}
     w = build_workload(0)
+    st = w.settings
+    ref = ob.RefScene(w.scene, fast=True)
+    L = ref.lib
+    nthreads = os.cpu_count() or 1
+    lm = ref.lumels(w.lightmap)
+    valid = int((lm.flags & 1).sum())
+    sky = np.asarray(st.sky_color, np.float32)
+    amb = np.asarray(st.ambient_color, np.float32)
+    pm = ref.maps[id(w.photonmap)]
+    mesh0 = ref.mesh(w.meshes[0])
+
+    def emit(passes):
+        L.ref_emit_photons(ref.h, passes, st.photon_bounce_count, st.photon_energy_threshold, st.photon_max_distance,
+                           st.final_gather_radius)
+
+    def fg(div):
+        L.ref_bake_sampled(ref.h, 2, mesh0, nthreads, div, 0, 0.8, 1.0, 1.0, st.final_gather_samples,
+                           st.final_gather_distance, st.final_gather_radius, ob.ptr(sky), ob.ptr(amb))
+
+    def sampled_step(div):
+        """Returns (wall s, extrapolated full-step s)."""
+        t0 = time.perf_counter()
+        emit(1)  # one pass, then Photonmap::gather (Relight::emitPhotons)
+        t1 = time.perf_counter()
+        L.ref_photonmap_gather(ref.h, pm, st.final_gather_radius)
+        t2 = time.perf_counter()
+        fg(div)
+        t3 = time.perf_counter()
+        t_gather = t2 - t1
+        t_pass = max((t1 - t0) - t_gather, 0.0)
+        return t3 - t0, st.photon_pass_count * t_pass + t_gather + div * (t3 - t2)
+
+    L.ref_set_rand(0, 1)
+    # Size the final-gather sample so a sampled step is about 2-3 s.  The
+    # sample is every div-th lumel; an odd div (coprime with the 1024-lumel
+    # rows) spreads it over all columns instead of a few.
+    npix = w.lightmap.width * w.lightmap.height
+    t0 = time.perf_counter()
+    fg(1023)
+    per_lumel = (time.perf_counter() - t0) / (npix / 1023)
+    div = int(max(9, min(4095, per_lumel * npix / 0.5))) | 1
     for _ in range(args.warmup):
-        cpu_baseline(w, budget_s=3.0)
-    vals = []
-    details = None
-    for _ in range(args.steps):
-        details, _err = cpu_baseline(w, budget_s=10.0)
-        vals.append(details["est_step_s"])
-    valid = int(details["value"] * details["est_step_s"])
-    total = sum(vals)
-    value = valid * args.steps / total
-    cb = dict(details)
-    cb["value"] = value
+        sampled_step(div)
+    wall, est = [], []
+    for i in range(args.steps):
+        L.ref_set_rand(0, 100 + i)
+        a, b = sampled_step(div)
+        wall.append(a)
+        est.append(b)
+    # one full, unsampled step
+    L.ref_set_rand(0, 7)
+    t0 = time.perf_counter()
+    emit(st.photon_pass_count)
+    t1 = time.perf_counter()
+    fg(1)
+    t2 = time.perf_counter()
+    full_s = t2 - t0
+    value = valid / full_s
+    extrapolated = valid / statistics.mean(est)
+    # the reference as shipped: glibc's global rand()
+    L.ref_set_rand(1, 5)
+    _, est_as_is = sampled_step(div)
+    L.ref_set_rand(0, 1)
+    sample = (f"reference C++ (Embree unavailable: project CPU BVH), {nthreads} host threads; value from one full "
+              f"unsampled step ({st.photon_pass_count} photon passes single-threaded as in Relight::emitPhotons, "
+              f"gather, final gather on all {valid} valid lumels); per-thread rand()")
     return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": total / args.steps * 1e3, "higher_is_better": True,
+            "warmup": args.warmup, "ms_per_step": statistics.mean(wall) * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded fBm terrain + boxes)",
-            "config": {"workload": WORKLOAD, "parallelism": f"{cb['cores']} host threads"},
-            "impl": "reference", "cpu_baseline": cb,
+            "config": terrain_config(st, valid, w.scene.flat.ntris, world),
+            "impl": "reference", "sampled": True,
+            "value_source": "one full, unsampled step timed once in this run",
+            "full_step": {"s": full_s, "photons_and_gather_s": t1 - t0, "fg_s": t2 - t1},
+            "sampled_steps": {"each": (f"1 of {st.photon_pass_count} photon passes, the gather, final gather on "
+                                       f"every {div}th lumel"),
+                              "scale": {"photon_passes": st.photon_pass_count, "fg_lumel_stride": div},
+                              "ms_per_step": statistics.mean(wall) * 1e3,
+                              "extrapolated_value": extrapolated,
+                              "extrapolation_error": extrapolated / value - 1.0},
+            "as_is_rand": {"value": valid / est_as_is, "unit": UNIT,
+                           "kind": "one sampled step with glibc's global rand(), extrapolated"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads, "kind": "reference", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
@@ -630,9 +751,9 @@ def room_cpu_baseline(w, budget_s=15.0, nthreads=None):
                            ao.exponent, 1, 1.0, 1, ob.ptr(zero), ob.ptr(zero))
         return time.perf_counter() - t0
 
-    probe_div = 256
+    probe_div = 255
     per_lumel = run(probe_div) / max(npix / probe_div, 1)
-    div = int(max(1, min(4096, per_lumel * npix / budget_s)))
+    div = int(max(1, min(4095, per_lumel * npix / budget_s))) | 1
     step_s = run(div) * div
     return {"value": valid / step_s, "unit": UNIT, "cores": nthreads, "kind": "reference",
             "sample": (f"reference C++ (Embree unavailable: project CPU BVH): Relight::bakeDirectLight + "
@@ -641,7 +762,7 @@ def room_cpu_baseline(w, budget_s=15.0, nthreads=None):
 
 
 def room_arm(args):
-    """BASELINE config 1 on one GPU: the closed 10^3 room with 8 boxes (108
+    """The room workload on one GPU: the closed 10^3 room with 8 boxes (108
     triangles), one 256^2 lightmap, direct light from a point light, a 45
     degree spot and a 1x1 area light sampled at its 16 triangle centroids,
     then AO with 64 hemisphere rays of length 2."""
@@ -711,14 +832,14 @@ def room_arm(args):
     e2e_value = valid * args.steps / (sum(e2e_ms) / 1e3)
 
     peak, peak_kind = load_peaks()
-    l2 = C.c_double()
-    _abi.check(L.rl_measure_read_bandwidth(48 << 20, 50, C.byref(l2)))
+    l1 = C.c_double()
+    _abi.check(L.rl_measure_l1_read_bandwidth(64 << 10, 2000, C.byref(l1)))
     ao_rays = valid * ao.samples
     achieved = ao_rays * ROOM_AO_BYTES_PER_RAY / (ao_avg_ms / 1e3) / 1e9
     result = {
         "metric": ROOM_METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": steps,
         "warmup": args.warmup, "ms_per_step": total_ms / steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded room, BASELINE config 1 shapes)",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded room)",
         "config": {"workload": "room 10^3 + 8 boxes (108 tris), 256^2 lightmap, point + 45 deg spot + area "
                                "(16 samples) lights, AO 64 spp r2", "valid_texels": valid,
                    "shadow_rays_per_lumel_max": shadow_per_lumel, "ao_samples": ao.samples,
@@ -727,10 +848,15 @@ def room_arm(args):
         "ao_grays_per_s": ao_rays / (ao_avg_ms / 1e3) / 1e9,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": sum(e2e_ms) / args.steps},
-        "roofline": {"kernel": "k_ao (AO 64 spp)", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
-                     "bytes_per_ray": ROOM_AO_BYTES_PER_RAY, "l2_read_gbs_measured": l2.value,
-                     "note": "the 108-triangle tree is L1-resident: the kernel is bound by issue, not memory"},
+        "roofline": {"kernel": "k_ao (AO 64 spp)", "bound": "l1", "achieved": achieved, "peak": l1.value,
+                     "unit": "GB/s", "frac": achieved / l1.value,
+                     "peak_source": ("L1 read bandwidth measured in this run by the library's probe "
+                                     "(rl_measure_l1_read_bandwidth: 64 KiB per block re-read 2,000 times)"),
+                     "working_set_bytes": 64 * (f.ntris - 1) + 48 * f.ntris, "traffic": None,
+                     "algorithmic_bytes_per_launch": ao_rays * ROOM_AO_BYTES_PER_RAY,
+                     "bytes_per_ray": ROOM_AO_BYTES_PER_RAY,
+                     "hbm": {"peak": peak, "source": peak_kind, "frac": achieved / peak},
+                     "note": "the 108-triangle tree stays in each SM's L1; the walk is bound by issue"},
         "gpu_launches": 3 * steps,
         "clocks": clocks.summary(),
     }
@@ -805,7 +931,7 @@ def radiosity_pairwise(w, ds, n, pos, nrm, sh, threshold=0.1, reps=3):
 
 
 def radiosity_arm(args):
-    """BASELINE config 3 on one GPU: a 10 x 5 x 10 room whose 128^2
+    """The radiosity workload on one GPU: a 10 x 5 x 10 room whose 128^2
     radiancemap texels are 16,384 patches; form factors from 512
     cosine-distributed rays per patch (rl_ff_hemisphere), then 50 fp32 Jacobi
     iterations of B = E + rho F B (rl_radiosity_solve), checked against the
@@ -925,6 +1051,9 @@ def radiosity_arm(args):
     l2 = C.c_double()
     _abi.check(L.rl_measure_read_bandwidth(48 << 20, 50, C.byref(l2)))
     jac_bytes = iters * (8.0 * k + 44.0 * n)
+    # the CSR, row offsets, E, rho and both [n][4] iterates
+    jac_set = 8 * k + 8 * (n + 1) + 24 * n + 32 * n
+    jac_bound = "l2" if jac_set < L2_BYTES else "hbm"
     achieved = jac_bytes / (solve_ms / 1e3) / 1e9
     pairwise = radiosity_pairwise(w, ds, n, pos, nrm, sh)
     h2d = 4 * n * 12
@@ -946,10 +1075,15 @@ def radiosity_arm(args):
         "e2e": {"value": e2e_value, "unit": "Grays/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": sum(e2e_ms) / steps,
                 "note": "patch positions and normals, E and rho up from pinned memory; form factors and solve; B down"},
-        "roofline": {"kernel": "k_jacobi4 (50 iterations)", "bound": "hbm", "achieved": achieved, "peak": peak,
-                     "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+        "roofline": {"kernel": "k_jacobi4 (50 iterations)", "bound": jac_bound, "achieved": achieved,
+                     "peak": l2.value if jac_bound == "l2" else peak, "unit": "GB/s",
+                     "frac": achieved / (l2.value if jac_bound == "l2" else peak),
+                     "peak_source": ("L2 read bandwidth measured in this run by the library's probe "
+                                     "(rl_measure_read_bandwidth: 48 MiB re-read 50 times)" if jac_bound == "l2"
+                                     else f"{peak_kind} HBM copy bandwidth"),
+                     "working_set_bytes": jac_set, "traffic": None,
                      "algorithmic_bytes": jac_bytes, "bytes_per_iteration": "8 B per nonzero + 44 B per row",
-                     "l2_read_gbs_measured": l2.value, "frac_of_l2": achieved / l2.value},
+                     "hbm": {"peak": peak, "source": peak_kind, "frac": achieved / peak}},
         # k_ff_hemi_rays / _rle / _compact, k_pack4, k_jacobi4 per iteration, k_unpack4
         "pairwise_form_factors": pairwise,
         "gpu_launches": (5 + iters) * steps,
@@ -970,6 +1104,9 @@ def main():
                     help="traversal tree for AO / final gather (0: the library's default)")
     ap.add_argument("--gather", default="disc", choices=["disc", "knn"],
                     help="photon estimate: Relight's disc gather (default) or the k-nearest-neighbour estimate")
+    ap.add_argument("--split", action="store_true",
+                    help="one terrain bake split over the ranks (photon shares and interleaved final-gather lumels, "
+                         "NCCL all-reduces; strong scaling) instead of one bake per rank")
     ap.add_argument("--knn-cell", type=int, default=0,
                     help="kNN grid cell width in 64ths of the radius (0: the library's default)")
     ap.add_argument("--workload", default="terrain",

@@ -14,12 +14,18 @@
  *     to it are sent back before the map's next bake.
  * Random numbers: each stochastic call draws from its own Philox4x32-10 key
  * (Relight::setSeed), where the reference calls the C library's rand().
+ * Threads: the bake calls of one Relight serialise on a lock, so Relight::bake
+ * accepts thread workers as the reference does; a GPU bake gains nothing
+ * from them (every call is one device pass), and the base Worker, which runs
+ * each job at once on the calling thread, is the natural choice.
  */
 #ifndef RELIGHT_B200_RELIGHT_H
 #define RELIGHT_B200_RELIGHT_H
 
 #include <cmath>
 #include <cstdint>
+#include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -115,6 +121,12 @@ class Texture;
 class Lightmap;
 class Photonmap;
 class Relight;
+class Worker;
+class Job;
+struct JobData;
+
+// Relight.h:70-71
+typedef std::vector<Worker*> Workers;
 
 // --------------------------------------------------------------- material
 
@@ -431,6 +443,51 @@ public:
     virtual void notify(const Mesh* instance, int step, int stepCount) {}
 };
 
+// ------------------------------------------------------- jobs and workers
+
+// Worker.h:35-42: what a worker is handed for one mesh.
+struct JobData {
+    Worker* m_worker = nullptr;            // parent worker (set by Worker::push)
+    Job* m_job = nullptr;                  // parent job
+    Relight* m_relight = nullptr;          // Relight instance
+    const Scene* m_scene = nullptr;        // scene to process
+    const Mesh* m_mesh = nullptr;          // mesh instance of the scene
+    bake::BakeIterator* m_iterator = nullptr;  // the worker's share of the mesh
+};
+
+// Worker.h:45-49: user code run for every (mesh, worker) pair, typically a
+// sequence of Relight::bake* calls on data->m_mesh with data->m_iterator.
+class Job {
+public:
+    virtual ~Job() {}
+    virtual void execute(JobData* data) = 0;
+};
+
+// Worker.h:52-69, Worker.cpp:43-83: for every scene mesh, largest bounding
+// volume first (ties keep scene order), push `job` to every worker j with
+// FaceBakeIterator(j, workers) (LumelBakeIterator(j, workers) for meshes with
+// fewer faces than workers), then wait for all workers.
+class FullBakeJob : public Job {
+public:
+    FullBakeJob(Job* job, const Workers& workers);
+    void execute(JobData* data) override;
+
+private:
+    Workers m_workers;
+    Job* m_job;
+};
+
+// Worker.h:72-84, Worker.cpp:86-106: the base worker runs a pushed job at
+// once on the calling thread (and then frees the JobData it was handed);
+// subclasses may run jobs on their own threads and take over the JobData.
+class Worker : public Progress {
+public:
+    Worker() {}
+    virtual ~Worker() {}
+    virtual void push(Job* job, JobData* data);
+    virtual void wait() {}
+};
+
 struct IndirectLightSettings {
     int m_photonPassCount;
     int m_photonBounceCount;
@@ -476,6 +533,9 @@ public:
     RelightStatus bakeAmbientOcclusion(const Scene* scene, const Mesh* mesh, Progress* progress,
                                        const AmbientOcclusionSettings& settings, bake::BakeIterator* iterator = nullptr);
     RelightStatus emitPhotons(const Scene* scene, const IndirectLightSettings& settings);
+    // Relight::bake (Relight.cpp:204-213): pushes a FullBakeJob over `workers`
+    // to `root`.  With the base Worker as root the bake is done on return.
+    void bake(const Scene* scene, Job* job, Worker* root, const Workers& workers);
     // Base of the Philox keys of the stochastic passes (no reference counterpart).
     void setSeed(uint64_t seed) { m_seed = seed; m_calls = 0; }
     // Message of the last failed device call.
@@ -489,6 +549,8 @@ private:
     uint64_t m_seed = 0x5EED;
     uint64_t m_calls = 0;
     std::string m_error;
+    std::mutex m_lock;  // serialises the bake calls of worker threads
+    std::vector<std::unique_ptr<FullBakeJob>> m_jobs;  // freed with the Relight
 };
 
 }  // namespace relight

@@ -117,6 +117,12 @@ int rl_scene_create(const rl_scene_desc* desc, int builder, void* stream, rl_sce
 int rl_scene_destroy(rl_scene* scene);
 /* BVH statistics: node count, leaf count, max depth, SAH cost. */
 int rl_scene_bvh_stats(const rl_scene* scene, int64_t* nodes, int64_t* leaves, int32_t* depth, double* sah);
+/* The scene's traversal status word, read after the work queued on `stream`
+   (waits for it): bit 0 = a traversal stack overflowed (a ray may have
+   skipped part of the tree).  `clear` != 0 resets it.  Embree reports no
+   such condition (rtcIntersect has no failure path); this is the check
+   behind every bake of a scene. */
+int rl_scene_status(rl_scene* scene, int clear, int32_t* flags, void* stream);
 
 /* ------------------------------------------------------------ tracing */
 
@@ -133,6 +139,24 @@ int rl_scene_bvh_stats(const rl_scene* scene, int64_t* nodes, int64_t* leaves, i
 int rl_trace_segments(const rl_scene* scene, int64_t n, const float* d_seg, int flags, int32_t* d_hit,
                       float* d_t_uv, int32_t* d_mesh_face, float* d_point, float* d_normal, float* d_rgba,
                       float* d_uv, void* stream);
+
+/* rtcIntersect / rtcOccluded (Embree 2, embree2/rtcore_ray.h:24-51 and
+   rtcore_scene.h; called at rt/Embree.cpp:139,151) for a batch of rays in
+   Embree's own terms: the closest hit (any_hit = 0) or some hit (any_hit =
+   1) on the open interval (tnear, tfar) of org + t * dir, ties to the
+   smaller (geomID, primID).  The Embree-level seam: the reference's
+   rt::Embree runs unchanged with these answering its Embree calls.
+     d_rays      [n][8]  org xyz, tnear, dir xyz, tfar (16-byte aligned)
+     d_geom_prim [n][2]  geomID (scene mesh), primID (face); -1, -1 on a miss
+     d_t_uv      [n][3]  t, u, v of the hit (may be NULL)
+   rl_intersect_rays_host is the same call on host arrays: it stages them
+   through a device buffer of the calling thread (kept for its next call),
+   runs on that thread's own stream and returns when the results are in
+   host memory, so several host threads may call it at once. */
+int rl_intersect_rays(const rl_scene* scene, int64_t n, const float* d_rays, int any_hit, int32_t* d_geom_prim,
+                      float* d_t_uv, void* stream);
+int rl_intersect_rays_host(const rl_scene* scene, int64_t n, const float* rays, int any_hit, int32_t* geom_prim,
+                           float* t_uv);
 
 /* ----------------------------------------------------------- lumel maps */
 
@@ -469,9 +493,12 @@ int rl_radiosity_solve(int n, const int64_t* d_row_ptr, const int32_t* d_cols, c
                        const float* d_E, const float* d_rho, int iters, float* d_B, void* stream);
 
 /* One Jacobi step restricted to rows [row_begin, row_end):
-   d_B_next[row] = E[row] + rho[row] * sum_k F[row][k] d_B[k].  The unit of a
-   row-sharded solve across GPUs (each GPU steps its rows, then the rows are
-   all-gathered into d_B). */
+   d_B_next[row] = E[row] + rho[row] * sum_k F[row][k] d_B[k] ([n][3] arrays,
+   rows written at their own index).  The unit of a row-sharded solve across
+   GPUs (each GPU steps its rows, then the rows are all-gathered into d_B).
+   Each row uses rl_radiosity_solve's arithmetic (the same 16-byte-load
+   choice for aligned d_cols / d_vals), so iterating it over all rows gives
+   rl_radiosity_solve's bits. */
 int rl_radiosity_step(int row_begin, int row_end, const int64_t* d_row_ptr, const int32_t* d_cols,
                       const float* d_vals, const float* d_E, const float* d_rho, const float* d_B, float* d_B_next,
                       void* stream);
@@ -480,14 +507,19 @@ int rl_radiosity_step(int row_begin, int row_end, const int64_t* d_row_ptr, cons
    inside a host application (a game engine or an editor) that owns every
    device allocation itself, or a bake server that reserved its HBM when the
    request was admitted.  This entry point calls no cudaMalloc, cudaFree or
-   allocating routine; its ping-pong buffer is a fixed array of
-   RL_SOLVE_NOALLOC_MAX_PATCHES x 3 floats (768 KiB) that every GPU loading
-   this library holds until the process exits.  Larger `n` is rejected with
-   RL_INVALID_CALL.  The first call on a device looks the array's address up
-   (once per device, with that device current); make that first call before
-   any stream capture.  All calls share the one array, so calls whose work
-   overlaps on the GPU race; run them on one stream or one at a time.  No
-   counterpart in the reference. */
+   allocating routine.  Its two ping-pong iterates live in a fixed device
+   array of 2 x RL_SOLVE_NOALLOC_MAX_PATCHES float4 (2 MiB), committed on a
+   device when this library's solver module first loads there (the first
+   launch of one of its kernels, or the first call of this entry point; a
+   call with n = 0 is enough) and held until the process exits.  Callers
+   that budget HBM up front make that warm-up call first.  Larger `n` is
+   rejected with RL_INVALID_CALL.  The first call on a device looks the
+   array's address up (once per device, with that device current); make it
+   before any stream capture.  It runs the same kernels in the same order as
+   rl_radiosity_solve, so both give the same bits, and d_B may alias d_E or
+   d_rho (it is written last).  All calls share the one array, so calls
+   whose work overlaps on the GPU race; run them on one stream or one at a
+   time.  No counterpart in the reference. */
 #define RL_SOLVE_NOALLOC_MAX_PATCHES 65536
 int rl_radiosity_solve_noalloc(int n, const int64_t* d_row_ptr, const int32_t* d_cols, const float* d_vals,
                                const float* d_E, const float* d_rho, int iters, float* d_B, void* stream);
@@ -528,6 +560,13 @@ int rl_tune_get(int param, int* value);
    loads; below the L2 size this is the L2 bandwidth the traversal kernels
    draw on.  A measurement utility with no counterpart in the reference. */
 int rl_measure_read_bandwidth(size_t bytes, int iters, double* gbs);
+/* L1 read bandwidth (GB/s, whole GPU): every block re-reads the same
+   `bytes_per_block` (a multiple of 16 KiB, at most 128 KiB) `iters` times
+   with 16-byte cached
+   loads, so after the first pass the loads hit each SM's L1 — the level a
+   tree of a few hundred triangles lives in.  No counterpart in the
+   reference. */
+int rl_measure_l1_read_bandwidth(size_t bytes_per_block, int iters, double* gbs);
 
 #ifdef __cplusplus
 }

@@ -20,6 +20,9 @@ ROOT = os.path.dirname(ORACLE_DIR)
 ORACLE_LIB = os.path.join(ORACLE_DIR, "liboracle.so")
 REF_LIB = os.environ.get("RELIGHT_REF_LIB") or os.path.join(ORACLE_DIR, "_ref", "librelight_ref.so")
 REF_FAST_LIB = os.path.join(ORACLE_DIR, "_ref", "librelight_ref_fast.so")
+# the reference over the GPU Embree backend (embree2_gpu.cpp): same sources,
+# its Embree calls answered by relight_b200/librelight_b200.so
+REF_GPU_LIB = os.path.join(ORACLE_DIR, "_ref", "librelight_ref_gpu.so")
 
 _P = C.c_void_p
 
@@ -31,6 +34,17 @@ def build_oracle():
 
 def reference_available():
     return os.path.exists(REF_LIB)
+
+
+def reference_root():
+    """The reference checkout the oracle/_ref build was compiled from, as
+    recorded by oracle/Makefile, or None where it is not present."""
+    p = os.path.join(ORACLE_DIR, "_ref", "reference_root.txt")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        root = f.read().strip()
+    return root if os.path.isdir(root) else None
 
 
 class Lumels(C.Structure):
@@ -413,7 +427,9 @@ _refs = {}
 
 
 def ref_lib(fast=False):
-    path = REF_FAST_LIB if fast else REF_LIB
+    """fast: False = the parity build, True = the timed build, "gpu" = the
+    parity build over the GPU Embree backend."""
+    path = REF_GPU_LIB if fast == "gpu" else REF_FAST_LIB if fast else REF_LIB
     if path not in _refs:
         _refs[path] = _load_ref(path)
     return _refs[path]

@@ -103,6 +103,9 @@ SIGNATURES = {
     "rl_scene_create": (_I, [_P, _I, _P, _P]),
     "rl_scene_destroy": (_I, [_P]),
     "rl_scene_bvh_stats": (_I, [_P, _P, _P, _P, _P]),
+    "rl_scene_status": (_I, [_P, _I, _P, _P]),
+    "rl_intersect_rays": (_I, [_P, C.c_int64, _P, _I, _P, _P, _P]),
+    "rl_intersect_rays_host": (_I, [_P, C.c_int64, _P, _I, _P, _P]),
     "rl_trace_segments": (_I, [_P, _I64, _P, _I, _P, _P, _P, _P, _P, _P, _P, _P]),
     "rl_map_create": (_I, [_I, _I, _I, _P]),
     "rl_map_destroy": (_I, [_P]),
@@ -170,6 +173,7 @@ SIGNATURES = {
     "rl_batch_work_items": (_I, [_P, _P]),
     "rl_batch_destroy": (_I, [_P]),
     "rl_measure_read_bandwidth": (_I, [C.c_size_t, _I, _P]),
+    "rl_measure_l1_read_bandwidth": (_I, [C.c_size_t, _I, _P]),
     "rl_tune_set": (_I, [_I, _I]),
     "rl_tune_get": (_I, [_I, _P]),
 }

@@ -66,7 +66,7 @@ def build_cpp_example(out_dir: str, name: str = "bake_room") -> str:
     API (include/relight/Relight.h) and this library."""
     src = os.path.join(ROOT, "tests", "cpp", name + ".cpp")
     exe = os.path.join(out_dir, name)
-    cmd = [os.environ.get("CXX", "g++"), "-std=c++17", "-O2", "-I", os.path.join(ROOT, "include"), src,
+    cmd = [os.environ.get("CXX", "g++"), "-std=c++17", "-O2", "-pthread", "-I", os.path.join(ROOT, "include"), src,
            "-L", HERE, "-lrelight_b200", "-Wl,-rpath," + HERE, "-o", exe]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:

@@ -462,6 +462,57 @@ AmbientOcclusionSettings AmbientOcclusionSettings::production(float f, float d, 
 
 // ----------------------------------------------------------------- relight
 
+// ------------------------------------------------------- jobs and workers
+
+void Worker::push(Job* job, JobData* data) {
+    data->m_worker = this;
+    job->execute(data);
+    delete data;
+}
+
+FullBakeJob::FullBakeJob(Job* job, const Workers& workers) : m_workers(workers), m_job(job) {}
+
+void FullBakeJob::execute(JobData* data) {
+    const int n = (int)m_workers.size();
+    std::vector<const Mesh*> meshes;
+    for (int i = 0; i < data->m_scene->meshCount(); i++) meshes.push_back(data->m_scene->mesh(i));
+    std::stable_sort(meshes.begin(), meshes.end(),
+                     [](const Mesh* a, const Mesh* b) { return a->bounds().volume() > b->bounds().volume(); });
+    for (const Mesh* mesh : meshes) {
+        std::vector<std::unique_ptr<bake::BakeIterator>> iterators;
+        for (int j = 0; j < n; j++) {
+            JobData* d = new JobData;
+            d->m_job = m_job;
+            d->m_scene = data->m_scene;
+            d->m_relight = data->m_relight;
+            d->m_mesh = mesh;
+            if (mesh->faceCount() >= n)
+                iterators.emplace_back(new bake::FaceBakeIterator(j, n));
+            else
+                iterators.emplace_back(new bake::LumelBakeIterator(j, n));
+            d->m_iterator = iterators.back().get();
+            m_workers[j]->push(m_job, d);
+        }
+        for (int j = 0; j < n; j++) m_workers[j]->wait();
+    }
+}
+
+void Relight::bake(const Scene* scene, Job* job, Worker* root, const Workers& workers) {
+    FullBakeJob* full;
+    {
+        std::unique_lock<std::mutex> g(m_lock);
+        m_jobs.emplace_back(new FullBakeJob(job, workers));
+        full = m_jobs.back().get();
+    }
+    JobData* data = new JobData;
+    data->m_scene = scene;
+    data->m_relight = this;
+    data->m_job = full;
+    root->push(full, data);
+}
+
+// ----------------------------------------------------------------- relight
+
 uint64_t Relight::nextSeed() {
     m_calls++;
     return m_seed * 0x9E3779B97F4A7C15ull + m_calls;
@@ -567,6 +618,7 @@ static std::vector<rl_map*> photon_maps(const Scene* scene) {
 // checks (baker/Baker.cpp:52-77).
 RelightStatus Relight::bakeDirectLight(const Scene* scene, const Mesh* mesh, Progress* progress,
                                        bake::BakeIterator* iterator) {
+    std::unique_lock<std::mutex> g(m_lock);
     if (!mesh || mesh->faceCount() == 0 || !mesh->lightmap() || !prepare(scene)) return RelightInvalidCall;
     Lightmap* lm = mesh->lightmap();
     lm->beforeDevice();
@@ -576,12 +628,14 @@ RelightStatus Relight::bakeDirectLight(const Scene* scene, const Mesh* mesh, Pro
                             (int)(t.verts.size() / 3), &it, nullptr);
     cudaStreamSynchronize(nullptr);
     lm->afterDevice();
+    g.unlock();  // the callback may take its own locks
     if (progress) progress->notify(mesh, 1, 1);
     return status(rc);
 }
 
 RelightStatus Relight::bakeAmbientOcclusion(const Scene* scene, const Mesh* mesh, Progress* progress,
                                             const AmbientOcclusionSettings& s, bake::BakeIterator* iterator) {
+    std::unique_lock<std::mutex> g(m_lock);
     if (!mesh || mesh->faceCount() == 0 || !mesh->lightmap() || !prepare(scene)) return RelightInvalidCall;
     Lightmap* lm = mesh->lightmap();
     lm->beforeDevice();
@@ -590,12 +644,14 @@ RelightStatus Relight::bakeAmbientOcclusion(const Scene* scene, const Mesh* mesh
                         s.m_exponent, nextSeed(), &it, nullptr);
     cudaStreamSynchronize(nullptr);
     lm->afterDevice();
+    g.unlock();  // the callback may take its own locks
     if (progress) progress->notify(mesh, 1, 1);
     return status(rc);
 }
 
 // Relight::emitPhotons (Relight.cpp:244-257): trace, then gather each photonmap.
 RelightStatus Relight::emitPhotons(const Scene* scene, const IndirectLightSettings& s) {
+    std::unique_lock<std::mutex> g(m_lock);
     if (!prepare(scene)) return RelightInvalidCall;
     std::vector<rl_map*> maps = photon_maps(scene);
     LightTables t = light_tables(scene);
@@ -612,6 +668,7 @@ RelightStatus Relight::emitPhotons(const Scene* scene, const IndirectLightSettin
 
 RelightStatus Relight::bakeIndirectLight(const Scene* scene, const Mesh* mesh, Progress* progress,
                                          const IndirectLightSettings& s, bake::BakeIterator* iterator) {
+    std::unique_lock<std::mutex> g(m_lock);
     if (!mesh || mesh->faceCount() == 0 || !mesh->lightmap() || !prepare(scene)) return RelightInvalidCall;
     Lightmap* lm = mesh->lightmap();
     lm->beforeDevice();
@@ -623,6 +680,7 @@ RelightStatus Relight::bakeIndirectLight(const Scene* scene, const Mesh* mesh, P
                               s.m_finalGatherDistance, sky, amb, nextSeed(), &it, nullptr);
     cudaStreamSynchronize(nullptr);
     lm->afterDevice();
+    g.unlock();  // the callback may take its own locks
     if (progress) progress->notify(mesh, 1, 1);
     return status(rc);
 }

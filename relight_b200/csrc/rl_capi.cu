@@ -10,7 +10,7 @@
 //   IndirectLight::bakeLumel           k_indirect
 //   RadiosityBuilder form factors      k_ff_pairs (+ host CSR assembly)
 //   hemisphere form factors            k_ff_hemi_rays + k_ff_hemi_rle + k_ff_hemi_compact
-//   radiosity gather iterations        k_jacobi
+//   radiosity gather iterations        k_jacobi4 (k_jacobi_rows per row shard)
 #include <cuda_runtime.h>
 
 #include <cub/block/block_scan.cuh>
@@ -368,6 +368,17 @@ extern "C" int rl_scene_bvh_stats(const rl_scene* s, int64_t* nodes, int64_t* le
     return RL_OK;
 }
 
+extern "C" int rl_scene_status(rl_scene* s, int clear, int32_t* flags, void* stream) {
+    if (!s || !flags) return fail(RL_INVALID_CALL, "rl_scene_status: null argument");
+    cudaStream_t st = S(stream);
+    int h = 0;
+    CK(cudaMemcpyAsync(&h, s->d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
+    if (clear) CK(cudaMemsetAsync(s->d_status, 0, sizeof(int), st));
+    CK(cudaStreamSynchronize(st));
+    *flags = h;
+    return RL_OK;
+}
+
 static int check_status(const rl_scene* s, cudaStream_t st) {
     int h = 0;
     CK(cudaMemcpyAsync(&h, s->d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -410,6 +421,88 @@ extern "C" int rl_trace_segments(const rl_scene* s, int64_t n, const float* d_se
     CK_LAUNCH("k_trace_segments");
     return RL_OK;
 }
+
+// rtcIntersect / rtcOccluded (embree2/rtcore_ray.h:24-51) for a batch of
+// rays given as Embree takes them: closest hit (or, with any_hit, some hit)
+// on the open interval (tnear, tfar) of org + t dir, ties to the smaller
+// (geomID, primID).
+__global__ void k_intersect_rays(DevScene s, long long n, const float4* rays, int any_hit, int* geom_prim,
+                                 float* tuv, int* status) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 a = rays[2 * i], b = rays[2 * i + 1];
+    const V3 o = mk3(a.x, a.y, a.z), d = mk3(b.x, b.y, b.z);
+    RayHit h;
+    const bool hit = any_hit ? traverse<true>(s, o, d, a.w, b.w, h, status)
+                             : traverse<false>(s, o, d, a.w, b.w, h, status);
+    int mesh = -1, prim = -1;
+    if (hit) {
+        mesh = __ldg(s.tri_vidx + h.gid).w;
+        prim = h.gid - s.mesh_first_tri[mesh];
+    }
+    geom_prim[2 * i] = mesh;
+    geom_prim[2 * i + 1] = prim;
+    if (tuv) {
+        tuv[3 * i] = hit ? h.t : 0.f;
+        tuv[3 * i + 1] = hit ? h.u : 0.f;
+        tuv[3 * i + 2] = hit ? h.v : 0.f;
+    }
+}
+
+extern "C" int rl_intersect_rays(const rl_scene* s, int64_t n, const float* d_rays, int any_hit, int32_t* d_geom_prim,
+                                 float* d_t_uv, void* stream) {
+    if (!s || n < 0 || (n > 0 && (!d_rays || !d_geom_prim)))
+        return fail(RL_INVALID_CALL, "rl_intersect_rays: bad arguments");
+    if ((uintptr_t)d_rays % 16) return fail(RL_INVALID_CALL, "rl_intersect_rays: rays must be 16-byte aligned");
+    if (n == 0) return RL_OK;
+    k_intersect_rays<<<blocks_for(n, 128), 128, 0, S(stream)>>>(s->dev, n, reinterpret_cast<const float4*>(d_rays),
+                                                                any_hit, d_geom_prim, d_t_uv, s->d_status);
+    CK_LAUNCH("k_intersect_rays");
+    return RL_OK;
+}
+
+namespace {
+// Per-host-thread staging of rl_intersect_rays_host: its own stream and a
+// device buffer that grows to the largest batch seen.
+struct IntersectStaging {
+    cudaStream_t stream = nullptr;
+    char* dev = nullptr;
+    size_t cap = 0;
+    ~IntersectStaging() {
+        if (dev) cudaFree(dev);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+thread_local IntersectStaging t_staging;
+}  // namespace
+
+extern "C" int rl_intersect_rays_host(const rl_scene* s, int64_t n, const float* rays, int any_hit,
+                                      int32_t* geom_prim, float* t_uv) {
+    if (!s || n < 0 || (n > 0 && (!rays || !geom_prim)))
+        return fail(RL_INVALID_CALL, "rl_intersect_rays_host: bad arguments");
+    if (n == 0) return RL_OK;
+    IntersectStaging& st = t_staging;
+    if (!st.stream) CK(cudaStreamCreateWithFlags(&st.stream, cudaStreamNonBlocking));
+    const size_t in = 32 * (size_t)n, gp = 8 * (size_t)n, tu = 12 * (size_t)n, need = in + gp + tu;
+    if (need > st.cap) {
+        if (st.dev) cudaFree(st.dev);
+        st.dev = nullptr;
+        st.cap = 0;
+        CK(cudaMalloc(&st.dev, need));
+        st.cap = need;
+    }
+    float* d_rays = reinterpret_cast<float*>(st.dev);
+    int32_t* d_gp = reinterpret_cast<int32_t*>(st.dev + in);
+    float* d_tuv = reinterpret_cast<float*>(st.dev + in + gp);
+    CK(cudaMemcpyAsync(d_rays, rays, in, cudaMemcpyHostToDevice, st.stream));
+    int rc = rl_intersect_rays(s, n, d_rays, any_hit, d_gp, t_uv ? d_tuv : nullptr, st.stream);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(geom_prim, d_gp, gp, cudaMemcpyDeviceToHost, st.stream));
+    if (t_uv) CK(cudaMemcpyAsync(t_uv, d_tuv, tu, cudaMemcpyDeviceToHost, st.stream));
+    CK(cudaStreamSynchronize(st.stream));
+    return RL_OK;
+}
+
 
 // ---------------------------------------------------------------- maps
 
@@ -1773,29 +1866,15 @@ __device__ __forceinline__ void row_dot3(int64_t b, int64_t e, int lane, const i
     }
 }
 
-// One warp per patch row: B'_i = E_i + rho_i * sum_k F_ik B_k (RGB).
-__global__ void k_jacobi(int n, const int64_t* row_ptr, const int32_t* cols, const float* vals, const float* E,
-                         const float* rho, const float* B, float* Bn) {
-    int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    int lane = threadIdx.x & 31;
-    if (warp >= n) return;
-    float s0, s1, s2;
-    row_dot3<0>(row_ptr[warp], row_ptr[warp + 1], lane, cols, vals, B, s0, s1, s2);
-    if (lane == 0) {
-        size_t i = 3 * (size_t)warp;
-        Bn[i] = __fmaf_rn(rho[i], s0, E[i]);
-        Bn[i + 1] = __fmaf_rn(rho[i + 1], s1, E[i + 1]);
-        Bn[i + 2] = __fmaf_rn(rho[i + 2], s2, E[i + 2]);
-    }
-}
-
 // Row dot with 16-byte column and weight loads: lane l takes the aligned
 // quads base + 4 l and base + 128 + 4 l, two per step (256 nonzeros per warp
 // step, about 6 KB in flight with their gathers); elements outside [b, e)
 // are loaded one by one or skipped, so no load leaves the row.  cols and
-// vals must be 16-byte aligned.
+// vals must be 16-byte aligned.  Both B layouts (kB as in row_dot3) load the
+// same values, so they give the same bits.
+template <int kB>
 __device__ __forceinline__ void row_dot3_quads(int64_t b, int64_t e, int lane, const int32_t* __restrict__ cols,
-                                               const float* __restrict__ vals, const float4* __restrict__ B,
+                                               const float* __restrict__ vals, const float* __restrict__ B,
                                                float& r0, float& r1, float& r2) {
     float s[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
     for (int64_t base = b & ~(int64_t)3; base < e; base += 256) {
@@ -1827,7 +1906,7 @@ __device__ __forceinline__ void row_dot3_quads(int64_t b, int64_t e, int lane, c
 #pragma unroll
             for (int j = 0; j < 4; j++)
                 if (c[u][j] >= 0) {
-                    const float4 x = __ldg(B + c[u][j]);
+                    const float3 x = patch_b<kB>(B, c[u][j]);
                     s[u][0] = __fmaf_rn(w[u][j], x.x, s[u][0]);
                     s[u][1] = __fmaf_rn(w[u][j], x.y, s[u][1]);
                     s[u][2] = __fmaf_rn(w[u][j], x.z, s[u][2]);
@@ -1844,9 +1923,10 @@ __device__ __forceinline__ void row_dot3_quads(int64_t b, int64_t e, int lane, c
     }
 }
 
-// k_jacobi on [n][4] iterates (w unused): one 16-byte gather per nonzero
-// instead of three 4-byte ones; with kQuads, 16-byte column and weight
-// loads as well (the accumulation order differs, within the fp32 tolerance).
+// One warp per patch row on [n][4] iterates (w unused), one 16-byte gather
+// per nonzero: B'_i = E_i + rho_i * sum_k F_ik B_k (RGB).  With kQuads,
+// 16-byte column and weight loads as well (a different accumulation order
+// from row_dot3, within the fp32 tolerance).
 template <bool kQuads>
 __global__ void k_jacobi4(int n, const int64_t* row_ptr, const int32_t* cols, const float* vals, const float* E,
                           const float* rho, const float4* B, float4* Bn) {
@@ -1855,7 +1935,8 @@ __global__ void k_jacobi4(int n, const int64_t* row_ptr, const int32_t* cols, co
     if (warp >= n) return;
     float s0, s1, s2;
     if (kQuads)
-        row_dot3_quads(row_ptr[warp], row_ptr[warp + 1], lane, cols, vals, B, s0, s1, s2);
+        row_dot3_quads<1>(row_ptr[warp], row_ptr[warp + 1], lane, cols, vals, reinterpret_cast<const float*>(B), s0,
+                          s1, s2);
     else
         row_dot3<1>(row_ptr[warp], row_ptr[warp + 1], lane, cols, vals, reinterpret_cast<const float*>(B), s0, s1,
                     s2);
@@ -1881,7 +1962,11 @@ __global__ void k_unpack4(int n, const float4* src, float* dst) {
     }
 }
 
-// One Jacobi step over rows [row_begin, row_end): Bn[row] from the full B.
+// One Jacobi step over rows [row_begin, row_end): Bn[row] from the full B,
+// [n][3] iterates, with k_jacobi4's row arithmetic (16-byte column and
+// weight loads under the same alignment rule), so a row-sharded solve gives
+// rl_radiosity_solve's bits.
+template <bool kQuads>
 __global__ void k_jacobi_rows(int row_begin, int row_end, const int64_t* row_ptr, const int32_t* cols,
                               const float* vals, const float* E, const float* rho, const float* B, float* Bn) {
     int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -1889,7 +1974,10 @@ __global__ void k_jacobi_rows(int row_begin, int row_end, const int64_t* row_ptr
     int row = row_begin + warp;
     if (row >= row_end) return;
     float s0, s1, s2;
-    row_dot3<0>(row_ptr[row], row_ptr[row + 1], lane, cols, vals, B, s0, s1, s2);
+    if (kQuads)
+        row_dot3_quads<0>(row_ptr[row], row_ptr[row + 1], lane, cols, vals, B, s0, s1, s2);
+    else
+        row_dot3<0>(row_ptr[row], row_ptr[row + 1], lane, cols, vals, B, s0, s1, s2);
     if (lane == 0) {
         size_t i = 3 * (size_t)row;
         Bn[i] = __fmaf_rn(rho[i], s0, E[i]);
@@ -1904,8 +1992,13 @@ extern "C" int rl_radiosity_step(int row_begin, int row_end, const int64_t* d_ro
     if (row_begin < 0 || row_end < row_begin || !d_row_ptr || !d_E || !d_rho || !d_B || !d_B_next)
         return fail(RL_INVALID_CALL, "rl_radiosity_step: bad arguments");
     if (row_end == row_begin) return RL_OK;
-    k_jacobi_rows<<<blocks_for((long long)(row_end - row_begin) * 32, 256), 256, 0, S(stream)>>>(
-        row_begin, row_end, d_row_ptr, d_cols, d_vals, d_E, d_rho, d_B, d_B_next);
+    const unsigned grid = blocks_for((long long)(row_end - row_begin) * 32, 256);
+    if (((uintptr_t)d_cols % 16) == 0 && ((uintptr_t)d_vals % 16) == 0)
+        k_jacobi_rows<true><<<grid, 256, 0, S(stream)>>>(row_begin, row_end, d_row_ptr, d_cols, d_vals, d_E, d_rho,
+                                                         d_B, d_B_next);
+    else
+        k_jacobi_rows<false><<<grid, 256, 0, S(stream)>>>(row_begin, row_end, d_row_ptr, d_cols, d_vals, d_E, d_rho,
+                                                          d_B, d_B_next);
     CK_LAUNCH("k_jacobi_rows");
     return RL_OK;
 }
@@ -2589,21 +2682,24 @@ extern "C" int rl_batch_destroy(rl_batch* b) {
 
 // ------------------------------------------------- solve without allocation
 
-// Ping-pong buffer of rl_radiosity_solve_noalloc: a fixed array in device
-// memory, reserved when the library is loaded (on every GPU that loads it,
-// until the process exits) so that the solve itself never allocates.
-static __device__ __align__(256) float g_solve_scratch[3 * RL_SOLVE_NOALLOC_MAX_PATCHES];
+// The two [n][4] ping-pong iterates of rl_radiosity_solve_noalloc: a fixed
+// array in device memory (2 x RL_SOLVE_NOALLOC_MAX_PATCHES float4, 2 MiB).
+// It is committed on a device when this file's module first loads there:
+// with CUDA's lazy module loading, at the first launch of any kernel of this
+// file or at the first rl_radiosity_solve_noalloc call (an n = 0 call is
+// enough), and it stays until the process exits.
+static __device__ __align__(256) float4 g_solve_scratch[2 * RL_SOLVE_NOALLOC_MAX_PATCHES];
 
 namespace {
 constexpr int kMaxDevices = 64;
 std::mutex g_scratch_mutex;
-float* g_scratch_ptr[kMaxDevices] = {};  // device address of g_solve_scratch, per device
+float4* g_scratch_ptr[kMaxDevices] = {};  // device address of g_solve_scratch, per device
 }  // namespace
 
 // Host code only sees a host-side stand-in for g_solve_scratch; the device
 // address comes from cudaGetSymbolAddress, looked up once per device with
 // that device current.
-static int solve_scratch(float** out) {
+static int solve_scratch(float4** out) {
     int dev = -1;
     CK(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kMaxDevices) return fail(RL_INVALID_CALL, "device ordinal %d out of range", dev);
@@ -2614,12 +2710,16 @@ static int solve_scratch(float** out) {
         if (e != cudaSuccess || !p)
             return fail(RL_CUDA_ERROR, "cudaGetSymbolAddress(g_solve_scratch) failed on device %d: %s", dev,
                         cudaGetErrorString(e));
-        g_scratch_ptr[dev] = (float*)p;
+        g_scratch_ptr[dev] = (float4*)p;
     }
     *out = g_scratch_ptr[dev];
     return RL_OK;
 }
 
+// The kernels and launch sequence of rl_radiosity_solve (k_pack4, k_jacobi4
+// with the same 16-byte-load choice, k_unpack4), so the two give the same
+// bits.  d_B is written only by the final k_unpack4, after every read of
+// d_E and d_rho, so d_B may alias either input.
 extern "C" int rl_radiosity_solve_noalloc(int n, const int64_t* d_row_ptr, const int32_t* d_cols,
                                           const float* d_vals, const float* d_E, const float* d_rho, int iters,
                                           float* d_B, void* stream) {
@@ -2628,23 +2728,34 @@ extern "C" int rl_radiosity_solve_noalloc(int n, const int64_t* d_row_ptr, const
     if (n > RL_SOLVE_NOALLOC_MAX_PATCHES)
         return fail(RL_INVALID_CALL, "rl_radiosity_solve_noalloc: %d patches exceed the fixed maximum of %d "
                                      "(use rl_radiosity_solve)", n, RL_SOLVE_NOALLOC_MAX_PATCHES);
-    float* tmp = nullptr;
-    int rc = solve_scratch(&tmp);
+    float4* scratch_base = nullptr;
+    int rc = solve_scratch(&scratch_base);
     if (rc) return rc;
     cudaStream_t st = S(stream);
     if (n == 0) return RL_OK;
-    CK(cudaMemcpyAsync(d_B, d_E, 12 * (size_t)n, cudaMemcpyDeviceToDevice, st));
-    // Every iteration writes all 3n values of its destination before the next
-    // one reads them, so the scratch array needs no clearing.
-    float* src = d_B;
-    float* dst = tmp;
+    if (iters == 0) {
+        if (d_B != d_E) CK(cudaMemcpyAsync(d_B, d_E, 12 * (size_t)n, cudaMemcpyDeviceToDevice, st));
+        return RL_OK;
+    }
+    // B0 = E; every iteration writes all n entries of its destination before
+    // the next one reads them, so what earlier calls left in the array is
+    // never read.
+    float4* src = scratch_base;
+    float4* dst = scratch_base + RL_SOLVE_NOALLOC_MAX_PATCHES;
+    k_pack4<<<blocks_for(n, 256), 256, 0, st>>>(n, d_E, src);
+    CK_LAUNCH("k_pack4");
     unsigned grid = blocks_for((long long)n * 32, 256);
+    const bool quads = ((uintptr_t)d_cols % 16) == 0 && ((uintptr_t)d_vals % 16) == 0;
     for (int it = 0; it < iters; it++) {
-        k_jacobi<<<grid, 256, 0, st>>>(n, d_row_ptr, d_cols, d_vals, d_E, d_rho, src, dst);
-        CK_LAUNCH("k_jacobi");
+        if (quads)
+            k_jacobi4<true><<<grid, 256, 0, st>>>(n, d_row_ptr, d_cols, d_vals, d_E, d_rho, src, dst);
+        else
+            k_jacobi4<false><<<grid, 256, 0, st>>>(n, d_row_ptr, d_cols, d_vals, d_E, d_rho, src, dst);
+        CK_LAUNCH("k_jacobi4");
         std::swap(src, dst);
     }
-    if (src != d_B) CK(cudaMemcpyAsync(d_B, src, 12 * (size_t)n, cudaMemcpyDeviceToDevice, st));
+    k_unpack4<<<blocks_for(n, 256), 256, 0, st>>>(n, src, d_B);
+    CK_LAUNCH("k_unpack4");
     return RL_OK;
 }
 
@@ -2683,6 +2794,53 @@ extern "C" int rl_measure_read_bandwidth(size_t bytes, int iters, double* gbs) {
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, e0, e1));
     *gbs = (double)bytes * iters / (ms * 1e-3) / 1e9;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(buf);
+    cudaFree(sink);
+    return RL_OK;
+}
+
+// Each block walks the same `n4` float4s (a multiple of 1024) `iters` times
+// with ld.global.nc (L1-cached) loads, four independent loads in flight per
+// thread: 148 x 4 blocks of 256 threads; after the first pass every load is
+// an L1 hit.
+__global__ void __launch_bounds__(256) k_read_probe_l1(const float4* __restrict__ buf, size_t n4, int iters,
+                                                       float* sink) {
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+    for (int it = 0; it < iters; it++)
+        for (size_t i = threadIdx.x; i + 3 * 256 < n4; i += 4 * 256) {
+            const float4 v0 = __ldg(buf + i), v1 = __ldg(buf + i + 256), v2 = __ldg(buf + i + 512),
+                         v3 = __ldg(buf + i + 768);
+            a0 += v0.x + v0.w;
+            a1 += v1.x + v1.w;
+            a2 += v2.x + v2.w;
+            a3 += v3.x + v3.w;
+        }
+    if (a0 + a1 + a2 + a3 == 1234.5f) *sink = a0;
+}
+
+extern "C" int rl_measure_l1_read_bandwidth(size_t bytes_per_block, int iters, double* gbs) {
+    if (!gbs || bytes_per_block < 16384 || bytes_per_block > (128u << 10) || bytes_per_block % 16384 || iters <= 0)
+        return fail(RL_INVALID_CALL, "rl_measure_l1_read_bandwidth: bad arguments (16 KiB multiple, at most 128 KiB)");
+    float4* buf = nullptr;
+    float* sink = nullptr;
+    CK(cudaMalloc(&buf, bytes_per_block));
+    CK(cudaMalloc(&sink, sizeof(float)));
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaMemset(buf, 0, bytes_per_block));
+    const size_t n4 = bytes_per_block / 16;
+    const int blocks = 4 * 148;
+    k_read_probe_l1<<<blocks, 256>>>(buf, n4, 1, sink);  // warm
+    CK(cudaEventRecord(e0));
+    k_read_probe_l1<<<blocks, 256>>>(buf, n4, iters, sink);
+    CK(cudaEventRecord(e1));
+    CK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, e0, e1));
+    *gbs = (double)bytes_per_block * blocks * iters / (ms * 1e-3) / 1e9;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     cudaFree(buf);

@@ -34,6 +34,68 @@ class FaceBakeIterator:
     step: int = 1
 
 
+@dataclass
+class JobData:
+    """Worker.h:35-42: what a worker is handed for one mesh."""
+    worker: Optional["Worker"] = None
+    job: Optional["Job"] = None
+    relight: Optional["Relight"] = None
+    scene: Optional[Scene] = None
+    mesh: Optional[Mesh] = None
+    iterator: object = None
+
+
+class Job:
+    """Worker.h:45-49: user code run for every (mesh, worker) pair."""
+
+    def execute(self, data: JobData):
+        raise NotImplementedError
+
+
+class Worker:
+    """Worker.h:72-84 (a Progress): runs a pushed job at once on the calling
+    thread; subclasses may run jobs elsewhere."""
+
+    def push(self, job: Job, data: JobData):
+        data.worker = self
+        job.execute(data)
+
+    def wait(self):
+        pass
+
+    def notify(self, instance, step, step_count):
+        pass
+
+
+def _volume(mesh: Mesh):
+    """Bounds::volume of the mesh's bounds, in float32 and the reference's
+    operation order."""
+    lo, hi = mesh.bounds()
+    d = (np.asarray(hi, np.float32) - np.asarray(lo, np.float32)).astype(np.float32)
+    return np.float32(np.float32(d[0] * d[1]) * d[2])
+
+
+class FullBakeJob(Job):
+    """Worker.h:52-69, Worker.cpp:43-83: for every scene mesh, largest bounding
+    volume first (ties keep scene order), push `job` to every worker j with
+    FaceBakeIterator(j, n) (LumelBakeIterator(j, n) when the mesh has fewer
+    faces than workers), then wait for every worker."""
+
+    def __init__(self, job: Job, workers):
+        self.job, self.workers = job, list(workers)
+
+    def execute(self, data: JobData):
+        n = len(self.workers)
+        meshes = sorted(data.scene.meshes, key=lambda m: -float(_volume(m)))
+        for mesh in meshes:
+            for j, w in enumerate(self.workers):
+                it = FaceBakeIterator(j, n) if mesh.face_count() >= n else LumelBakeIterator(j, n)
+                w.push(self.job, JobData(job=self.job, relight=data.relight, scene=data.scene, mesh=mesh,
+                                         iterator=it))
+            for w in self.workers:
+                w.wait()
+
+
 class DeviceScene:
     """An rl_scene: the flat scene uploaded and its BVH built (Scene::end)."""
 
@@ -48,6 +110,13 @@ class DeviceScene:
         nodes, leaves, depth, sah = C.c_int64(), C.c_int64(), C.c_int32(), C.c_double()
         check(lib().rl_scene_bvh_stats(self.handle, C.byref(nodes), C.byref(leaves), C.byref(depth), C.byref(sah)))
         return {"nodes": nodes.value, "leaves": leaves.value, "depth": depth.value, "sah": sah.value}
+
+    def status(self, clear=False, stream=None):
+        """The traversal status word after the queued work: bit 0 = a
+        traversal stack overflowed (rl_scene_status)."""
+        flags = C.c_int32()
+        check(lib().rl_scene_status(self.handle, int(clear), C.byref(flags), stream or self.stream))
+        return flags.value
 
     def close(self):
         if self.handle:
@@ -354,6 +423,65 @@ class Relight:
                                      settings.final_gather_samples, settings.final_gather_distance, sky, amb, seed,
                                      it, self.stream))
         return RelightStatus.RelightSuccess
+
+
+    def bake(self, scene: Scene, job: Job, root: Worker, workers) -> None:
+        """Relight::bake (Relight.cpp:204-213): push a FullBakeJob over
+        `workers` to `root`."""
+        full = FullBakeJob(job, workers)
+        root.push(full, JobData(job=full, relight=self, scene=scene))
+
+    # ------------------------------------------- one bake over several GPUs
+    # The engine interface of relight_b200.parallel: torch views of the
+    # device accumulators, and the shard-sized calls of each pass.
+
+    def torch_stream(self):
+        """The torch stream the collectives must run on so they order with
+        this object's kernels (None: torch's current stream)."""
+        import torch
+        return None if self.stream is None else torch.cuda.ExternalStream(int(self.stream))
+
+    def color_tensor(self, lightmap: Lightmap):
+        from .parallel import map_tensor
+        return map_tensor(lightmap._device, "color")
+
+    def photon_accumulators(self, scene: Scene):
+        """Colour sums, then photon counts, of every photonmap (zero-copy)."""
+        from .parallel import map_tensor
+        self.device_scene(scene)
+        maps = [m._device for m in scene.flat.photonmaps]
+        return [map_tensor(m, "color") for m in maps] + [map_tensor(m, "photons") for m in maps]
+
+    def photon_total(self, scene: Scene, settings: IndirectLightSettings) -> int:
+        f = scene.flat
+        total = C.c_int64()
+        check(lib().rl_photon_count(C.c_void_p(f.lights.ctypes.data), len(f.lights), settings.photon_pass_count,
+                                    C.byref(total)))
+        return total.value
+
+    def emit_photon_range(self, scene: Scene, settings: IndirectLightSettings, seed: int, first: int, count: int):
+        """Photons [first, first + count) of the emission's global sequence
+        (rl_emit_photons_range), deposited into every photonmap."""
+        ds = self.device_scene(scene)
+        f = scene.flat
+        maps = [m._device for m in f.photonmaps]
+        check(lib().rl_emit_photons_range(ds.handle, _map_array(maps), len(maps), C.c_void_p(f.lights.ctypes.data),
+                                          len(f.lights), settings.photon_pass_count, settings.photon_bounce_count,
+                                          settings.photon_energy_threshold, settings.photon_max_distance, seed,
+                                          first, count, None, self.stream))
+
+    def gather_photons(self, scene: Scene, settings: IndirectLightSettings):
+        """Photonmap::gather on every photonmap (Relight.cpp:250-254)."""
+        for m in scene.flat.photonmaps:
+            check(lib().rl_photonmap_gather(m._device.handle, settings.final_gather_radius, self.stream))
+
+    def radiosity_step(self, r0, r1, row, cols, vals, E, rho, B, B_next):
+        """Rows [r0, r1) of one Jacobi step (rl_radiosity_step); torch
+        tensors on the device, [n][3] iterates."""
+        check(lib().rl_radiosity_step(int(r0), int(r1), C.c_void_p(row.data_ptr()), C.c_void_p(cols.data_ptr()),
+                                      C.c_void_p(vals.data_ptr()), C.c_void_p(E.data_ptr()),
+                                      C.c_void_p(rho.data_ptr()), C.c_void_p(B.data_ptr()),
+                                      C.c_void_p(B_next.data_ptr()), self.stream))
 
 
 def lumels(lightmap: Lightmap, stream=None):

@@ -18,8 +18,10 @@ Each pass shards its units with no exchange until the step that needs one:
   radiosity     rank r steps its block of rows of B' = E + rho .* (F B); one
                 all-gather of B per iteration.
 
-The functions take the collective and the compute as arguments, so the same
-code drives the CUDA library under NCCL and the CPU oracle under gloo.
+The sharded_* functions take the collective and the compute as arguments;
+the *_distributed functions take an engine object (the CUDA Relight, or an
+oracle adapter in the tests), so the same code drives the CUDA library
+under NCCL and the CPU oracle under gloo.
 """
 from __future__ import annotations
 
@@ -88,33 +90,101 @@ def map_tensor(dev_map, field: str):
     return torch.as_tensor(_CudaArray(ptrs[field], (n, 3), "<f4"), device="cuda")
 
 
-def emit_photons_distributed(relight, scene, settings, seed: int, group=None) -> None:
-    """Relight::emitPhotons for one bake split over the ranks of `group`
-    (NCCL): every rank ends with the full, gathered photonmaps."""
-    import ctypes as C
-
+def _group_info(group):
     import torch.distributed as dist
+    return dist.get_rank(group), dist.get_world_size(group)
 
-    from . import _abi
-    from .device import _map_array
 
-    rank, world = dist.get_rank(group), dist.get_world_size(group)
-    ds = relight.device_scene(scene)
-    f = scene.flat
-    maps = [m._device for m in f.photonmaps]
-    lights = C.c_void_p(f.lights.ctypes.data)
-    total = C.c_int64()
-    _abi.check(_abi.lib().rl_photon_count(lights, len(f.lights), settings.photon_pass_count, C.byref(total)))
-    L = _abi.lib()
+def _all_reduce_sum(group):
+    import torch.distributed as dist
+    return lambda t: dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
 
-    def emit_range(first, count):
-        _abi.check(L.rl_emit_photons_range(ds.handle, _map_array(maps), len(maps), lights, len(f.lights),
-                                           settings.photon_pass_count, settings.photon_bounce_count,
-                                           settings.photon_energy_threshold, settings.photon_max_distance, seed,
-                                           first, count, None, relight.stream))
 
-    accs = [map_tensor(m, "color") for m in maps] + [map_tensor(m, "photons") for m in maps]
-    sharded_photons(emit_range, accs, total.value, rank, world,
-                    lambda t: dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group))
-    for m in maps:
-        _abi.check(L.rl_photonmap_gather(m.handle, settings.final_gather_radius, relight.stream))
+class _on_stream:
+    """Run the collectives on the engine's stream (torch's current stream
+    when it has none), so they order with its kernels."""
+
+    def __init__(self, engine):
+        self.s = engine.torch_stream() if hasattr(engine, "torch_stream") else None
+
+    def __enter__(self):
+        if self.s is not None:
+            import torch
+            self.ctx = torch.cuda.stream(self.s)
+            self.ctx.__enter__()
+        return self
+
+    def __exit__(self, *a):
+        if self.s is not None:
+            self.ctx.__exit__(*a)
+
+
+# An engine provides: photon_total, emit_photon_range, photon_accumulators,
+# gather_photons, color_tensor, bake_indirect_light (Relight's signature,
+# with iterator and seed), radiosity_step and, for CUDA, torch_stream.
+# relight_b200.device.Relight is the CUDA engine (NCCL); the tests drive the
+# same functions with the oracle under gloo.
+
+def emit_photons_distributed(engine, scene, settings, seed: int, group=None) -> None:
+    """Relight::emitPhotons for one bake split over the ranks of `group`:
+    every rank traces its share of the photon sequence, the photonmap
+    accumulators are summed over ranks, and every rank gathers its (now
+    complete) photonmaps."""
+    rank, world = _group_info(group)
+    total = engine.photon_total(scene, settings)
+    with _on_stream(engine):
+        sharded_photons(lambda first, count: engine.emit_photon_range(scene, settings, seed, first, count),
+                        engine.photon_accumulators(scene), total, rank, world, _all_reduce_sum(group))
+    engine.gather_photons(scene, settings)
+
+
+def bake_indirect_distributed(engine, scene, mesh, settings, seed: int, group=None) -> None:
+    """Relight::bakeIndirectLight over the whole lightmap of `mesh`, split
+    over the ranks of `group`: rank r bakes LumelBakeIterator(r, world) into
+    zeroed colours, the contributions are summed over ranks (one non-zero
+    term per lumel, so exactly), and every rank adds its base colours.
+    Every lumel gets base + contribution, the single-GPU bake's own float
+    addition: the same bits on every rank as one GPU baking alone."""
+    from .device import LumelBakeIterator
+    rank, world = _group_info(group)
+    color = engine.color_tensor(mesh.lightmap)
+    with _on_stream(engine):
+        base = color.clone()
+        color.zero_()
+    sharded_final_gather(
+        lambda first, step: engine.bake_indirect_light(scene, mesh, None, settings, LumelBakeIterator(first, step),
+                                                       seed=seed),
+        color, base, rank, world, lambda t: _run_on(engine, _all_reduce_sum(group), t),
+        lambda b, c: _run_on(engine, lambda t: t.add_(b), c))
+
+
+def _run_on(engine, fn, t):
+    with _on_stream(engine):
+        return fn(t)
+
+
+def radiosity_solve_distributed(engine, n: int, row, cols, vals, E, rho, iters: int, B_out, group=None) -> None:
+    """The 50-iteration Jacobi solve with rows sharded over the ranks of
+    `group`: each iteration, rank r steps its block of rows
+    (engine.radiosity_step) and one all-gather assembles B on every rank.
+    Tensors are [n][3] (colours) on the engine's device; B_out receives B."""
+    import torch
+    import torch.distributed as dist
+    rank, world = _group_info(group)
+    r0, r1 = row_block(n, rank, world)
+    blocks = [row_block(n, q, world) for q in range(world)]
+    rows = max(b - a for a, b in blocks)
+    with _on_stream(engine):
+        B = E.clone()
+        Bn = torch.empty_like(E)
+        local = torch.zeros((rows, 3), dtype=E.dtype, device=E.device)
+        gathered = torch.empty((world * rows, 3), dtype=E.dtype, device=E.device)
+    for _ in range(iters):
+        engine.radiosity_step(r0, r1, row, cols, vals, E, rho, B, Bn)
+        with _on_stream(engine):
+            local[:r1 - r0].copy_(Bn[r0:r1])
+            dist.all_gather(list(gathered.view(world, rows, 3).unbind(0)), local, group=group)
+            for q, (a, b) in enumerate(blocks):
+                B[a:b].copy_(gathered[q * rows:q * rows + (b - a)])
+    with _on_stream(engine):
+        B_out.copy_(B)

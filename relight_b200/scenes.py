@@ -3,6 +3,9 @@
   room_scene      10x10x10 closed room (6 inward quads) + N axis-aligned boxes,
                   one mesh, one lightmap; point, spot (45 deg cone) and 1x1
                   area (16-triangle) lights.  The direct-light + AO workload.
+                  textured=True gives the walls plain coloured materials and
+                  the boxes an RGBA texture with cut-out texels (alpha <= 0.1),
+                  so shadow rays take Relight's alpha re-trace.
   terrain_scene   256x256-vertex fBm heightfield (amplitude 5) split into 2x2
                   tiles (16-bit index limit) + 2,000 boxes; per-vertex albedo in
                   [0.2, 0.8]; one sun + 4 point lights; one shared 1024^2
@@ -26,7 +29,7 @@ from typing import List
 import numpy as np
 
 from .api import (AmbientOcclusionSettings, IndirectLightSettings, Light, LinearLightAttenuation, Material, Mesh,
-                  Photonmap, Lightmap, Scene)
+                  Photonmap, Lightmap, Scene, Texture, TexturedMaterial)
 
 F32 = np.float32
 
@@ -85,8 +88,23 @@ class RoomWorkload:
     ao: AmbientOcclusionSettings
 
 
+def alpha_texture(size: int = 16, seed: int = 5) -> Texture:
+    """An RGBA texture of random colours whose alpha is a checkerboard of
+    4x4-texel cells: cut-out cells hold alpha 0 or 25 (25/255 <= 0.1, so
+    Relight's HitUseAlpha passes through them) and opaque cells 26 (just
+    above 0.1), 128 or 255."""
+    rng = np.random.default_rng(seed)
+    px = np.zeros((size, size, 4), np.uint8)
+    px[..., :3] = rng.integers(40, 256, (size, size, 3))
+    y, x = np.mgrid[0:size, 0:size]
+    cut = ((x // 4 + y // 4) % 2) == 0
+    px[..., 3] = np.where(cut, rng.choice([0, 25], (size, size)), rng.choice([26, 128, 255], (size, size)))
+    return Texture.create(size, size, 4, px.reshape(-1))
+
+
 def room_scene(seed: int = 1, size: int = 256, n_boxes: int = 8, room: float = 10.0,
-               area_light: bool = True, spot_light: bool = True, material=None) -> RoomWorkload:
+               area_light: bool = True, spot_light: bool = True, material=None,
+               textured: bool = False) -> RoomWorkload:
     rng = np.random.default_rng(seed)
     faces = _box_faces((0, 0, 0), (room, room, room), inward=True)
     for _ in range(n_boxes):
@@ -95,10 +113,26 @@ def room_scene(seed: int = 1, size: int = 256, n_boxes: int = 8, room: float = 1
         faces += _box_faces(c - s / 2, c + s / 2)
     cols = int(math.ceil(math.sqrt(len(faces))))
     cell = size // cols
+    mats = [material] * len(faces)
+    uv0s = [None] * len(faces)
+    if textured:
+        # own generator: the geometry stays that of the untextured room
+        trng = np.random.default_rng(seed + 1000)
+        tex = alpha_texture(16, seed + 2000)
+        for k in range(6):
+            mats[k] = Material(trng.uniform(0.3, 0.9, 3))
+        box_mats = [TexturedMaterial(tex, trng.uniform(0.5, 1.0, 3)) for _ in range(3)]
+        for k in range(6, len(faces)):
+            mats[k] = box_mats[k % 3]
+            # diffuse uvs over 1 or 2 texture periods (wrap), some starting
+            # below 0 (Texture::colorAt's out-of-range colour)
+            span = 1.0 + (k % 2)
+            u0, v0 = (-0.5, -0.25) if k % 5 == 0 else (0.0, 0.0)
+            uv0s[k] = np.array([[u0, v0], [u0 + span, v0], [u0 + span, v0 + span], [u0, v0 + span]], F32)
     src = Mesh.create()
     for k, (corners, n) in enumerate(faces):
         pos, nrm, uv, idx = _quad(corners, n, _cell_rect(k, cols, cell, size, size))
-        src.add_faces(pos, nrm, None, uv, idx, material)
+        src.add_faces(pos, nrm, uv0s[k], uv, idx, mats[k])
     scene = Scene()
     scene.begin()
     mesh = scene.add_mesh(src)

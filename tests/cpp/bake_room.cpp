@@ -1,107 +1,22 @@
-// A Relight C++ program, unchanged apart from the include: builds a closed
+// A Relight-style C++ program (the scene comes from room_scene.h): builds a closed
 // room with a box, a point, a spot and a 2-triangle area light, bakes direct
 // light, AO, photons and the final gather through relight::Relight, and
 // writes the lightmap (flags + RGB) after AO and after the final gather.
 //
 //   bake_room <out-prefix>    -> <out-prefix>.direct_ao.bin, <out-prefix>.final.bin
-#include <relight/Relight.h>
-
-#include <cstdio>
-#include <string>
+#include "room_scene.h"
 
 using namespace relight;
-
-static void quad(VertexBuffer& vb, IndexBuffer& ib, Vec3 p0, Vec3 p1, Vec3 p2, Vec3 p3, Vec3 n, float u0, float v0,
-                 float u1, float v1) {
-    Index base = (Index)vb.size();
-    Vec3 ps[4] = {p0, p1, p2, p3};
-    Uv uvs[4] = {Uv(u0, v0), Uv(u1, v0), Uv(u1, v1), Uv(u0, v1)};
-    for (int k = 0; k < 4; k++) {
-        Vertex v;
-        v.position = ps[k];
-        v.normal = n;
-        v.uv[Vertex::Lightmap] = uvs[k];
-        vb.push_back(v);
-    }
-    Index idx[6] = {0, 1, 2, 0, 2, 3};
-    for (Index i : idx) ib.push_back((Index)(base + i));
-}
-
-// An axis-aligned box: lo/hi corners, inward or outward normals, chart cells
-// starting at `cell` in a 4x4 grid of the unit uv square.
-static void box(VertexBuffer& vb, IndexBuffer& ib, Vec3 lo, Vec3 hi, bool inward, int cell) {
-    for (int axis = 0; axis < 3; axis++) {
-        int i = (axis + 1) % 3, j = (axis + 2) % 3;
-        for (int side = 0; side < 2; side++) {
-            float c = side ? (&hi.x)[axis] : (&lo.x)[axis];
-            Vec3 n;
-            (&n.x)[axis] = (side ? 1.0f : -1.0f) * (inward ? -1.0f : 1.0f);
-            Vec3 p[4];
-            int ab[4][2] = {{0, 0}, {1, 0}, {1, 1}, {0, 1}};
-            for (int k = 0; k < 4; k++) {
-                (&p[k].x)[axis] = c;
-                (&p[k].x)[i] = ab[k][0] ? (&hi.x)[i] : (&lo.x)[i];
-                (&p[k].x)[j] = ab[k][1] ? (&hi.x)[j] : (&lo.x)[j];
-            }
-            int cx = cell % 4, cy = cell / 4;
-            cell++;
-            quad(vb, ib, p[0], p[1], p[2], p[3], n, (cx * 16 + 1) / 64.0f, (cy * 16 + 1) / 64.0f,
-                 (cx * 16 + 15) / 64.0f, (cy * 16 + 15) / 64.0f);
-        }
-    }
-}
-
-static bool dump(Lightmap* lm, const std::string& path) {
-    FILE* f = fopen(path.c_str(), "wb");
-    if (!f) return false;
-    Lumel* l = lm->lumels();
-    int n = lm->width() * lm->height();
-    for (int i = 0; i < n; i++) fwrite(&l[i].m_flags, sizeof(int), 1, f);
-    for (int i = 0; i < n; i++) fwrite(&l[i].m_color, sizeof(float), 3, f);
-    fclose(f);
-    return true;
-}
+using namespace room_example;
 
 int main(int argc, char** argv) {
     std::string out = argc > 1 ? argv[1] : "bake_room";
-    Relight* relight = Relight::create();
-    Scene* scene = relight->createScene();
-    scene->begin();
-
-    Material* grey = new Material(Rgb(0.7f, 0.7f, 0.7f));
-    Material* red = new Material(Rgb(0.8f, 0.2f, 0.2f));
-    VertexBuffer vb;
-    IndexBuffer ib;
-    box(vb, ib, Vec3(0, 0, 0), Vec3(10, 10, 10), true, 0);
-    Mesh* room = Mesh::create();
-    room->addFaces(vb, ib, grey);
-    vb.clear();
-    ib.clear();
-    box(vb, ib, Vec3(3, 0, 4), Vec3(6, 3, 6), false, 6);
-    Mesh* crate = Mesh::create();
-    crate->addFaces(vb, ib, red);
-
-    Mesh* r = scene->addMesh(room, Matrix4());
-    Mesh* c = scene->addMesh(crate, Matrix4());
-    Lightmap* lm = relight->createLightmap(64, 64);
-    Photonmap* pm = relight->createPhotonmap(64, 64);
-    lm->addMesh(r); lm->addMesh(c);
-    pm->addMesh(r); pm->addMesh(c);
-
-    scene->addLight(Light::createPointLight(Vec3(5, 9, 5), 10.0f, Rgb(1, 1, 1), 1.0f));
-    scene->addLight(Light::createSpotLight(Vec3(2, 8, 2), Vec3(0.5f, -0.7f, 0.5f), 0.9238795f, 10.0f,
-                                           Rgb(1.0f, 0.9f, 0.7f), 1.0f));
-    VertexBuffer lv;
-    IndexBuffer li;
-    quad(lv, li, Vec3(-0.5f, 0, -0.5f), Vec3(0.5f, 0, -0.5f), Vec3(0.5f, 0, 0.5f), Vec3(-0.5f, 0, 0.5f),
-         Vec3(0, -1, 0), 0, 0, 1, 1);
-    Mesh* lightMesh = Mesh::create();
-    lightMesh->addFaces(lv, li);
-    Light* area = Light::createAreaLight(lightMesh, Vec3(7, 9, 7), Rgb(0.8f, 0.9f, 1.0f), 1.0f);
-    area->setAttenuation(new LinearLightAttenuation(area, 10.0f));
-    scene->addLight(area);
-    if (scene->end() != RelightSuccess) return 2;
-
+    RoomScene rs;
+    if (!build_room(rs)) return 2;
+    Relight* relight = rs.relight;
+    Scene* scene = rs.scene;
+    Mesh* r = rs.room;
+    Lightmap* lm = rs.lightmap;
     if (relight->bakeDirectLight(scene, r, nullptr) != RelightSuccess) return 3;
     AmbientOcclusionSettings ao = AmbientOcclusionSettings::draft(0.8f, 2.0f);
     ao.m_samples = 16;

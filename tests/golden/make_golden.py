@@ -10,6 +10,10 @@ Every fixture is a deterministic output of the reference's code:
                     scene's transformed vertices and area-light samples.
   trace_room.npz    rt::Embree::traceSegment results for 4,000 seeded segments
                     (hit, point, normal, rgba, lightmap uv, mesh) with HitAll.
+  textured_room48.npz  the textured room (RGBA texture with cut-out texels on
+                    the boxes, coloured walls) at 48x48: traceSegment with
+                    HitAll and with HitAll | HitUseAlpha on 6,000 segments,
+                    and Relight::bakeDirectLight colours (alpha shadow rays).
   gather.npz        Photonmap::gather(7) over seeded photon accumulators on
                     square and non-square maps.
   ff_room24.npz     RadiosityBuilder::build(0.1) on a 24x24-texel
@@ -177,6 +181,18 @@ def main():
     r = ref.trace_segments(seg, 15)
     np.savez_compressed(os.path.join(HERE, "trace_room.npz"), seg=seg, **r)
     out["trace_room"] = int(r["hit"].sum())
+    # textured room: Texture::colorAt and the HitUseAlpha re-trace
+    w = scenes.room_scene(size=48, textured=True)
+    ref = RefScene(w.scene)
+    seg = segments(w.scene.flat, 6000, 13)
+    t = {"seg": seg}
+    for flags in (15, 31):
+        r = ref.trace_segments(seg, flags)
+        t.update({f"{k}_{flags}": v for k, v in r.items()})
+    ref.lib.ref_bake_direct(ref.h, ref.mesh(w.mesh), 0, 0, 1)
+    lm = ref.lumels(w.lightmap)
+    np.savez_compressed(os.path.join(HERE, "textured_room48.npz"), color=lm.color, flags=lm.flags, **t)
+    out["textured_room48"] = int((lm.color.sum(1) > 0).sum())
     # Photonmap::gather
     g = {}
     for (W, H) in ((48, 48), (56, 40), (40, 56)):

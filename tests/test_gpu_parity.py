@@ -43,12 +43,14 @@ def _segments(rng, lo, hi, n):
 
 
 @pytest.mark.parametrize("builder", [0, 1])
-@pytest.mark.parametrize("which", ["room", "terrain"])
+@pytest.mark.parametrize("which", ["room", "terrain", "textured"])
 def test_trace_segments_match_oracle(cuda, which, builder):
+    """Segments through the C ABI; "textured" adds RGBA textures with cut-out
+    texels (Texture::colorAt and the HitUseAlpha re-trace)."""
     import torch
     from relight_b200 import _abi
-    if which == "room":
-        w = scenes.room_scene(size=64)
+    if which in ("room", "textured"):
+        w = scenes.room_scene(size=64, textured=which == "textured")
         scene = w.scene
     else:
         w = scenes.terrain_scene(verts=48, n_boxes=60, size=128, tiles=2)
@@ -107,6 +109,59 @@ def test_direct_light_bit_exact(cuda):
     orc.bake_direct(lm)
     assert (g["color"].sum(1) > 0).sum() > 1000
     assert np.array_equal(g["color"], lm.color)
+
+
+def test_textured_direct_light_and_ao_bit_exact(cuda):
+    """Direct light whose shadow rays pass through cut-out texels (alpha <=
+    0.1, re-traced 1 unit further on), then AO, on the textured room."""
+    w = scenes.room_scene(size=128, textured=True)
+    rl = _relight()
+    rl.bake_direct_light(w.scene, w.mesh, None)
+    g_direct = _lumels(w.lightmap)["color"].copy()
+    rl.bake_ambient_occlusion(w.scene, w.mesh, None, w.ao, seed=12)
+    g = _lumels(w.lightmap)
+    assert w.scene._device.status() == 0
+    orc = Oracle(w.scene.flat).bind_scene(w.scene)
+    lm = orc.maps()[0]
+    orc.bake_direct(lm)
+    assert (lm.color.sum(1) > 0).sum() > 1000
+    assert np.array_equal(g_direct, lm.color)
+    # the cut-out texels changed the shadows (the same room untextured differs)
+    wu = scenes.room_scene(size=128)
+    ou = Oracle(wu.scene.flat).bind_scene(wu.scene)
+    lu = ou.maps()[0]
+    ou.bake_direct(lu)
+    assert np.any(lu.color != lm.color, 1).sum() > 100
+    orc.bake_ao(lm, w.ao.samples, w.ao.occluded_fraction, w.ao.max_distance, w.ao.exponent, 12)
+    assert np.array_equal(g["color"], lm.color)
+
+
+def test_textured_photon_bounce_colours(cuda):
+    """Photon deposits coloured by Face::colorAt through the texture
+    (baker/Photons.cpp:116-119, hit.m_color)."""
+    from relight_b200.api import Photonmap, Scene
+    w = scenes.room_scene(size=64, textured=True)
+    sc = Scene()
+    sc.begin()
+    inst = sc.add_mesh(w.mesh.source[0])
+    pm = Photonmap(64, 64)
+    pm.add_mesh(inst)
+    for l in w.scene.lights:
+        sc.add_light(l)
+    sc.end()
+    st = scenes.IndirectLightSettings(1, 3, 0.05, 20.0, 8, 20.0, 7)
+    rl = _relight()
+    rl.emit_photons(sc, st, seed=8)
+    g = _lumels(pm)
+    orc = Oracle(sc.flat).bind_scene(sc)
+    opm = orc.maps("photonmap")[0]
+    stored = orc.emit_photons([opm], 1, 3, 0.05, 20.0, 8)
+    assert stored > 1000
+    assert np.array_equal(g["photons"], opm.photons)
+    np.testing.assert_allclose(g["color"], opm.color, rtol=1e-5, atol=1e-6)
+    # textured albedo: deposits on the boxes are not grey
+    c = g["color"][g["photons"] > 0]
+    assert np.abs(c[:, 0] - c[:, 1]).max() > 1e-3
 
 
 def test_direct_light_iterator_subset(cuda):
@@ -458,11 +513,17 @@ def test_photon_shares_sum_to_the_full_emission(cuda):
     np.testing.assert_allclose(a["color"] + b["color"], full["color"], rtol=1e-5, atol=1e-6)
 
 
-def test_distributed_emission_on_one_rank_matches(cuda):
+def test_distributed_bake_on_one_rank_matches(cuda):
+    """The split bake's CUDA engine under NCCL with one rank (the only
+    multi-GPU path a one-GPU box can run): the photon split equals the
+    unsplit emission (counts exact, the gather within the atomics'
+    tolerance); the final-gather split and the row-sharded radiosity solve
+    give the single-GPU bake's bits."""
     import os
     import socket
+    import torch
     import torch.distributed as dist
-    from relight_b200 import parallel
+    from relight_b200 import _abi, parallel
     with socket.socket() as s:
         s.bind(("127.0.0.1", 0))
         port = s.getsockname()[1]
@@ -476,6 +537,33 @@ def test_distributed_emission_on_one_rank_matches(cuda):
         a, b = _lumels(w1.photonmap), _lumels(w2.photonmap)
         assert np.array_equal(a["photons"], b["photons"])
         np.testing.assert_allclose(a["gathered"], b["gathered"], rtol=1e-4, atol=1e-6)
+        # final gather: the same photonmap and base colours, split and unsplit
+        rl.bake_direct_light(w1.scene, w1.meshes[0], None)
+        base = _lumels(w1.lightmap)["color"].copy()
+        rl.bake_indirect_light(w1.scene, w1.meshes[0], None, w1.settings, seed=9)
+        want = _lumels(w1.lightmap)["color"].copy()
+        w1.lightmap._device.upload(color=base)
+        parallel.bake_indirect_distributed(rl, w1.scene, w1.meshes[0], w1.settings, seed=9)
+        got = _lumels(w1.lightmap)["color"]
+        assert (want != base).any()
+        assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+        # radiosity: rows sharded over one rank == rl_radiosity_solve
+        n, per = 5000, 24
+        rng = np.random.default_rng(8)
+        cols = np.sort(rng.integers(0, n, (n, per)), axis=1).astype(np.int32).reshape(-1)
+        vals = rng.random(n * per).astype(np.float32) * np.float32(0.9 / per)
+        row = np.arange(n + 1, dtype=np.int64) * per
+        rho = rng.uniform(0.3, 0.9, (n, 3)).astype(np.float32)
+        E = np.zeros((n, 3), np.float32)
+        E[rng.choice(n, 16, replace=False)] = 1.0
+        dr, dc, dv, dE, drho = (_dev(x, torch) for x in (row, cols, vals, E, rho))
+        want = torch.zeros((n, 3), dtype=torch.float32, device="cuda")
+        _abi.check(_abi.lib().rl_radiosity_solve(n, dr.data_ptr(), dc.data_ptr(), dv.data_ptr(), dE.data_ptr(),
+                                                 drho.data_ptr(), 50, want.data_ptr(), None))
+        got = torch.zeros_like(want)
+        parallel.radiosity_solve_distributed(rl, n, dr, dc, dv, dE, drho, 50, got)
+        torch.cuda.synchronize()
+        assert torch.equal(got.view(torch.int32), want.view(torch.int32))
     finally:
         dist.destroy_process_group()
 

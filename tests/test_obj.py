@@ -25,7 +25,8 @@ sys.path.insert(0, os.path.join(HERE, "golden"))
 from make_golden import obj_texts  # noqa: E402
 
 GOLD = np.load(os.path.join(HERE, "golden", "obj.npz"))
-REF_DATA = "/root/reference/data"
+_REF_ROOT = ob.reference_root()
+REF_DATA = os.path.join(_REF_ROOT, "data") if _REF_ROOT else None
 
 
 def _load(path):
@@ -93,7 +94,7 @@ def test_obj_undefined_inputs_are_errors(tmp_path):
         assert "out of range" in _abi.last_error()
 
 
-@pytest.mark.skipif(not (os.path.exists(ob.REF_LIB) and os.path.isdir(REF_DATA)),
+@pytest.mark.skipif(not (os.path.exists(ob.REF_LIB) and REF_DATA and os.path.isdir(REF_DATA)),
                     reason="reference build or its sample meshes absent")
 def test_obj_matches_reference_sample_meshes():
     L = ob.ref_lib()

@@ -70,6 +70,61 @@ def test_trace_segments_match_golden():
         assert np.array_equal(r[f][m], g[f][m]), f
 
 
+# fields traceSegment fills for each flag set (rt/Embree.cpp:167-174)
+_TRACE_FIELDS = {15: ("point", "normal", "rgba", "uv", "mesh"), 31: ("point", "normal", "rgba", "uv", "mesh")}
+
+
+def test_textured_alpha_trace_and_direct_match_golden():
+    """RGBA textures (Texture::colorAt: nearest texel, wrap, out-of-range
+    colour) and the HitUseAlpha re-trace through cut-out texels
+    (rt/Embree.cpp:157-165): traceSegment with and without HitUseAlpha, and
+    direct light whose shadow rays pass through alpha <= 0.1."""
+    from golden.make_golden import segments
+    g = golden("textured_room48.npz")
+    w = scenes.room_scene(size=48, textured=True)
+    orc = Oracle(w.scene.flat).bind_scene(w.scene)
+    seg = segments(w.scene.flat, 6000, 13)
+    assert np.array_equal(seg, g["seg"])
+    for flags in (15, 31):
+        r = orc.trace_segments(seg, flags)
+        assert np.array_equal(r["hit"], g[f"hit_{flags}"])
+        m = g[f"hit_{flags}"] > 0
+        for f in _TRACE_FIELDS[flags]:
+            assert np.array_equal(r[f][m], g[f"{f}_{flags}"][m]), (flags, f)
+    # the alpha re-trace changed hundreds of results, and textures coloured them
+    moved = (g["hit_15"] != g["hit_31"]) | np.any(g["point_15"] != g["point_31"], 1)
+    assert moved.sum() > 100
+    m = g["hit_15"] > 0
+    assert len(np.unique(g["rgba_15"][m], axis=0)) > 50
+    lm = orc.maps()[0]
+    assert np.array_equal(lm.flags, g["flags"])
+    orc.bake_direct(lm)
+    assert (g["color"].sum(1) > 0).sum() > 300
+    assert np.array_equal(lm.color, g["color"])
+
+
+@needs_ref
+def test_textured_alpha_matches_reference():
+    """The same on a larger textured room, live against the reference."""
+    from golden.make_golden import segments
+    w = scenes.room_scene(size=96, textured=True, seed=4)
+    ref = RefScene(w.scene)
+    orc = Oracle(w.scene.flat).bind_scene(w.scene)
+    seg = segments(w.scene.flat, 20000, 3)
+    for flags in (15, 31):
+        r, o = ref.trace_segments(seg, flags), orc.trace_segments(seg, flags)
+        assert np.array_equal(r["hit"], o["hit"])
+        m = r["hit"] > 0
+        for f in _TRACE_FIELDS[flags]:
+            assert np.array_equal(r[f][m], o[f][m]), (flags, f)
+    ref.lib.ref_bake_direct(ref.h, ref.mesh(w.mesh), 0, 0, 1)
+    lm = orc.maps()[0]
+    orc.bake_direct(lm)
+    r = ref.lumels(w.lightmap)
+    assert (r.color.sum(1) > 0).sum() > 1000
+    assert np.array_equal(lm.color, r.color)
+
+
 @pytest.mark.parametrize("W,H", [(48, 48), (56, 40), (40, 56)])
 def test_photon_gather_matches_golden(W, H):
     from golden.make_golden import gather_inputs

@@ -1,5 +1,6 @@
 """The multi-GPU split of one bake (relight_b200/parallel.py), run as two gloo
-ranks on CPU with the oracle as the compute engine: photon shares
+ranks on CPU with the oracle as the compute engine, through the same
+*_distributed functions the CUDA engine runs under NCCL: photon shares
 all-reduced, interleaved final-gather lumels all-reduced, row-sharded
 Jacobi all-gathered — each compared with the unsplit single-process result."""
 import os
@@ -39,58 +40,65 @@ def _csr(n, seed):
     return row, cols, vals, E, rho
 
 
+class OracleEngine:
+    """relight_b200.parallel's engine interface over the oracle (CPU):
+    torch tensors that share the oracle's numpy lumel arrays."""
+
+    def __init__(self, scene):
+        from oracle_bind import Oracle
+        self.orc = Oracle(scene.flat).bind_scene(scene)
+        self.lms = dict(zip(map(id, scene.flat.lightmaps), self.orc.maps()))
+        self.pms = dict(zip(map(id, scene.flat.photonmaps), self.orc.maps("photonmap")))
+
+    def photon_total(self, scene, st):
+        return int(sum(int(l["intensity"] * 25000) for l in scene.flat.lights if l["emitter"])) * st.photon_pass_count
+
+    def emit_photon_range(self, scene, st, seed, first, count):
+        self.orc.emit_photons_range(list(self.pms.values()), st.photon_pass_count, st.photon_bounce_count,
+                                    st.photon_energy_threshold, st.photon_max_distance, seed, first, count)
+
+    def photon_accumulators(self, scene):
+        pms = list(self.pms.values())
+        return [torch.from_numpy(p.color) for p in pms] + [torch.from_numpy(p.photons) for p in pms]
+
+    def gather_photons(self, scene, st):
+        for p in self.pms.values():
+            self.orc.gather(p, st.final_gather_radius)
+
+    def color_tensor(self, lightmap):
+        return torch.from_numpy(self.lms[id(lightmap)].color)
+
+    def bake_indirect_light(self, scene, mesh, progress, st, iterator, seed):
+        self.orc.bake_indirect(self.lms[id(mesh.lightmap)], list(self.pms.values()), st.final_gather_samples,
+                               st.final_gather_distance, st.sky_color, st.ambient_color, seed, iterator.first,
+                               iterator.step)
+
+    def radiosity_step(self, r0, r1, row, cols, vals, E, rho, B, B_next):
+        x = B.numpy().astype(np.float64)
+        r, c, v = row.numpy(), cols.numpy(), vals.numpy().astype(np.float64)
+        for i in range(r0, r1):
+            s = (v[r[i]:r[i + 1], None] * x[c[r[i]:r[i + 1]]]).sum(0)
+            B_next[i] = torch.from_numpy((E[i].numpy() + rho[i].numpy() * s).astype(np.float32))
+
+
 def _worker(rank, world, port, outdir):
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
-        from oracle_bind import Oracle
         w = _scene()
         st = w.settings
-        orc = Oracle(w.scene.flat).bind_scene(w.scene)
-        pm = orc.maps("photonmap")[0]
-        total = int(sum(int(l["intensity"] * 25000) for l in w.scene.flat.lights if l["emitter"])) * \
-            st.photon_pass_count
-
-        def emit_range(first, count):
-            orc.emit_photons_range([pm], st.photon_pass_count, st.photon_bounce_count, st.photon_energy_threshold,
-                                   st.photon_max_distance, 7, first, count)
-
-        parallel.sharded_photons(emit_range, [torch.from_numpy(pm.color), torch.from_numpy(pm.photons)], total,
-                                 rank, world, lambda t: dist.all_reduce(t, op=dist.ReduceOp.SUM))
-        orc.gather(pm, st.final_gather_radius)
-        lm = orc.maps()[0]
-        base = np.full_like(lm.color, 0.25)
-        contrib = lm.copy()
-        contrib.color[:] = 0
-
-        def bake_subset(first, step):
-            orc.bake_indirect(contrib, [pm], st.final_gather_samples, st.final_gather_distance, st.sky_color,
-                              st.ambient_color, 13, first, step)
-
-        parallel.sharded_final_gather(bake_subset, torch.from_numpy(contrib.color), base, rank, world,
-                                      lambda t: dist.all_reduce(t, op=dist.ReduceOp.SUM),
-                                      lambda b, c: np.add(b, c.numpy(), out=b))
-        row, cols, vals, E, rho = _csr(300, 3)
-        B = torch.from_numpy(E.copy())
-        r0, r1 = parallel.row_block(300, rank, world)
-        local = torch.zeros((r1 - r0, 3), dtype=torch.float32)
-
-        def step_rows(a, b, Bin, out):
-            x = Bin.numpy().astype(np.float64)
-            for i in range(a, b):
-                s = (vals[row[i]:row[i + 1], None].astype(np.float64) * x[cols[row[i]:row[i + 1]]]).sum(0)
-                out[i - a] = torch.from_numpy((E[i] + rho[i] * s).astype(np.float32))
-
-        def all_gather_rows(out, Bfull):
-            sizes = [parallel.row_block(300, r, world) for r in range(world)]
-            parts = [torch.zeros((q1 - q0, 3), dtype=torch.float32) for q0, q1 in sizes]
-            dist.all_gather(parts, out)
-            Bfull.copy_(torch.cat(parts))
-
-        parallel.sharded_jacobi(step_rows, B, local, 20, 300, rank, world, all_gather_rows)
+        eng = OracleEngine(w.scene)
+        parallel.emit_photons_distributed(eng, w.scene, st, 7)
+        pm = eng.pms[id(w.photonmap)]
+        lm = eng.lms[id(w.lightmap)]
+        lm.color[:] = 0.25
+        parallel.bake_indirect_distributed(eng, w.scene, w.meshes[0], st, 13)
+        row, cols, vals, E, rho = (torch.from_numpy(a) for a in _csr(300, 3))
+        B = torch.zeros((300, 3), dtype=torch.float32)
+        parallel.radiosity_solve_distributed(eng, 300, row, cols, vals, E, rho, 20, B)
         np.savez(os.path.join(outdir, f"rank{rank}.npz"), photons=pm.photons, color=pm.color, gathered=pm.gathered,
-                 fg=base, B=B.numpy())
+                 fg=lm.color, B=B.numpy())
     finally:
         dist.destroy_process_group()
 
@@ -104,13 +112,15 @@ def test_photon_share_partition():
             assert sum(c for _, c in shares) == total
 
 
-def test_two_gloo_ranks_reproduce_the_unsplit_bake():
+@pytest.mark.parametrize("world", [2, 3])
+def test_gloo_ranks_reproduce_the_unsplit_bake(world):
     from oracle_bind import Oracle, jacobi_f64
     with tempfile.TemporaryDirectory() as d:
-        mp.start_processes(_worker, args=(2, _free_port(), d), nprocs=2, join=True, start_method="spawn")
-        r = [np.load(os.path.join(d, f"rank{k}.npz")) for k in range(2)]
-    for f in ("photons", "color", "gathered", "fg", "B"):
-        assert np.array_equal(r[0][f], r[1][f]), f
+        mp.start_processes(_worker, args=(world, _free_port(), d), nprocs=world, join=True, start_method="spawn")
+        r = [np.load(os.path.join(d, f"rank{k}.npz")) for k in range(world)]
+    for k in range(1, world):
+        for f in ("photons", "color", "gathered", "fg", "B"):
+            assert np.array_equal(r[0][f], r[k][f]), f
     # unsplit, single process
     w = _scene()
     st = w.settings

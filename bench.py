@@ -567,7 +567,59 @@ def batch_arm(args):
     }
 
 
-DENOISE_METRIC = "lightmaps/s at equal per-texel RMSE vs an 8192 spp bake (final gather 16 spp + denoiser vs plain)"
+DENOISE_METRIC = ("lightmaps/s at equal per-texel RMSE vs the FP64 oracle (final gather 16 spp + denoiser vs "
+                  "plain)")
+TRUTH_TEXELS, TRUTH_SAMPLES = 4096, 16384
+
+
+def _fg_truth_part(recipe, gathered, texels, samples, seed):
+    """Oracle.fg_expect (FP64, uniform hemisphere) on some texels of a
+    rebuilt training scene whose photonmap holds the device's gathered
+    values.  Runs in a spawned worker process."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_bind as ob
+    from relight_b200 import scenes
+    wl = scenes.terrain_scene(**recipe)
+    orc = ob.Oracle(wl.scene.flat).bind_scene(wl.scene)
+    pm = orc.maps("photonmap")[0]
+    pm.gathered[:] = gathered
+    lm = orc.maps()[0]
+    st = wl.settings
+    return orc.fg_expect(lm, [pm], texels, samples, st.final_gather_distance, st.sky_color, st.ambient_color, seed)
+
+
+class FgTruth:
+    """The FP64 final-gather truth for denoise.evaluate: the oracle's
+    expectation over TRUTH_TEXELS seeded valid lumels at TRUTH_SAMPLES
+    samples, in two independent halves whose difference estimates the
+    truth's own noise variance (returned, and taken out of every RMSE).
+    Spread over a process pool started with spawn."""
+
+    def __init__(self, procs=None):
+        import multiprocessing as mp
+        self.procs = procs or max(1, os.cpu_count() or 1)
+        self.pool = mp.get_context("spawn").Pool(self.procs)
+        self.seconds = 0.0
+
+    def __call__(self, i, wl):
+        t0 = time.perf_counter()
+        pmap = wl.photonmap._device.download(fields=("gathered",))["gathered"]
+        flags = wl.lightmap._device.download(fields=("flags",))["flags"]
+        valid = np.nonzero(flags & 1)[0]
+        tex = np.sort(np.random.default_rng(1000 + i).choice(valid, min(TRUTH_TEXELS, len(valid)), replace=False))
+        chunks = np.array_split(tex.astype(np.int32), self.procs)
+        halves = []
+        for h in range(2):
+            jobs = [(wl.recipe, pmap, c, TRUTH_SAMPLES // 2, 7919 * (i + 1) + h) for c in chunks if len(c)]
+            halves.append(np.concatenate(self.pool.starmap(_fg_truth_part, jobs)))
+        expect = 0.5 * (halves[0] + halves[1])
+        noise_var = float(np.mean((halves[0] - halves[1]) ** 2) / 4.0)
+        self.seconds += time.perf_counter() - t0
+        return tex, expect, noise_var
+
+    def close(self):
+        self.pool.close()
+        self.pool.join()
 
 
 def train_denoiser(small):
@@ -599,15 +651,17 @@ def train_denoiser(small):
 def denoise_arm(args):
     """The denoiser end to end on one GPU: train it (train_denoiser), then on
     held-out 512^2 scenes compare RMSE and device time of 16 spp + denoiser
-    against plain final gathers of 16-1024 spp, all against an 8192 spp
-    bake."""
+    against plain final gathers of 16-1024 spp, all against the FP64 oracle
+    (FgTruth)."""
     import torch
     from relight_b200 import denoise as D
     torch.cuda.set_device(0)
     n_eval = 2 if SMALL else 4
+    truth = FgTruth()
     dn, info = train_denoiser(SMALL)
     with ClockSampler(0) as clocks:
-        ev = D.evaluate(dn, D.training_scenes(n_eval, seed=900, sides=(512,)), spp_lo=16)
+        ev = D.evaluate(dn, D.training_scenes(n_eval, seed=900, sides=(512,)), spp_lo=16, truth=truth)
+    truth.close()
     dn_ms = ev["denoised"][1]
     return {
         "metric": DENOISE_METRIC, "value": 1e3 / dn_ms, "unit": "lightmaps/s", "n_gpus": 1, "steps": n_eval,
@@ -615,7 +669,11 @@ def denoise_arm(args):
         "dtype": "bf16 (network), f32 (baker)", "data": "synthetic (seeded heightfield + boxes)",
         "config": {"workload": f"train on {info['patches']} 64x64 patches from {info['scenes']} scenes "
                                f"(256-512^2 lightmaps), evaluate on {n_eval} held-out 512^2 lightmaps",
-                   "spp_low": 16, "spp_train_target": 1024, "spp_ref": 8192},
+                   "spp_low": 16, "spp_train_target": 1024,
+                   "reference": (f"FP64 oracle final-gather expectation on {TRUTH_TEXELS} seeded valid lumels per "
+                                 f"scene, {TRUTH_SAMPLES} samples in two halves (their difference estimates the "
+                                 f"truth's noise variance, taken out of every RMSE)")},
+        "truth_s": truth.seconds,
         "plain_at_equal_rmse": {"spp": ev["equal_rmse_spp"], "extrapolated": ev["extrapolated"],
                                 "ms": ev["plain_ms_at_equal_rmse"], "lightmaps_per_s": 1e3 / ev["plain_ms_at_equal_rmse"]},
         "speedup_at_equal_rmse": ev["speedup"],
@@ -638,8 +696,8 @@ def serve_arm(args):
     the final gather denoised at completion.  Latency is arrival to colours
     in host memory on the host clock.  A closed-loop run (all requests
     queued at once) gives the saturated throughput, compared with the plain
-    per-job GPU path at the final-gather sample count whose RMSE (against an
-    8192 spp bake) equals the denoised one."""
+    per-job GPU path at the final-gather sample count whose RMSE (against the
+    FP64 oracle, FgTruth) equals the denoised one."""
     import torch
     from dataclasses import replace
     from relight_b200 import batch, denoise as D, scenes, serve
@@ -648,8 +706,10 @@ def serve_arm(args):
     n_scenes = 8 if SMALL else 32
     n_req = 40 if SMALL else 300
     t0 = time.perf_counter()
+    truth = FgTruth()
     dn, info = train_denoiser(SMALL)
-    ev = D.evaluate(dn, D.training_scenes(2 if SMALL else 3, seed=900, sides=(512,)), spp_lo=16)
+    ev = D.evaluate(dn, D.training_scenes(2 if SMALL else 3, seed=900, sides=(512,)), spp_lo=16, truth=truth)
+    truth.close()
     t_denoiser = time.perf_counter() - t0
     # the plain path runs at the equal-RMSE sample count, capped at the largest one measured
     eq_spp = int(round(min(ev["equal_rmse_spp"], max(ev["plain"]))))
@@ -698,7 +758,8 @@ def serve_arm(args):
                    "latency_clock": "host (arrival to colours in pinned host memory)"},
         "rates": rates, "saturated": sat,
         "denoiser": {"rmse_denoised_16spp": ev["denoised"][0], "max_err": ev["denoised_max_err"],
-                     "equal_rmse_spp": ev["equal_rmse_spp"], "extrapolated": ev["extrapolated"], "spp_ref": 8192,
+                     "equal_rmse_spp": ev["equal_rmse_spp"], "extrapolated": ev["extrapolated"],
+                     "reference": f"FP64 oracle, {TRUTH_TEXELS} lumels x {TRUTH_SAMPLES} samples per scene",
                      "rmse_plain": {str(k): v[0] for k, v in ev["plain"].items()}, "train": info,
                      "setup_s": t_denoiser},
         "plain_per_job_at_equal_rmse": {"fg_spp": eq_spp, "lightmaps_per_s": plain_lps, "requests": n_plain},

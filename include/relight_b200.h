@@ -540,7 +540,12 @@ int rl_radiosity_solve_noalloc(int n, const int64_t* d_row_ptr, const int32_t* d
      RL_TUNE_KNN_CELL: cell width of rl_photonmap_gather_knn's grid in 64ths
                        of its radius (8..256, default 80);
      RL_TUNE_AO_SPLIT: lanes that share one lumel's AO samples (1, 2, 4 or 8;
-                       0 = chosen from the map size, the default). */
+                       0 = chosen from the map size, the default);
+     RL_TUNE_FG_POOL: 1 = final gather on a persistent grid whose lanes take
+                      lumels from their warp's pool as they finish one (no
+                      idle lanes until the map runs dry), 0 = one lumel per
+                      thread;
+     RL_TUNE_FG_CHUNK: lumels a warp claims for its pool at a time (8..256). */
 enum {
     RL_TUNE_FG_REFILL = 0,
     RL_TUNE_FG_BLOCK = 1,
@@ -549,7 +554,9 @@ enum {
     RL_TUNE_BVH_WIDTH = 4,
     RL_TUNE_SPECULATIVE = 5,
     RL_TUNE_KNN_CELL = 6,
-    RL_TUNE_AO_SPLIT = 7
+    RL_TUNE_AO_SPLIT = 7,
+    RL_TUNE_FG_POOL = 8,
+    RL_TUNE_FG_CHUNK = 9
 };
 int rl_tune_set(int param, int value);
 int rl_tune_get(int param, int* value);

@@ -19,6 +19,7 @@ HIT_ALL = 15
 TUNE_FG_REFILL, TUNE_FG_BLOCK, TUNE_AO_REFILL, TUNE_AO_BLOCK, TUNE_BVH_WIDTH, TUNE_SPECULATIVE = 0, 1, 2, 3, 4, 5
 TUNE_KNN_CELL = 6
 TUNE_AO_SPLIT = 7
+TUNE_FG_POOL, TUNE_FG_CHUNK = 8, 9
 SOLVE_NOALLOC_MAX_PATCHES = 65536
 
 

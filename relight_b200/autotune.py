@@ -56,6 +56,24 @@ def set_speculative(on):
     _abi.check(_abi.lib().rl_tune_set(_abi.TUNE_SPECULATIVE, int(bool(on))))
 
 
+def get_pool():
+    """(pool, chunk): the final gather's persistent lumel pool (0/1) and the
+    lumels a warp claims at a time."""
+    v = C.c_int()
+    out = []
+    for p in (_abi.TUNE_FG_POOL, _abi.TUNE_FG_CHUNK):
+        _abi.check(_abi.lib().rl_tune_get(p, C.byref(v)))
+        out.append(v.value)
+    return tuple(out)
+
+
+def set_pool(on=None, chunk=None):
+    if on is not None:
+        _abi.check(_abi.lib().rl_tune_set(_abi.TUNE_FG_POOL, int(bool(on))))
+    if chunk is not None:
+        _abi.check(_abi.lib().rl_tune_set(_abi.TUNE_FG_CHUNK, int(chunk)))
+
+
 def get_knn_cell():
     v = C.c_int()
     _abi.check(_abi.lib().rl_tune_get(_abi.TUNE_KNN_CELL, C.byref(v)))

@@ -70,9 +70,10 @@ inline cudaStream_t S(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 // Launch tuning (rl_tune_set): per ray-stream kernel, the number of lanes a
 // warp waits for before refilling rays and the threads per block.  Defaults
 // are the autotuner's picks on the terrain final-gather / room AO workloads.
-// Then the BVH width, speculative traversal, and the kNN grid's cell width
-// in 64ths of the search radius (the fastest on the terrain kNN bench).
-int g_tune[8] = {24, 256, 32, 128, 2, 0, 80, 0};
+// Then the BVH width, speculative traversal, the kNN grid's cell width in
+// 64ths of the search radius (the fastest on the terrain kNN bench), the AO
+// lane split, and the final gather's persistent lumel pool and its chunk.
+int g_tune[10] = {24, 256, 32, 128, 2, 0, 80, 0, 1, 32};
 
 inline unsigned blocks_for(long long n, int threads) { return (unsigned)((n + threads - 1) / threads); }
 
@@ -135,6 +136,7 @@ struct rl_map {
     int kind = 0;
     DevMap dev{};
     int* d_owner = nullptr;  // rasterisation scratch: winning face per texel
+    unsigned long long* d_work = nullptr;  // work-list counter of the persistent bake kernels
     char* block = nullptr;   // rl_map_create_async: every array carved from this block
     ~rl_map() {
         if (block) {
@@ -143,6 +145,7 @@ struct rl_map {
         }
         cudaFree(dev.flags); cudaFree(dev.face); cudaFree(dev.position); cudaFree(dev.normal);
         cudaFree(dev.color); cudaFree(dev.photons); cudaFree(dev.gathered); cudaFree(dev.mesh); cudaFree(d_owner);
+        cudaFree(d_work);
     }
 };
 
@@ -170,10 +173,13 @@ extern "C" int rl_tune_set(int param, int value) {
     bool spec = param == RL_TUNE_SPECULATIVE;
     bool cell = param == RL_TUNE_KNN_CELL;
     bool split = param == RL_TUNE_AO_SPLIT;
+    bool pool = param == RL_TUNE_FG_POOL;
+    bool chunk = param == RL_TUNE_FG_CHUNK;
     if ((refill && value >= 1 && value <= 32) || (block && (value == 64 || value == 128 || value == 256)) ||
         (width && (value == 2 || value == 4 || value == 8)) || (spec && (value == 0 || value == 1)) ||
         (cell && value >= 8 && value <= 256) ||
-        (split && (value == 0 || value == 1 || value == 2 || value == 4 || value == 8)))
+        (split && (value == 0 || value == 1 || value == 2 || value == 4 || value == 8)) ||
+        (pool && (value == 0 || value == 1)) || (chunk && value >= 8 && value <= 256))
         g_tune[param] = value;
     else
         return fail(RL_INVALID_CALL, "rl_tune_set: bad parameter %d or value %d", param, value);
@@ -181,7 +187,7 @@ extern "C" int rl_tune_set(int param, int value) {
 }
 
 extern "C" int rl_tune_get(int param, int* value) {
-    if (!value || param < 0 || param > RL_TUNE_AO_SPLIT) return fail(RL_INVALID_CALL, "rl_tune_get: bad parameter");
+    if (!value || param < 0 || param > RL_TUNE_FG_CHUNK) return fail(RL_INVALID_CALL, "rl_tune_get: bad parameter");
     *value = g_tune[param];
     return RL_OK;
 }
@@ -526,6 +532,7 @@ extern "C" int rl_map_create(int kind, int width, int height, rl_map** out) {
     if (!rc) rc = dalloc(&m->dev.gathered, 3 * n);
     if (!rc) rc = dalloc(&m->dev.mesh, n);
     if (!rc) rc = dalloc(&m->d_owner, n);
+    if (!rc) rc = dalloc(&m->d_work, 2);
     if (rc) {
         delete m;
         return rc;
@@ -631,10 +638,10 @@ __global__ void k_map_init(DevMap m, int* owner, long long n) {
     }
 }
 
-static size_t map_block_bytes(size_t n, size_t offs[9]) {
-    const size_t sz[9] = {4 * n, 4 * n, 4 * n, 12 * n, 12 * n, 12 * n, 4 * n, 12 * n, 4 * n};
+static size_t map_block_bytes(size_t n, size_t offs[10]) {
+    const size_t sz[10] = {4 * n, 4 * n, 4 * n, 12 * n, 12 * n, 12 * n, 4 * n, 12 * n, 4 * n, 16};
     size_t off = 0;
-    for (int k = 0; k < 9; k++) {
+    for (int k = 0; k < 10; k++) {
         offs[k] = off;
         off = (off + sz[k] + 255) & ~(size_t)255;
     }
@@ -643,7 +650,7 @@ static size_t map_block_bytes(size_t n, size_t offs[9]) {
 
 extern "C" int rl_map_bytes(int width, int height, int64_t* bytes) {
     if (!bytes || width <= 0 || height <= 0) return fail(RL_INVALID_CALL, "rl_map_bytes: bad arguments");
-    size_t offs[9];
+    size_t offs[10];
     *bytes = (int64_t)map_block_bytes((size_t)width * height, offs);
     return RL_OK;
 }
@@ -654,7 +661,7 @@ extern "C" int rl_map_create_async(int kind, int width, int height, void* stream
     if ((long long)width * height > (1ll << 30)) return fail(RL_INVALID_CALL, "map too large");
     *out = nullptr;
     cudaStream_t st = S(stream);
-    size_t n = (size_t)width * height, offs[9];
+    size_t n = (size_t)width * height, offs[10];
     size_t bytes = map_block_bytes(n, offs);
     char* blk = nullptr;
     if (int rc = pool_alloc((void**)&blk, bytes, st)) return rc;
@@ -676,6 +683,7 @@ extern "C" int rl_map_create_async(int kind, int width, int height, void* stream
     m->dev.photons = (int*)(blk + offs[6]);
     m->dev.gathered = (float*)(blk + offs[7]);
     m->d_owner = (int*)(blk + offs[8]);
+    m->d_work = (unsigned long long*)(blk + offs[9]);
     int grid = (int)std::min<long long>(((long long)n + 255) / 256, 148 * 16);
     k_map_init<<<grid, 256, 0, st>>>(m->dev, m->d_owner, (long long)n);
     cudaError_t e = cudaGetLastError();
@@ -683,6 +691,7 @@ extern "C" int rl_map_create_async(int kind, int width, int height, void* stream
         m->block = nullptr;
         m->dev = DevMap{};
         m->d_owner = nullptr;
+        m->d_work = nullptr;
         cudaFreeAsync(blk, st);
         delete m;
         return fail(RL_CUDA_ERROR, "k_map_init: %s", cudaGetErrorString(e));
@@ -698,6 +707,7 @@ extern "C" int rl_map_destroy_async(rl_map* m, void* stream) {
     m->block = nullptr;
     m->dev = DevMap{};
     m->d_owner = nullptr;
+    m->d_work = nullptr;
     delete m;
     if (e != cudaSuccess) return fail(RL_CUDA_ERROR, "map free: %s", cudaGetErrorString(e));
     return RL_OK;
@@ -1453,6 +1463,82 @@ __global__ void __launch_bounds__(256, 4) k_indirect(DevScene s, DevMap m, const
     col[0] = col[0] + g.gr / ns; col[1] = col[1] + g.gg / ns; col[2] = col[2] + g.gb / ns;
 }
 
+// FgGen over a work list of lumels (ray_loop_pool): lumel item k of the
+// iteration `it` (iter_lumel), its samples in order, its colour written when
+// its last sample is shaded — the same arithmetic as k_indirect.
+struct FgPoolGen : FgGen {
+    const DevMap* map;
+    const Iter* it;
+    int nsamples;
+    long long li;
+    __device__ bool has_more() const { return j < samples; }
+    __device__ void end_item() {
+        if (samples == 0) return;
+        const float ns = (float)samples;
+        float* col = map->color + 3 * li;
+        col[0] = col[0] + gr / ns; col[1] = col[1] + gg / ns; col[2] = col[2] + gb / ns;
+        samples = 0;
+    }
+    __device__ bool start_item(long long k) {
+        long long i;
+        if (!iter_lumel(*map, *it, k, i)) return false;
+        li = i;
+        pos = ld3(map->position + 3 * i);
+        nrm = ld3(map->normal + 3 * i);
+        item = (uint32_t)i;
+        j = 0;
+        samples = nsamples;
+        gr = gg = gb = 0.f;
+        return true;
+    }
+};
+
+// Persistent final gather: a grid the size of the resident blocks, lanes
+// taking lumels from their warp's pool (ray_loop_pool).
+__global__ void __launch_bounds__(256, 4) k_indirect_pool(DevScene s, const __grid_constant__ DevMap m,
+                                                          const __grid_constant__ GatherMaps G, int samples,
+                                                          float maxd, V3 sky, V3 amb, uint2 key,
+                                                          const __grid_constant__ Iter it, long long count,
+                                                          int refill, int* status, unsigned long long* counter,
+                                                          int chunk) {
+    FgPoolGen g;
+    g.s = &s;
+    g.G = &G;
+    g.map = &m;
+    g.it = &it;
+    g.nsamples = samples;
+    g.samples = 0;
+    g.j = 0;
+    g.li = 0;
+    g.sky = sky;
+    g.amb = amb;
+    g.key = key;
+    g.item = 0;
+    g.maxd = maxd;
+    g.gr = g.gg = g.gb = 0.f;
+    g.influence = 0.f;
+    g.pos = g.nrm = g.dir = mk3(0.f, 0.f, 0.f);
+    ray_loop_pool<false>(s, g, refill, status, counter, count, chunk);
+}
+
+// Blocks of `threads` that fit on the device at once for `kernel`
+// (persistent grids), cached per kernel and block size.
+template <typename K>
+static int resident_blocks(K kernel, int threads) {
+    static std::mutex mu;
+    static std::map<std::pair<const void*, int>, int> cache;
+    std::lock_guard<std::mutex> g(mu);
+    const auto key = std::make_pair((const void*)kernel, threads);
+    auto f = cache.find(key);
+    if (f != cache.end()) return f->second;
+    int dev = 0, sms = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) !=
+                                                  cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0) != cudaSuccess || per_sm <= 0)
+        return 0;
+    return cache[key] = sms * per_sm;
+}
+
 extern "C" int rl_bake_indirect(const rl_scene* s, rl_map* lm, rl_map* const* maps, int nmaps, int samples,
                                 float maxd, const float sky[3], const float ambient[3], uint64_t seed,
                                 const rl_iterator* iterator, void* stream) {
@@ -1478,6 +1564,18 @@ extern "C" int rl_bake_indirect(const rl_scene* s, rl_map* lm, rl_map* const* ma
     int bs = g_tune[RL_TUNE_FG_BLOCK];
     bool wide = g_tune[RL_TUNE_BVH_WIDTH] == 4 && s->dev.nodes4 != nullptr;
     bool wide8 = g_tune[RL_TUNE_BVH_WIDTH] == 8 && s->dev.nodes8 != nullptr;
+    if (g_tune[RL_TUNE_FG_POOL] && !wide && !wide8 && !g_tune[RL_TUNE_SPECULATIVE]) {
+        const int resident = resident_blocks(k_indirect_pool, bs);
+        if (resident <= 0) return fail(RL_CUDA_ERROR, "k_indirect_pool: occupancy query failed");
+        const long long want = ((long long)count + bs - 1) / bs;
+        const unsigned grid = (unsigned)(want < resident ? want : resident);
+        CK(cudaMemsetAsync(lm->d_work, 0, sizeof(unsigned long long), st));
+        k_indirect_pool<<<grid, bs, 0, st>>>(s->dev, lm->dev, G, samples, maxd, skyv, ambv, key, it, count,
+                                             g_tune[RL_TUNE_FG_REFILL], s->d_status, lm->d_work,
+                                             g_tune[RL_TUNE_FG_CHUNK]);
+        CK_LAUNCH("k_indirect_pool");
+        return RL_OK;
+    }
     auto kern = wide8 ? k_indirect<8> : wide ? k_indirect<4> : (g_tune[RL_TUNE_SPECULATIVE] ? k_indirect<3> : k_indirect<2>);
     kern<<<blocks_for(count, bs), bs, 0, st>>>(s->dev, lm->dev, G, samples, maxd, skyv, ambv, key, it, count,
                                               g_tune[RL_TUNE_FG_REFILL], s->d_status);

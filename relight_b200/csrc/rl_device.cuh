@@ -426,6 +426,124 @@ __device__ __forceinline__ void ray_loop(const DevScene& s, Gen& g, int refill, 
     }
 }
 
+// ray_loop over a shared list of work items (lumels) instead of one per
+// lane: a lane whose item has no rays left takes the next item from its
+// warp's pool, and the warp refills the pool `chunk` items at a time from
+// the global `counter` (items [0, count)).  Lanes therefore keep tracing
+// until the list runs dry, instead of idling until the warp's slowest item
+// is done, and a persistent grid has no wave tail.  Neighbouring items of a
+// chunk stay in one warp (coherent rays).  Each item is still one lane's
+// rays in order, so results are those of ray_loop.  The generator adds:
+//   has_more()        the current item has rays left
+//   end_item()        the current item is done (write its result); no-op
+//                     when the lane holds none
+//   start_item(k)     take item k; false if k is not to be baked (then the
+//                     lane takes another)
+template <bool kAny, typename Gen>
+__device__ __forceinline__ void ray_loop_pool(const DevScene& s, Gen& g, int refill, int* overflow,
+                                              unsigned long long* counter, long long count, int chunk) {
+    V3 o = mk3(0.f, 0.f, 0.f), d = o, idir = o, ood = o;
+    float tnear = 0.f, tfar = 0.f, best = 0.f;
+    int best_gid = 0x7fffffff;
+    RayHit hit;
+    hit.gid = -1; hit.t = hit.u = hit.v = 0.f;
+    int stack[kStackSize];
+    int sp = 0;
+    int node = kNodeDone;
+    bool have = false, exhausted = false;
+    const unsigned lanes_below = (1u << (threadIdx.x & 31)) - 1u;
+    long long pool_next = 0, pool_end = 0;  // warp-uniform: items claimed, not yet handed out
+    bool dry = false;                       // warp-uniform: the list is used up
+    for (;;) {
+        const bool need = node == kNodeDone && !exhausted;
+        const unsigned alive = __ballot_sync(0xffffffffu, !exhausted);
+        if (alive == 0) break;
+        const unsigned needm = __ballot_sync(0xffffffffu, need);
+        if (needm && (__popc(needm) >= refill || needm == alive)) {
+            if (need && have) {
+                g.finish(hit);
+                have = false;
+            }
+            bool want = need && !g.has_more();
+            if (want) g.end_item();
+            unsigned wm = __ballot_sync(0xffffffffu, want);
+            while (wm) {
+                if (pool_next >= pool_end) {
+                    if (dry) break;
+                    unsigned long long base = 0;
+                    if ((threadIdx.x & 31) == 0) base = atomicAdd(counter, (unsigned long long)chunk);
+                    base = __shfl_sync(0xffffffffu, base, 0);
+                    if ((long long)base >= count) {
+                        dry = true;
+                        break;
+                    }
+                    pool_next = (long long)base;
+                    pool_end = (long long)base + chunk < count ? (long long)base + chunk : count;
+                }
+                const long long item = pool_next + __popc(wm & lanes_below);
+                if (want && item < pool_end && g.start_item(item)) want = false;
+                const long long handed = __popc(wm);
+                pool_next = pool_end - pool_next < handed ? pool_end : pool_next + handed;
+                wm = __ballot_sync(0xffffffffu, want);
+            }
+            if (want) exhausted = true;
+            if (need && !exhausted) {
+                g.next(o, d, tnear, tfar);
+                have = true;
+                idir = mk3(safe_inv(d.x), safe_inv(d.y), safe_inv(d.z));
+                ood = mk3(o.x * idir.x, o.y * idir.y, o.z * idir.z);
+                best = tfar;
+                best_gid = 0x7fffffff;
+                hit.gid = -1;
+                sp = 0;
+                node = s.ntris > 0 ? 0 : kNodeDone;
+            }
+        }
+        if (node == kNodeDone) continue;
+        // inner nodes until a leaf (or the end of the walk)
+        while (node >= 0) {
+            const float4* np = s.nodes + 4 * (size_t)node;
+            float4 n0 = __ldg(np), n1 = __ldg(np + 1), n2 = __ldg(np + 2), n3 = __ldg(np + 3);
+            bool h0, h1;
+            float e0, e1;
+            slab2(n0, n1, n2, idir, ood, tnear, best, h0, h1, e0, e1);
+            int c0 = __float_as_int(n3.x), c1 = __float_as_int(n3.y);
+            if (h0 && h1) {
+                int nearc = c0, farc = c1;
+                if (e1 < e0) { nearc = c1; farc = c0; }
+                if (sp < kStackSize) stack[sp++] = farc;
+                else if (overflow) *overflow = 1;
+                node = nearc;
+            } else if (h0) {
+                node = c0;
+            } else if (h1) {
+                node = c1;
+            } else {
+                node = sp > 0 ? stack[--sp] : kNodeDone;
+            }
+        }
+        if (node == kNodeDone) continue;
+        // one leaf
+        int code = ~node;
+        int first = code >> 3, count_tris = (code & 7) + 1;
+        bool stop = false;
+        for (int i = first; i < first + count_tris; i++) {
+            const float4* tp = s.tris + 3 * (size_t)i;
+            float4 t0 = __ldg(tp), t1 = __ldg(tp + 1), t2 = __ldg(tp + 2);
+            float t, u, v;
+            if (tri_test(t0, t1, t2, o, d, tnear, tfar, t, u, v)) {
+                int gid = __float_as_int(t0.w);
+                if (t < best || (t == best && gid < best_gid)) {
+                    best = t; best_gid = gid;
+                    hit.t = t; hit.u = u; hit.v = v; hit.gid = gid;
+                    if (kAny) { stop = true; break; }
+                }
+            }
+        }
+        node = (!stop && sp > 0) ? stack[--sp] : kNodeDone;
+    }
+}
+
 template <bool kAny, typename Gen>
 __device__ __forceinline__ void ray_loop_spec(const DevScene& s, Gen& g, int refill, int* overflow) {
     V3 o = mk3(0.f, 0.f, 0.f), d = o, idir = o, ood = o;

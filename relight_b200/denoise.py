@@ -181,8 +181,10 @@ def training_scenes(n, seed=100, sides=(256, 384, 512)):
         verts = int(rng.integers(48, 160))
         boxes = int(rng.integers(20, 600))
         side = int(rng.choice(sides))
-        out.append(scenes.terrain_scene(seed=seed * 1000 + k, verts=verts, n_boxes=boxes, size=side, tiles=1,
-                                        passes=2))
+        recipe = dict(seed=seed * 1000 + k, verts=verts, n_boxes=boxes, size=side, tiles=1, passes=2)
+        wl = scenes.terrain_scene(**recipe)
+        wl.recipe = recipe  # scenes.terrain_scene(**recipe) rebuilds it (e.g. in another process)
+        out.append(wl)
     return out
 
 
@@ -250,11 +252,17 @@ def rmse(a, b, valid):
     return float(np.sqrt((d * d).mean()))
 
 
-def evaluate(dn, workloads, spp_lo=16, spp_ref=8192, plain=(16, 64, 256, 1024), seed=900, stream=None):
-    """Per-texel RMSE against a `spp_ref` bake (valid lumels, linear colour)
-    of the plain final gather at each sample count in `plain` and of the
-    `spp_lo` bake after the denoiser, with the device time of each (bake,
-    and bake + denoise).  The plain bake's sample count of equal RMSE is
+def evaluate(dn, workloads, spp_lo=16, spp_ref=8192, plain=(16, 64, 256, 1024), seed=900, stream=None,
+             truth=None):
+    """Per-texel RMSE against a reference (linear colour) of the plain final
+    gather at each sample count in `plain` and of the `spp_lo` bake after the
+    denoiser, with the device time of each (bake, and bake + denoise).  The
+    reference is truth(i, workload) -> (texel indices, expected colours
+    [n][3][, the estimate's own noise variance per colour value]) when given
+    (an FP64 high-sample estimate, called after the workload's photons are
+    gathered on the device; its noise variance, when returned, is taken out
+    of every mean squared error), else a `spp_ref` bake over all valid
+    lumels.  The plain bake's sample count of equal RMSE is
     interpolated (log-log) inside the measured range, or past its end from
     the fit RMSE^2 = a / spp + c (c: the reference's own noise and any
     bias).  Returns {"plain": {spp: (rmse, ms)}, "denoised": (rmse, ms),
@@ -276,10 +284,22 @@ def evaluate(dn, workloads, spp_lo=16, spp_ref=8192, plain=(16, 64, 256, 1024), 
         rl.emit_photons(wl.scene, wl.settings)
         lm = wl.lightmap._device
         pms = [m._device for m in wl.scene.flat.photonmaps]
-        bake_fg(rl, ds, lm, pms, wl.settings, spp_ref, seed * 13 + i, stream)
-        d = lm.download(stream, fields=("flags", "color"))
-        valid = (d["flags"] & 1).astype(bool)
-        ref = d["color"]
+        noise_var = 0.0
+        if truth is not None:
+            torch.cuda.synchronize()
+            t = truth(i, wl)
+            texels, expect = t[0], t[1]
+            noise_var = float(t[2]) if len(t) > 2 else 0.0
+            n = wl.lightmap.width * wl.lightmap.height
+            ref = np.zeros((n, 3), np.float64)
+            ref[texels] = expect
+            valid = np.zeros(n, bool)
+            valid[texels] = True
+        else:
+            bake_fg(rl, ds, lm, pms, wl.settings, spp_ref, seed * 13 + i, stream)
+            d = lm.download(stream, fields=("flags", "color"))
+            valid = (d["flags"] & 1).astype(bool)
+            ref = d["color"]
 
         def timed(fn):
             e0, e1 = ev(), ev()
@@ -292,7 +312,7 @@ def evaluate(dn, workloads, spp_lo=16, spp_ref=8192, plain=(16, 64, 256, 1024), 
         for k in plain:
             ms = timed(lambda: bake_fg(rl, ds, lm, pms, wl.settings, k, seed * 17 + i * 31 + k, stream))
             c = lm.download(stream, fields=("color",))["color"]
-            acc_plain[k][0] += rmse(c, ref, valid) ** 2
+            acc_plain[k][0] += rmse(c, ref, valid) ** 2 - noise_var
             acc_plain[k][1] += ms
             acc_plain[k][2] += 1
 
@@ -304,12 +324,12 @@ def evaluate(dn, workloads, spp_lo=16, spp_ref=8192, plain=(16, 64, 256, 1024), 
             lo_and_denoise()  # untimed warm-up of the denoiser's kernels
         ms = timed(lo_and_denoise)
         c = lm.download(stream, fields=("color",))["color"]
-        acc_dn[0] += rmse(c, ref, valid) ** 2
+        acc_dn[0] += rmse(c, ref, valid) ** 2 - noise_var
         acc_dn[1] += ms
         acc_dn[2] += 1
         max_err = max(max_err, float(np.abs(c - ref)[valid].max()) if valid.any() else 0.0)
-    res_plain = {k: (float(np.sqrt(v[0] / v[2])), v[1] / v[2]) for k, v in acc_plain.items()}
-    dn_rmse, dn_ms = float(np.sqrt(acc_dn[0] / acc_dn[2])), acc_dn[1] / acc_dn[2]
+    res_plain = {k: (float(np.sqrt(max(v[0], 0.0) / v[2])), v[1] / v[2]) for k, v in acc_plain.items()}
+    dn_rmse, dn_ms = float(np.sqrt(max(acc_dn[0], 0.0) / acc_dn[2])), acc_dn[1] / acc_dn[2]
     ks = sorted(res_plain)
     r = np.array([res_plain[k][0] for k in ks])
     extrapolated = False

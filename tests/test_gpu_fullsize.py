@@ -8,9 +8,9 @@
     1,000,000 photons with 3 bounces, gather radius 7, final gather 256 rays
     per lumel.  Photon counts exact and colours within 1e-5 relative (atomic
     float adds); the gather within 1e-4; the final gather baked by the GPU over
-    the whole map (8x8 lumel tiles, the default launch tuning, per-triangle
-    shading records) from a photonmap pinned to the GPU's, and compared bit
-    for bit with the oracle on every 997th lumel;
+    the whole map (8x8 lumel tiles, the persistent lumel pool, the default
+    launch tuning, per-triangle shading records) from a photonmap pinned to
+    the GPU's, and compared bit for bit with the oracle on every 997th lumel;
   - the scene's traversal status word stays 0 (no stack overflow) after
     every pass.
 """
@@ -26,11 +26,6 @@ pytestmark = pytest.mark.gpu
 def _lumels(m):
     from relight_b200.device import lumels
     return lumels(m)
-
-
-def _default_tuning():
-    from relight_b200 import autotune
-    return autotune.get("indirect"), autotune.get("ao"), autotune.get_width(), autotune.get_speculative()
 
 
 def test_room_benchmark_bake_bit_exact(cuda):
@@ -87,7 +82,7 @@ def test_terrain_benchmark_final_gather_bit_exact_on_lumel_subset(terrain):
     st = w.settings
     # the production launch: library defaults, whole-map iterator (8x8 tiles)
     assert autotune.get("indirect") == {"refill": 24, "block": 256}
-    assert autotune.get_width() == 2 and autotune.get_speculative() == 0
+    assert autotune.get_width() == 2 and autotune.get_speculative() == 0 and autotune.get_pool() == (1, 32)
     rl.bake_indirect_light(w.scene, w.meshes[0], None, st, seed=77)
     gl = _lumels(w.lightmap)
     assert w.scene._device.status() == 0

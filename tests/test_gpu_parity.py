@@ -418,16 +418,21 @@ def test_radiosity_solve_large_aligned_and_not(cuda):
 
 def test_launch_tuning_changes_no_result(cuda):
     """The autotuner's knobs (refill threshold, block size, BVH width 2 / 4 /
-    compressed 8, speculative walk) reschedule rays only: every setting
-    bakes the same bits."""
+    compressed 8, speculative walk, the final gather's persistent lumel pool
+    and its chunk) reschedule rays only: every setting bakes the same bits."""
     from relight_b200 import autotune
-    saved = autotune.get("ao"), autotune.get("indirect"), autotune.get_width(), autotune.get_speculative()
+    saved = (autotune.get("ao"), autotune.get("indirect"), autotune.get_width(), autotune.get_speculative(),
+             autotune.get_pool())
     colors, fg = [], []
     try:
-        for refill, block, width, spec in ((1, 64, 2, 0), (13, 128, 4, 0), (32, 256, 2, 1), (24, 64, 2, 1),
-                                           (16, 64, 8, 0), (32, 128, 8, 0)):
+        for refill, block, width, spec, pool in ((1, 64, 2, 0, (0, 32)), (13, 128, 4, 0, (0, 32)),
+                                                 (32, 256, 2, 1, (0, 32)), (24, 64, 2, 1, (0, 32)),
+                                                 (16, 64, 8, 0, (0, 32)), (32, 128, 8, 0, (0, 32)),
+                                                 (24, 256, 2, 0, (1, 32)), (1, 64, 2, 0, (1, 8)),
+                                                 (32, 128, 2, 0, (1, 256)), (20, 256, 2, 0, (1, 64))):
             autotune.set_width(width)
             autotune.set_speculative(spec)
+            autotune.set_pool(*pool)
             autotune.set(refill, block, "ao")
             autotune.set(refill, block, "indirect")
             rl = _relight()
@@ -443,6 +448,7 @@ def test_launch_tuning_changes_no_result(cuda):
         autotune.set(saved[1]["refill"], saved[1]["block"], "indirect")
         autotune.set_width(saved[2])
         autotune.set_speculative(saved[3])
+        autotune.set_pool(*saved[4])
     assert all(np.array_equal(colors[0], c) for c in colors[1:])
     # photon deposits are atomic float sums, so the final gather is compared
     # through the photonmap's tolerance

@@ -197,9 +197,10 @@ def _rmse(a, b):
 
 @needs_ref
 def test_ambient_occlusion_statistics_match_reference():
-    """Same expectation: per-texel RMSE against an FP64 4,096-sample estimate
-    within 1.25x of the reference's, and no bias beyond 3 standard errors."""
-    w = scenes.room_scene(size=96)
+    """Same expectation at equal sample count (64): over 4,096 seeded texels,
+    the per-texel RMSE against an FP64 2,048-sample estimate is within 1.1x
+    of the reference's, and neither is biased beyond 3 standard errors."""
+    w = scenes.room_scene(size=128)
     ref = RefScene(w.scene)
     orc = Oracle(w.scene.flat).bind_scene(w.scene)
     lm = orc.maps()[0]
@@ -209,13 +210,13 @@ def test_ambient_occlusion_statistics_match_reference():
     ref.lib.ref_bake_ao(ref.h, ref.mesh(w.mesh), 64, 0.8, 2.0, 1.0, 0, 0, 1)
     orc.bake_ao(lm, 64, 0.8, 2.0, 1.0, 4242)
     r = ref.lumels(w.lightmap)
-    tex = np.nonzero(lm.flags & 1)[0][::31]
-    ex = orc.ao_expect(lm, tex, 4096, 0.8, 2.0, 99)
+    valid = np.nonzero(lm.flags & 1)[0]
+    tex = np.sort(np.random.default_rng(3).choice(valid, 4096, replace=False))
+    ex = orc.ao_expect(lm, tex, 2048, 0.8, 2.0, 99)
     e_ref, e_or = r.color[tex, 0] - ex, lm.color[tex, 0] - ex
-    assert _rmse(lm.color[tex, 0], ex) <= 1.25 * _rmse(r.color[tex, 0], ex)
-    se = e_or.std() / np.sqrt(len(tex))
-    assert abs(e_or.mean()) < 3 * se + 1e-3
-    assert abs(e_ref.mean() - e_or.mean()) < 3 * np.hypot(se, e_ref.std() / np.sqrt(len(tex))) + 2e-3
+    assert _rmse(lm.color[tex, 0], ex) <= 1.1 * _rmse(r.color[tex, 0], ex)
+    for e in (e_or, e_ref):
+        assert abs(e.mean()) < 3 * e.std() / np.sqrt(len(tex)) + 1e-3
 
 
 @needs_ref
@@ -244,8 +245,10 @@ def test_photon_pass_statistics_match_reference():
 
 @needs_ref
 def test_final_gather_statistics_match_reference():
-    """Final gather from the same (reference-gathered) photonmap: RMSE of
-    both against an FP64 2,048-sample estimate agree within 25%."""
+    """Final gather from the same (reference-gathered) photonmap at equal
+    sample count (32): over 4,096 seeded texels, the per-texel RMSE against
+    an FP64 2,048-sample estimate is within 1.1x of the reference's, and
+    neither is biased beyond 3 standard errors (per channel)."""
     w = scenes.terrain_scene(verts=40, n_boxes=40, size=96, tiles=2, passes=1, bounces=2, fg_samples=32)
     st = w.settings
     ref = RefScene(w.scene)
@@ -253,7 +256,7 @@ def test_final_gather_statistics_match_reference():
     ref.lib.ref_emit_photons(ref.h, st.photon_pass_count, st.photon_bounce_count, st.photon_energy_threshold,
                              st.photon_max_distance, st.final_gather_radius)
     rp = ref.lumels(w.photonmap)
-    sky = (C_float3 := np.asarray(st.sky_color, np.float32))
+    sky = np.asarray(st.sky_color, np.float32)
     amb = np.asarray(st.ambient_color, np.float32)
     ref.lib.ref_bake_indirect(ref.h, ref.mesh(w.meshes[0]), st.final_gather_samples, st.final_gather_distance,
                               st.final_gather_radius, ptr(sky), ptr(amb), 0, 0, 1)
@@ -263,11 +266,13 @@ def test_final_gather_statistics_match_reference():
     pm.gathered[:] = rp.gathered
     lm = orc.maps()[0]
     orc.bake_indirect(lm, [pm], st.final_gather_samples, st.final_gather_distance, sky, amb, 77)
-    tex = np.nonzero(lm.flags & 1)[0][::23]
+    valid = np.nonzero(lm.flags & 1)[0]
+    tex = np.sort(np.random.default_rng(4).choice(valid, 4096, replace=False))
     ex = orc.fg_expect(lm, [pm], tex, 2048, st.final_gather_distance, sky, amb, 8)
-    a, b = _rmse(lm.color[tex], ex), _rmse(r.color[tex], ex)
-    assert a <= 1.25 * b and b <= 1.25 * a
-    del C_float3
+    assert _rmse(lm.color[tex], ex) <= 1.1 * _rmse(r.color[tex], ex)
+    for c in (lm.color[tex], r.color[tex]):
+        e = c - ex
+        assert (np.abs(e.mean(0)) < 3 * e.std(0) / np.sqrt(len(tex)) + 1e-3).all()
 
 
 @needs_ref

@@ -1471,6 +1471,7 @@ struct FgPoolGen : FgGen {
     const Iter* it;
     int nsamples;
     long long li;
+    long long k_begin, limit;  // item k is iteration item k_begin + k, for k < limit
     __device__ bool has_more() const { return j < samples; }
     __device__ void end_item() {
         if (samples == 0) return;
@@ -1481,7 +1482,7 @@ struct FgPoolGen : FgGen {
     }
     __device__ bool start_item(long long k) {
         long long i;
-        if (!iter_lumel(*map, *it, k, i)) return false;
+        if (k >= limit || !iter_lumel(*map, *it, k_begin + k, i)) return false;
         li = i;
         pos = ld3(map->position + 3 * i);
         nrm = ld3(map->normal + 3 * i);
@@ -1510,6 +1511,8 @@ __global__ void __launch_bounds__(256, 4) k_indirect_pool(DevScene s, const __gr
     g.samples = 0;
     g.j = 0;
     g.li = 0;
+    g.k_begin = 0;
+    g.limit = count;
     g.sky = sky;
     g.amb = amb;
     g.key = key;
@@ -1518,7 +1521,8 @@ __global__ void __launch_bounds__(256, 4) k_indirect_pool(DevScene s, const __gr
     g.gr = g.gg = g.gb = 0.f;
     g.influence = 0.f;
     g.pos = g.nrm = g.dir = mk3(0.f, 0.f, 0.f);
-    ray_loop_pool<false>(s, g, refill, status, counter, count, chunk);
+    CounterSource src{counter, count, chunk};
+    ray_loop_pool<false>(s, g, refill, status, src);
 }
 
 // Blocks of `threads` that fit on the device at once for `kernel`
@@ -2356,6 +2360,7 @@ struct rl_batch {
     int slot = 0;
     long long items = 0, total[3] = {0, 0, 0};
     int grid[3] = {0, 0, 0}, block[3] = {128, 128, 128}, refill[3] = {0, 0, 0};
+    bool pool = false;  // AO / final gather through k_batch_pool (RL_TUNE_FG_POOL at creation)
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     ~rl_batch() {
@@ -2468,6 +2473,131 @@ __global__ void __launch_bounds__(kKind == 0 ? 128 : 256, kKind == 0 ? 1 : 4) k_
     }
 }
 
+// AoGen over a work list of lumels (ray_loop_pool), as FgPoolGen.
+struct AoPoolGen : AoGen {
+    const DevMap* map;
+    const Iter* it;
+    int nsamples;
+    float fraction, exponent;
+    long long li, k_begin, limit;
+    __device__ bool has_more() const { return j < samples; }
+    __device__ void end_item() {
+        if (samples == 0) return;
+        float value = 1.0f - occluded / (samples * fraction);
+        if (fabsf(1.0f - exponent) > 0.01f) value = powf(value, exponent);
+        float* col = map->color + 3 * li;
+        col[0] = col[0] * value; col[1] = col[1] * value; col[2] = col[2] * value;
+        samples = 0;
+    }
+    __device__ bool start_item(long long k) {
+        long long i;
+        if (k >= limit || !iter_lumel(*map, *it, k_begin + k, i)) return false;
+        li = i;
+        pos = ld3(map->position + 3 * i);
+        nrm = ld3(map->normal + 3 * i);
+        item = (uint32_t)i;
+        j = 0;
+        samples = nsamples;
+        occluded = 0;
+        return true;
+    }
+};
+
+// Work source of the pooled batch kernel: the kind's 32-item chunks in
+// counter order, restricted to one job ([job_lo, job_hi) of the kind's item
+// space).  A chunk of a later job ends this job's pass and is kept in `next`
+// for the warp's next job; `first` is the chunk the pass starts with.
+struct BatchSource {
+    unsigned long long* counter;
+    long long total, job_lo, job_hi, first, next;
+    __device__ __forceinline__ bool claim(long long& lo, long long& hi) {
+        long long base = first;
+        first = -1;
+        if (base < 0) {
+            unsigned long long b = 0;
+            if ((threadIdx.x & 31) == 0) b = atomicAdd(counter, 32ull);
+            base = (long long)__shfl_sync(0xffffffffu, b, 0);
+        }
+        if (base >= total) return false;
+        if (base >= job_hi) {
+            next = base;
+            return false;
+        }
+        lo = base - job_lo;
+        hi = lo + 32;
+        return true;
+    }
+};
+
+// The AO / final-gather batch kernels with ray_loop_pool: a warp keeps its
+// lanes on the lumels of one job, taking the job's next chunk as lanes
+// finish instead of waiting for the chunk's slowest lumel, and moves to the
+// next job when the chunks run past its own.  Same lumels, keys and
+// arithmetic as k_batch.
+template <int kKind>
+__global__ void __launch_bounds__(256, 4) k_batch_pool(const BatchHeader* __restrict__ hdrs,
+                                                       unsigned long long* counter, int refill) {
+    const BatchHeader* H = hdrs + kKind;
+    const long long total = H->total;
+    if (total <= 0) return;
+    long long next;
+    {
+        unsigned long long b = 0;
+        if ((threadIdx.x & 31) == 0) b = atomicAdd(counter + kKind, 32ull);
+        next = (long long)__shfl_sync(0xffffffffu, b, 0);
+    }
+    while (next >= 0 && next < total) {
+        const int jx = find_job(H->prefix, H->njobs, next);
+        const DevJob& J = H->jobs[jx];
+        BatchSource src{counter + kKind, total, H->prefix[jx], jx + 1 < H->njobs ? H->prefix[jx + 1] : total, next,
+                        -1};
+        const DevScene s = J.s;
+        if (kKind == 1) {
+            AoPoolGen g;
+            g.map = &J.m;
+            g.it = &J.it;
+            g.nsamples = J.samples;
+            g.fraction = J.fraction;
+            g.exponent = J.exponent;
+            g.li = 0;
+            g.k_begin = J.k_begin;
+            g.limit = J.count;
+            g.pos = g.nrm = mk3(0.f, 0.f, 0.f);
+            g.key = J.key;
+            g.item = 0;
+            g.j = 0;
+            g.stride = 1;
+            g.samples = 0;
+            g.occluded = 0;
+            g.maxd = J.maxd;
+            ray_loop_pool<true>(s, g, refill, J.status, src);
+        } else {
+            FgPoolGen g;
+            g.s = &J.s;
+            g.G = J.maps;
+            g.map = &J.m;
+            g.it = &J.it;
+            g.nsamples = J.samples;
+            g.samples = 0;
+            g.j = 0;
+            g.li = 0;
+            g.k_begin = J.k_begin;
+            g.limit = J.count;
+            g.sky = J.sky;
+            g.amb = J.amb;
+            g.key = J.key;
+            g.item = 0;
+            g.maxd = J.maxd;
+            g.gr = g.gg = g.gb = 0.f;
+            g.influence = 0.f;
+            g.pos = g.nrm = g.dir = mk3(0.f, 0.f, 0.f);
+            ray_loop_pool<false>(s, g, refill, J.status, src);
+        }
+        next = src.next;
+        __syncwarp();
+    }
+}
+
 // Whether two jobs of one pass kind may visit a common lumel (a race: both
 // read-modify-write its colour).  Disjoint for sure: different lightmaps;
 // face iterators over different meshes; lumel iterators of one step with
@@ -2506,7 +2636,10 @@ static int batch_init(rl_batch* b) {
     int dev = 0, sms = 0;
     CK(cudaGetDevice(&dev));
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    const void* kern[3] = {(const void*)k_batch<0>, (const void*)k_batch<1>, (const void*)k_batch<2>};
+    b->pool = g_tune[RL_TUNE_FG_POOL] != 0;
+    const void* kern[3] = {(const void*)k_batch<0>,
+                           b->pool ? (const void*)k_batch_pool<1> : (const void*)k_batch<1>,
+                           b->pool ? (const void*)k_batch_pool<2> : (const void*)k_batch<2>};
     b->block[0] = 128;
     b->block[1] = g_tune[RL_TUNE_AO_BLOCK];
     b->block[2] = g_tune[RL_TUNE_FG_BLOCK];
@@ -2729,7 +2862,9 @@ extern "C" int rl_batch_update(rl_batch* b, const rl_batch_job* jobs, int njobs,
 static int batch_enqueue(rl_batch* b, cudaStream_t st) {
     CK(cudaMemsetAsync(b->d_counter, 0, 3 * sizeof(unsigned long long), st));
     for (int k = 0; k < 3; k++) {
-        auto kern = k == 0 ? k_batch<0> : k == 1 ? k_batch<1> : k_batch<2>;
+        auto kern = k == 0 ? k_batch<0>
+                    : k == 1 ? (b->pool ? k_batch_pool<1> : k_batch<1>)
+                             : (b->pool ? k_batch_pool<2> : k_batch<2>);
         kern<<<b->grid[k], b->block[k], 0, st>>>(b->d_hdr, b->d_counter, b->refill[k]);
         CK_LAUNCH("k_batch");
     }

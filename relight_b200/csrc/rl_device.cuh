@@ -252,6 +252,20 @@ __device__ __forceinline__ float safe_inv(float d) {
     return 1.0f / a;
 }
 
+// Three-input minimum / maximum (one instruction on sm_100).  Min and max
+// round nothing, so these equal the two-input cascades exactly (the slab
+// operands are never NaN: safe_inv keeps 1/d finite).
+__device__ __forceinline__ float fmin3(float a, float b, float c) {
+    float r;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+__device__ __forceinline__ float fmax3(float a, float b, float c) {
+    float r;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+
 // Slab test of both children of a node against [tnear, tmax]; returns the
 // entry distances.  Conservative: boxes were padded at build and the exit
 // bound is widened by a few ulps.
@@ -260,13 +274,13 @@ __device__ __forceinline__ void slab2(float4 n0, float4 n1, float4 n2, V3 idir, 
     float a0 = __fmaf_rn(n0.x, idir.x, -ood.x), a1 = __fmaf_rn(n0.y, idir.x, -ood.x);
     float b0 = __fmaf_rn(n0.z, idir.y, -ood.y), b1 = __fmaf_rn(n0.w, idir.y, -ood.y);
     float c0 = __fmaf_rn(n2.x, idir.z, -ood.z), c1 = __fmaf_rn(n2.y, idir.z, -ood.z);
-    float lo0 = fmaxf(fmaxf(fminf(a0, a1), fminf(b0, b1)), fmaxf(fminf(c0, c1), tnear));
-    float hi0 = fminf(fminf(fmaxf(a0, a1), fmaxf(b0, b1)), fminf(fmaxf(c0, c1), tmax));
+    float lo0 = fmax3(fminf(a0, a1), fminf(b0, b1), fmaxf(fminf(c0, c1), tnear));
+    float hi0 = fmin3(fmaxf(a0, a1), fmaxf(b0, b1), fminf(fmaxf(c0, c1), tmax));
     float d0 = __fmaf_rn(n1.x, idir.x, -ood.x), d1 = __fmaf_rn(n1.y, idir.x, -ood.x);
     float f0 = __fmaf_rn(n1.z, idir.y, -ood.y), f1 = __fmaf_rn(n1.w, idir.y, -ood.y);
     float g0 = __fmaf_rn(n2.z, idir.z, -ood.z), g1 = __fmaf_rn(n2.w, idir.z, -ood.z);
-    float lo1 = fmaxf(fmaxf(fminf(d0, d1), fminf(f0, f1)), fmaxf(fminf(g0, g1), tnear));
-    float hi1 = fminf(fminf(fmaxf(d0, d1), fmaxf(f0, f1)), fminf(fmaxf(g0, g1), tmax));
+    float lo1 = fmax3(fminf(d0, d1), fminf(f0, f1), fmaxf(fminf(g0, g1), tnear));
+    float hi1 = fmin3(fmaxf(d0, d1), fmaxf(f0, f1), fminf(fmaxf(g0, g1), tmax));
     h0 = lo0 <= hi0 * 1.0000003f;
     h1 = lo1 <= hi1 * 1.0000003f;
     e0 = lo0;
@@ -428,20 +442,37 @@ __device__ __forceinline__ void ray_loop(const DevScene& s, Gen& g, int refill, 
 
 // ray_loop over a shared list of work items (lumels) instead of one per
 // lane: a lane whose item has no rays left takes the next item from its
-// warp's pool, and the warp refills the pool `chunk` items at a time from
-// the global `counter` (items [0, count)).  Lanes therefore keep tracing
-// until the list runs dry, instead of idling until the warp's slowest item
-// is done, and a persistent grid has no wave tail.  Neighbouring items of a
-// chunk stay in one warp (coherent rays).  Each item is still one lane's
-// rays in order, so results are those of ray_loop.  The generator adds:
+// warp's pool, and the warp refills the pool from `src` (src.claim(lo, hi):
+// called by the whole warp, gives the same [lo, hi) to every lane, false
+// when the source is dry).  Lanes therefore keep tracing until the source
+// runs dry, instead of idling until the warp's slowest item is done, and a
+// persistent grid has no wave tail.  Neighbouring items of a chunk stay in
+// one warp (coherent rays).  Each item is still one lane's rays in order,
+// so results are those of ray_loop.  The generator adds:
 //   has_more()        the current item has rays left
 //   end_item()        the current item is done (write its result); no-op
 //                     when the lane holds none
 //   start_item(k)     take item k; false if k is not to be baked (then the
 //                     lane takes another)
-template <bool kAny, typename Gen>
-__device__ __forceinline__ void ray_loop_pool(const DevScene& s, Gen& g, int refill, int* overflow,
-                                              unsigned long long* counter, long long count, int chunk) {
+
+// A source of `chunk` consecutive items [0, count) from a global counter.
+struct CounterSource {
+    unsigned long long* counter;
+    long long count;
+    int chunk;
+    __device__ __forceinline__ bool claim(long long& lo, long long& hi) {
+        unsigned long long base = 0;
+        if ((threadIdx.x & 31) == 0) base = atomicAdd(counter, (unsigned long long)chunk);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if ((long long)base >= count) return false;
+        lo = (long long)base;
+        hi = lo + chunk < count ? lo + chunk : count;
+        return true;
+    }
+};
+
+template <bool kAny, typename Gen, typename Src>
+__device__ __forceinline__ void ray_loop_pool(const DevScene& s, Gen& g, int refill, int* overflow, Src& src) {
     V3 o = mk3(0.f, 0.f, 0.f), d = o, idir = o, ood = o;
     float tnear = 0.f, tfar = 0.f, best = 0.f;
     int best_gid = 0x7fffffff;
@@ -470,15 +501,10 @@ __device__ __forceinline__ void ray_loop_pool(const DevScene& s, Gen& g, int ref
             while (wm) {
                 if (pool_next >= pool_end) {
                     if (dry) break;
-                    unsigned long long base = 0;
-                    if ((threadIdx.x & 31) == 0) base = atomicAdd(counter, (unsigned long long)chunk);
-                    base = __shfl_sync(0xffffffffu, base, 0);
-                    if ((long long)base >= count) {
+                    if (!src.claim(pool_next, pool_end)) {
                         dry = true;
                         break;
                     }
-                    pool_next = (long long)base;
-                    pool_end = (long long)base + chunk < count ? (long long)base + chunk : count;
                 }
                 const long long item = pool_next + __popc(wm & lanes_below);
                 if (want && item < pool_end && g.start_item(item)) want = false;

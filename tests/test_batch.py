@@ -24,16 +24,25 @@ def _colors(res):
 
 
 @pytest.mark.gpu
-def test_batch_matches_per_job_loop(cuda):
+@pytest.mark.parametrize("pool", [1, 0])
+def test_batch_matches_per_job_loop(cuda, pool):
+    """pool: the AO and final-gather batch kernels with per-warp lumel pools
+    (k_batch_pool, the default) or one lumel per lane per chunk (k_batch);
+    the per-job loop runs with the same setting."""
     import torch
-    from relight_b200 import batch
-    res = batch.make_resident(_small_workload())
-    batch.run_per_job(res.jobs)
-    torch.cuda.synchronize()
-    want = _colors(res)
-    assert any(np.abs(w).sum() > 0 for w in want)
-    res.clear()
-    b = batch.Batch(res.jobs)
+    from relight_b200 import autotune, batch
+    saved = autotune.get_pool()
+    autotune.set_pool(pool)
+    try:
+        res = batch.make_resident(_small_workload())
+        batch.run_per_job(res.jobs)
+        torch.cuda.synchronize()
+        want = _colors(res)
+        assert any(np.abs(w).sum() > 0 for w in want)
+        res.clear()
+        b = batch.Batch(res.jobs)
+    finally:
+        autotune.set_pool(*saved)
     assert b.work_items == 3 * sum(m.width * m.height for m in res.lightmaps)
     b.launch()
     torch.cuda.synchronize()

@@ -1063,6 +1063,24 @@ extern "C" int rl_bake_direct(const rl_scene* s, rl_map* lm, const rl_light* lig
     return RL_OK;
 }
 
+// Blocks of `threads` that fit on the device at once for `kernel`
+// (persistent grids), cached per kernel and block size.
+template <typename K>
+static int resident_blocks(K kernel, int threads) {
+    static std::mutex mu;
+    static std::map<std::pair<const void*, int>, int> cache;
+    std::lock_guard<std::mutex> g(mu);
+    const auto key = std::make_pair((const void*)kernel, threads);
+    auto f = cache.find(key);
+    if (f != cache.end()) return f->second;
+    int dev = 0, sms = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) !=
+                                                  cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0) != cudaSuccess || per_sm <= 0)
+        return 0;
+    return cache[key] = sms * per_sm;
+}
+
 // ------------------------------------------------------------------ AO
 
 // AmbientOcclusion::bakeLumel (baker/AmbientOcclusion.cpp:46-66): the
@@ -1122,6 +1140,65 @@ __global__ void __launch_bounds__(256) k_ao(DevScene s, DevMap m, int samples, f
     col[0] = col[0] * value; col[1] = col[1] * value; col[2] = col[2] * value;
 }
 
+// AoGen over a work list of lumels (ray_loop_pool): lumel item k of the
+// iteration (items k_begin + k, k < limit), its samples in order, its colour
+// scaled when its last sample is counted — the same arithmetic as k_ao.
+struct AoPoolGen : AoGen {
+    const DevMap* map;
+    const Iter* it;
+    int nsamples;
+    float fraction, exponent;
+    long long li, k_begin, limit;
+    __device__ bool has_more() const { return j < samples; }
+    __device__ void end_item() {
+        if (samples == 0) return;
+        float value = 1.0f - occluded / (samples * fraction);
+        if (fabsf(1.0f - exponent) > 0.01f) value = powf(value, exponent);
+        float* col = map->color + 3 * li;
+        col[0] = col[0] * value; col[1] = col[1] * value; col[2] = col[2] * value;
+        samples = 0;
+    }
+    __device__ bool start_item(long long k) {
+        long long i;
+        if (k >= limit || !iter_lumel(*map, *it, k_begin + k, i)) return false;
+        li = i;
+        pos = ld3(map->position + 3 * i);
+        nrm = ld3(map->normal + 3 * i);
+        item = (uint32_t)i;
+        j = 0;
+        samples = nsamples;
+        occluded = 0;
+        return true;
+    }
+};
+
+// Persistent AO over a whole-lumel work list (one lane per lumel at a time,
+// lanes refilled from their warp's pool), for maps that need no lane split.
+__global__ void __launch_bounds__(256, 4) k_ao_pool(DevScene s, const __grid_constant__ DevMap m, int samples,
+                                                    float fraction, float maxd, float exponent, uint2 key,
+                                                    const __grid_constant__ Iter it, long long count, int refill,
+                                                    int* status, unsigned long long* counter, int chunk) {
+    AoPoolGen g;
+    g.map = &m;
+    g.it = &it;
+    g.nsamples = samples;
+    g.fraction = fraction;
+    g.exponent = exponent;
+    g.li = 0;
+    g.k_begin = 0;
+    g.limit = count;
+    g.pos = g.nrm = mk3(0.f, 0.f, 0.f);
+    g.key = key;
+    g.item = 0;
+    g.j = 0;
+    g.stride = 1;
+    g.samples = 0;
+    g.occluded = 0;
+    g.maxd = maxd;
+    CounterSource src{counter, count, chunk};
+    ray_loop_pool<true>(s, g, refill, status, src);
+}
+
 extern "C" int rl_bake_ao(const rl_scene* s, rl_map* lm, int samples, float fraction, float maxd, float exponent,
                           uint64_t seed, const rl_iterator* iterator, void* stream) {
     if (!s || !lm) return fail(RL_INVALID_CALL, "rl_bake_ao: null argument");
@@ -1150,6 +1227,18 @@ extern "C" int rl_bake_ao(const rl_scene* s, rl_map* lm, int samples, float frac
     int bs = g_tune[RL_TUNE_AO_BLOCK];
     bool wide = g_tune[RL_TUNE_BVH_WIDTH] == 4 && s->dev.nodes4 != nullptr;
     bool wide8 = g_tune[RL_TUNE_BVH_WIDTH] == 8 && s->dev.nodes8 != nullptr;
+    if (split == 1 && g_tune[RL_TUNE_FG_POOL] && !wide && !wide8 && !g_tune[RL_TUNE_SPECULATIVE]) {
+        const int resident = resident_blocks(k_ao_pool, bs);
+        if (resident <= 0) return fail(RL_CUDA_ERROR, "k_ao_pool: occupancy query failed");
+        const long long want = ((long long)count + bs - 1) / bs;
+        const unsigned grid = (unsigned)(want < resident ? want : resident);
+        CK(cudaMemsetAsync(lm->d_work, 0, sizeof(unsigned long long), S(stream)));
+        k_ao_pool<<<grid, bs, 0, S(stream)>>>(s->dev, lm->dev, samples, fraction, maxd, exponent, key, it, count,
+                                              g_tune[RL_TUNE_AO_REFILL], s->d_status, lm->d_work,
+                                              g_tune[RL_TUNE_FG_CHUNK]);
+        CK_LAUNCH("k_ao_pool");
+        return RL_OK;
+    }
     auto kern = wide8 ? k_ao<8> : wide ? k_ao<4> : (g_tune[RL_TUNE_SPECULATIVE] ? k_ao<3> : k_ao<2>);
     kern<<<blocks_for(count * split, bs), bs, 0, S(stream)>>>(s->dev, lm->dev, samples, fraction, maxd, exponent,
                                                               key, it, count * split, split,
@@ -1523,24 +1612,6 @@ __global__ void __launch_bounds__(256, 4) k_indirect_pool(DevScene s, const __gr
     g.pos = g.nrm = g.dir = mk3(0.f, 0.f, 0.f);
     CounterSource src{counter, count, chunk};
     ray_loop_pool<false>(s, g, refill, status, src);
-}
-
-// Blocks of `threads` that fit on the device at once for `kernel`
-// (persistent grids), cached per kernel and block size.
-template <typename K>
-static int resident_blocks(K kernel, int threads) {
-    static std::mutex mu;
-    static std::map<std::pair<const void*, int>, int> cache;
-    std::lock_guard<std::mutex> g(mu);
-    const auto key = std::make_pair((const void*)kernel, threads);
-    auto f = cache.find(key);
-    if (f != cache.end()) return f->second;
-    int dev = 0, sms = 0, per_sm = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) !=
-                                                  cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0) != cudaSuccess || per_sm <= 0)
-        return 0;
-    return cache[key] = sms * per_sm;
 }
 
 extern "C" int rl_bake_indirect(const rl_scene* s, rl_map* lm, rl_map* const* maps, int nmaps, int samples,
@@ -2472,36 +2543,6 @@ __global__ void __launch_bounds__(kKind == 0 ? 128 : 256, kKind == 0 ? 1 : 4) k_
         __syncwarp();
     }
 }
-
-// AoGen over a work list of lumels (ray_loop_pool), as FgPoolGen.
-struct AoPoolGen : AoGen {
-    const DevMap* map;
-    const Iter* it;
-    int nsamples;
-    float fraction, exponent;
-    long long li, k_begin, limit;
-    __device__ bool has_more() const { return j < samples; }
-    __device__ void end_item() {
-        if (samples == 0) return;
-        float value = 1.0f - occluded / (samples * fraction);
-        if (fabsf(1.0f - exponent) > 0.01f) value = powf(value, exponent);
-        float* col = map->color + 3 * li;
-        col[0] = col[0] * value; col[1] = col[1] * value; col[2] = col[2] * value;
-        samples = 0;
-    }
-    __device__ bool start_item(long long k) {
-        long long i;
-        if (k >= limit || !iter_lumel(*map, *it, k_begin + k, i)) return false;
-        li = i;
-        pos = ld3(map->position + 3 * i);
-        nrm = ld3(map->normal + 3 * i);
-        item = (uint32_t)i;
-        j = 0;
-        samples = nsamples;
-        occluded = 0;
-        return true;
-    }
-};
 
 // Work source of the pooled batch kernel: the kind's 32-item chunks in
 // counter order, restricted to one job ([job_lo, job_hi) of the kind's item

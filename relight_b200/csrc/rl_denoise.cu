@@ -172,6 +172,16 @@ __device__ __forceinline__ uint64_t desc_sw128(uint32_t saddr, uint32_t lbo_byte
            ((uint64_t)((sbo_bytes >> 4) & 0x3FFF) << 32) | (1ull << 46) | (2ull << 61);
 }
 
+// K-major operand whose rows are `kb` BF16 channels (16, 32 or 64: rows of
+// 32, 64 or 128 bytes, TMA's 32 / 64 / 128-byte swizzle): layout type 6 / 4
+// / 2, eight-row groups 8 x row bytes apart.
+__device__ __forceinline__ uint64_t desc_kmajor(uint32_t saddr, int kb) {
+    const uint32_t row = (uint32_t)kb * 2;
+    const uint64_t layout = kb == 64 ? 2ull : kb == 32 ? 4ull : 6ull;
+    return (uint64_t)((saddr >> 4) & 0x3FFF) | (1ull << 16) | ((uint64_t)(((8 * row) >> 4) & 0x3FFF) << 32) |
+           (1ull << 46) | (layout << 61);
+}
+
 // Instruction descriptor of kind::f16: BF16 A and B, FP32 D, M = 128.
 __host__ __device__ constexpr uint32_t idesc_bf16(int n, bool a_mn_major, bool b_mn_major) {
     return (1u << 4) | (1u << 7) | (1u << 10) | ((a_mn_major ? 1u : 0u) << 15) | ((b_mn_major ? 1u : 0u) << 16) |
@@ -190,7 +200,9 @@ constexpr uint32_t kABytes = 128 * 128;   // 128 pixels x 64 channels x 2 bytes
 
 struct ConvArgs {
     int W, H;              // spatial size (input = output)
-    int nblk[2];           // 64-channel blocks per input segment
+    int nblk[2];           // channel blocks per input segment
+    int kb[2];             // channels per block of each segment: 16, 32 or 64
+    int woff[2];           // first weight column (input channel) of each segment
     int ncols;             // MMA N = output channels (multiple of 16, <= 256)
     int tmem_cols;         // power of two >= max(32, ncols)
     int stages;
@@ -264,7 +276,8 @@ constexpr int kConvPThreads = 192;
 
 __global__ void __launch_bounds__(kConvPThreads, 1) k_conv3x3_p(const __grid_constant__ CUtensorMap tmA0,
                                                                const __grid_constant__ CUtensorMap tmA1,
-                                                               const __grid_constant__ CUtensorMap tmB,
+                                                               const __grid_constant__ CUtensorMap tmB0,
+                                                               const __grid_constant__ CUtensorMap tmB1,
                                                                const ConvArgs a, int tiles_x, int tiles_y,
                                                                int ntiles) {
     extern __shared__ uint8_t smem_raw[];
@@ -316,10 +329,11 @@ __global__ void __launch_bounds__(kConvPThreads, 1) k_conv3x3_p(const __grid_con
                 }
                 const int tap = kb / per_tap, j = kb % per_tap;
                 const int seg = j < a.nblk[0] ? 0 : 1, cb = seg ? j - a.nblk[0] : j;
-                mbar_expect_tx(full + s, kABytes + b_bytes);
-                tma_load_4d(sa + s * kABytes, seg ? &tmA1 : &tmA0, full + s, cb * 64, x0 + tap % 3 - 1,
+                const int w = a.kb[seg];
+                mbar_expect_tx(full + s, (uint32_t)(128 * w * 2 + a.ncols * w * 2));
+                tma_load_4d(sa + s * kABytes, seg ? &tmA1 : &tmA0, full + s, cb * w, x0 + tap % 3 - 1,
                             y0 + tap / 3 - 1, img);
-                tma_load_3d(sb + s * b_bytes, &tmB, full + s, j * 64, tap, 0);
+                tma_load_3d(sb + s * b_bytes, seg ? &tmB1 : &tmB0, full + s, a.woff[seg] + cb * w, tap, 0);
             }
         }
         for (long long k = g > S ? g - S : 0; k < g; k++) mbar_wait(full + k % S, (uint32_t)((k / S) & 1), a.err, 64);
@@ -340,10 +354,12 @@ __global__ void __launch_bounds__(kConvPThreads, 1) k_conv3x3_p(const __grid_con
                     break;
                 }
                 tc_fence_after();
-                const uint64_t ad = desc_sw128(smem_u32(sa + s * kABytes), 16, 1024);
-                const uint64_t bd = desc_sw128(smem_u32(sb + s * b_bytes), 16, 1024);
-#pragma unroll
-                for (int kk = 0; kk < 4; kk++) umma_bf16(d, ad + 2 * kk, bd + 2 * kk, idesc, (kb | kk) != 0);
+                const int j = kb % per_tap;
+                const int w = a.kb[j < a.nblk[0] ? 0 : 1];
+                const uint64_t ad = desc_kmajor(smem_u32(sa + s * kABytes), w);
+                const uint64_t bd = desc_kmajor(smem_u32(sb + s * b_bytes), w);
+                // K = 16 channels (32 bytes) per MMA, stepping along the swizzled row
+                for (int kk = 0; kk < w / 16; kk++) umma_bf16(d, ad + 2 * kk, bd + 2 * kk, idesc, (kb | kk) != 0);
                 umma_commit(empty + s);
             }
             umma_commit(accf + buf);  // also after a timeout: the epilogue then waits for the issued MMAs
@@ -508,34 +524,48 @@ EncodeTiledFn encode_fn() {
     return fn;
 }
 
-// NHWC BF16 activations [n][h][w][c] (c a multiple of 8), boxes of 64
-// channels x 16 x 8 pixels, 128-byte swizzle, zero fill outside.
-int act_map(CUtensorMap* tm, const void* base, int c, int w, int h, int n) {
+// TMA swizzle for rows of `kb` BF16 channels (the UMMA layouts of desc_kmajor).
+CUtensorMapSwizzle swizzle_for(int kb) {
+    return kb == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : kb == 32 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B;
+}
+
+// Channels per K-block for a segment of c channels: the narrowest of 16 /
+// 32 / 64 that tiles c without a partial block, 64 where several fit.
+int block_channels(int c) {
+    if (c <= 16) return 16;
+    if (c <= 32) return 32;
+    if (c % 64 == 0) return 64;
+    return c % 32 == 0 ? 32 : 16;
+}
+
+// NHWC BF16 activations [n][h][w][c] (c a multiple of 8), boxes of `kb`
+// channels x 16 x 8 pixels, swizzled for kb, zero fill outside.
+int act_map(CUtensorMap* tm, const void* base, int c, int w, int h, int n, int kb = 64) {
     EncodeTiledFn fn = encode_fn();
     if (!fn) return dn_fail(RL_CUDA_ERROR, "cuTensorMapEncodeTiled unavailable");
     if (c % 8 || ((uintptr_t)base & 15)) return dn_fail(RL_INVALID_CALL, "activation layout: %d channels", c);
     cuuint64_t dims[4] = {(cuuint64_t)c, (cuuint64_t)w, (cuuint64_t)h, (cuuint64_t)n};
     cuuint64_t strides[3] = {(cuuint64_t)c * 2, (cuuint64_t)c * 2 * w, (cuuint64_t)c * 2 * w * h};
-    cuuint32_t box[4] = {64, kTileW, kTileH, 1};
+    cuuint32_t box[4] = {(cuuint32_t)kb, kTileW, kTileH, 1};
     cuuint32_t es[4] = {1, 1, 1, 1};
     CUresult r = fn(tm, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(base), dims, strides, box, es,
-                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle_for(kb), CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return dn_fail(RL_CUDA_ERROR, "tensor map (activation) error %d", (int)r);
     return RL_OK;
 }
 
-// Weights [rows][9][k] (k a multiple of 64), boxes of 64 x 1 x rows.
-int weight_map(CUtensorMap* tm, const void* base, int k, int rows) {
+// Weights [rows][9][k] (k a multiple of 64), boxes of kb x 1 x rows.
+int weight_map(CUtensorMap* tm, const void* base, int k, int rows, int kb = 64) {
     EncodeTiledFn fn = encode_fn();
     if (!fn) return dn_fail(RL_CUDA_ERROR, "cuTensorMapEncodeTiled unavailable");
     if (k % 64 || rows > 256 || rows % 16) return dn_fail(RL_INVALID_CALL, "weight layout %d x %d", rows, k);
     cuuint64_t dims[3] = {(cuuint64_t)k, 9, (cuuint64_t)rows};
     cuuint64_t strides[2] = {(cuuint64_t)k * 2, (cuuint64_t)k * 2 * 9};
-    cuuint32_t box[3] = {64, 1, (cuuint32_t)rows};
+    cuuint32_t box[3] = {(cuuint32_t)kb, 1, (cuuint32_t)rows};
     cuuint32_t es[3] = {1, 1, 1};
     CUresult r = fn(tm, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void*>(base), dims, strides, box, es,
-                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle_for(kb), CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return dn_fail(RL_CUDA_ERROR, "tensor map (weights) error %d", (int)r);
     return RL_OK;
@@ -558,22 +588,32 @@ extern "C" int rl_dn_conv3x3(const void* in0, int c0, const void* in1, int c1, i
     if (!in0 || !weights || !out0 || width <= 0 || height <= 0 || images <= 0)
         return dn_fail(RL_INVALID_CALL, "rl_dn_conv3x3: bad arguments");
     if (ncols < 16 || ncols > 256 || ncols % 16) return dn_fail(RL_INVALID_CALL, "rl_dn_conv3x3: ncols %d", ncols);
-    const int nb0 = (c0 + 63) / 64, nb1 = in1 ? (c1 + 63) / 64 : 0;
+    // K-blocks as wide as each segment's channels need (16, 32 or 64): the
+    // weights keep each segment padded to 64 columns, the boxes read only
+    // the block's own columns
+    const int kb0 = block_channels(c0), kb1 = in1 ? block_channels(c1) : 64;
+    const int nb0 = (c0 + kb0 - 1) / kb0, nb1 = in1 ? (c1 + kb1 - 1) / kb1 : 0;
+    const int kpad = 64 * ((c0 + 63) / 64 + (in1 ? (c1 + 63) / 64 : 0));
     const int nout = out1 ? 2 : 1;
     const int oc0[2] = {out0_c0, out1_c0}, ocn[2] = {out0_cn, out1_cn}, ocs[2] = {out0_cs, out1_cs};
     for (int o = 0; o < nout; o++)
         if (ocn[o] % 16 || ocs[o] % 16 || oc0[o] % 16 || ocn[o] > ocs[o] || oc0[o] + ocn[o] > ncols)
             return dn_fail(RL_INVALID_CALL, "rl_dn_conv3x3: output segment %d", o);
-    CUtensorMap tA0, tA1, tB;
-    if (int rc = act_map(&tA0, in0, c0, width, height, images)) return rc;
-    if (int rc = act_map(&tA1, in1 ? in1 : in0, in1 ? c1 : c0, width, height, images)) return rc;
-    if (int rc = weight_map(&tB, weights, 64 * (nb0 + nb1), ncols)) return rc;
+    CUtensorMap tA0, tA1, tB0, tB1;
+    if (int rc = act_map(&tA0, in0, c0, width, height, images, kb0)) return rc;
+    if (int rc = act_map(&tA1, in1 ? in1 : in0, in1 ? c1 : c0, width, height, images, in1 ? kb1 : kb0)) return rc;
+    if (int rc = weight_map(&tB0, weights, kpad, ncols, kb0)) return rc;
+    if (int rc = weight_map(&tB1, weights, kpad, ncols, kb1)) return rc;
     ConvArgs a;
     memset(&a, 0, sizeof a);
     a.W = width;
     a.H = height;
     a.nblk[0] = nb0;
     a.nblk[1] = nb1;
+    a.kb[0] = kb0;
+    a.kb[1] = kb1;
+    a.woff[0] = 0;
+    a.woff[1] = 64 * ((c0 + 63) / 64);
     a.ncols = ncols;
     a.tmem_cols = pow2_cols(ncols);
     // ring depth: two CTAs per SM while both fit in TMEM (2 x 2 accumulators of
@@ -611,7 +651,7 @@ extern "C" int rl_dn_conv3x3(const void* in0, int c0, const void* in1, int c1, i
     const long long ntiles = (long long)tiles_x * tiles_y * images;
     if (ntiles > INT32_MAX) return dn_fail(RL_INVALID_CALL, "rl_dn_conv3x3: too many tiles");
     const int grid = (int)std::min<long long>(ntiles, (long long)per_sm * std::max(sms, 1));
-    k_conv3x3_p<<<grid, kConvPThreads, smem, (cudaStream_t)stream>>>(tA0, tA1, tB, a, tiles_x, tiles_y,
+    k_conv3x3_p<<<grid, kConvPThreads, smem, (cudaStream_t)stream>>>(tA0, tA1, tB0, tB1, a, tiles_x, tiles_y,
                                                                     (int)ntiles);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return dn_fail(RL_CUDA_ERROR, "k_conv3x3_p: %s", cudaGetErrorString(e));

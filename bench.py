@@ -1153,6 +1153,38 @@ def radiosity_arm(args):
     return result
 
 
+def _summary(r, keys):
+    out = {k: r[k] for k in keys if k in r}
+    if "roofline" in r:
+        rf = r["roofline"]
+        out["roofline"] = {k: rf[k] for k in ("kernel", "bound", "achieved", "peak", "unit", "frac") if k in rf}
+    if "e2e" in r:
+        out["e2e"] = {k: r["e2e"][k] for k in ("value", "unit") if k in r["e2e"]}
+    if "clocks" in r:
+        out["clocks"] = r["clocks"]
+    return out
+
+
+def other_workloads(args):
+    """The room (direct + AO, 256^2) and radiosity (16,384 patches) workloads,
+    measured after the terrain step in the same run and summarised (their
+    own --workload runs print the full lines)."""
+    import copy
+    out = {}
+    a = copy.copy(args)
+    a.steps, a.warmup, a.no_cpu_baseline = 20, 3, True
+    r = room_arm(a)
+    out["room"] = _summary(r, ("metric", "value", "unit", "ms_per_step", "steps", "ao_ms", "direct_ms",
+                               "ao_grays_per_s"))
+    r = radiosity_arm(a)
+    out["radiosity"] = _summary(r, ("metric", "value", "unit", "ms_per_step", "steps", "ff_ms", "solve_ms",
+                                    "jacobi_vs_fp64_50_iters_max_rel"))
+    pw = r.get("pairwise_form_factors", {})
+    out["radiosity"]["pairwise_form_factors"] = {k: pw[k] for k in ("gpu_ms", "reference_s", "speedup_vs_reference",
+                                                                    "matches_reference", "nnz") if k in pw}
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1160,6 +1192,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the room and radiosity summaries the default terrain line carries")
     ap.add_argument("--small", action="store_true", help="512^2 / 64 spp / 2 passes case for ncu captures")
     ap.add_argument("--bvh-width", type=int, default=0, choices=[0, 2, 4, 8],
                     help="traversal tree for AO / final gather (0: the library's default)")
@@ -1217,6 +1251,8 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb, err = cpu_baseline(w)
         result["cpu_baseline"] = cb if cb else {"unavailable": err}
+    if rank == 0 and world == 1 and not args.split and args.gather == "disc" and not args.no_extras:
+        result["other_workloads"] = other_workloads(args)
     if world > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()

@@ -300,7 +300,7 @@ def gpu_arm(args, rank, world, local_rank):
         "scaling": "strong" if split else "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded fBm terrain + boxes)",
         "config": terrain_config(st, valid, flat.ntris, world, knn, split),
-        "tuning": {"bvh_width": autotune.get_width(), "fg": autotune.get("indirect"),
+        "tuning": {"bvh_width": autotune.get_width(), "fg": autotune.get("indirect"), "fg_pool": autotune.get_pool(),
                    **({"knn_cell_64ths": autotune.get_knn_cell()} if knn else {})},
         "grays_per_s": rays_per_step * args.steps * jobs / (total_ms / 1e3) / 1e9,
         "fg_ms": sum(fg_ms) / len(fg_ms),
@@ -1199,6 +1199,9 @@ def main():
                     help="traversal tree for AO / final gather (0: the library's default)")
     ap.add_argument("--gather", default="disc", choices=["disc", "knn"],
                     help="photon estimate: Relight's disc gather (default) or the k-nearest-neighbour estimate")
+    ap.add_argument("--fg-pool", type=int, default=-1, choices=[-1, 0, 1],
+                    help="final gather / AO / batch kernels with per-warp lumel pools (1) or one lumel per lane (0); "
+                         "-1: the library's default")
     ap.add_argument("--split", action="store_true",
                     help="one terrain bake split over the ranks (photon shares and interleaved final-gather lumels, "
                          "NCCL all-reduces; strong scaling) instead of one bake per rank")
@@ -1218,6 +1221,9 @@ def main():
     if args.knn_cell:
         from relight_b200 import autotune
         autotune.set_knn_cell(args.knn_cell)
+    if args.fg_pool >= 0:
+        from relight_b200 import autotune
+        autotune.set_pool(args.fg_pool)
     if args.workload == "batch":
         print(json.dumps(batch_arm(args)), flush=True)
         return

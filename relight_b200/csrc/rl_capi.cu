@@ -93,7 +93,11 @@ int dupload(T** p, const T* host, size_t count, cudaStream_t st) {
     return RL_OK;
 }
 
-// A stream-ordered scratch buffer freed when it goes out of scope.
+// A stream-ordered scratch buffer freed when it goes out of scope, drawn from
+// the library's memory pool (rl_internal_pool_alloc, below): freed blocks
+// stay mapped for the next call.  The device's default pool returns them at
+// every synchronisation, and a call that waits on the host in its middle
+// (the form factors wait for their row counts) then maps ~100 MB afresh.
 struct Scratch {
     void* p = nullptr;
     cudaStream_t st = nullptr;
@@ -102,12 +106,16 @@ struct Scratch {
     }
 };
 
+}  // namespace
+int rl_internal_pool_alloc(void** p, size_t bytes, cudaStream_t st);
+namespace {
+
 template <typename T>
 int scratch(Scratch& s, T** out, size_t count, cudaStream_t st) {
     s.st = st;
     *out = nullptr;
     if (count == 0) return RL_OK;
-    CK(cudaMallocAsync(&s.p, sizeof(T) * count, st));
+    if (int rc = rl_internal_pool_alloc(&s.p, sizeof(T) * count, st)) return rc;
     *out = (T*)s.p;
     return RL_OK;
 }

@@ -202,6 +202,7 @@ struct ConvArgs {
     int W, H;              // spatial size (input = output)
     int nblk[2];           // channel blocks per input segment
     int kb[2];             // channels per block of each segment: 16, 32 or 64
+    int a_stage, b_stage;  // bytes of one ring stage's A and B tiles (the widest block's)
     int woff[2];           // first weight column (input channel) of each segment
     int ncols;             // MMA N = output channels (multiple of 16, <= 256)
     int tmem_cols;         // power of two >= max(32, ncols)
@@ -283,9 +284,9 @@ __global__ void __launch_bounds__(kConvPThreads, 1) k_conv3x3_p(const __grid_con
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = align1024(smem_raw);
     const int S = a.stages;
-    const uint32_t b_bytes = (uint32_t)a.ncols * 128;
+    const uint32_t a_bytes = (uint32_t)a.a_stage, b_bytes = (uint32_t)a.b_stage;
     uint8_t* sa = smem;
-    uint8_t* sb = smem + S * kABytes;
+    uint8_t* sb = smem + S * a_bytes;
     uint64_t* full = (uint64_t*)(sb + S * b_bytes);
     uint64_t* empty = full + S;
     uint64_t* accf = empty + S;  // accumulator k ready for the epilogue
@@ -331,7 +332,7 @@ __global__ void __launch_bounds__(kConvPThreads, 1) k_conv3x3_p(const __grid_con
                 const int seg = j < a.nblk[0] ? 0 : 1, cb = seg ? j - a.nblk[0] : j;
                 const int w = a.kb[seg];
                 mbar_expect_tx(full + s, (uint32_t)(128 * w * 2 + a.ncols * w * 2));
-                tma_load_4d(sa + s * kABytes, seg ? &tmA1 : &tmA0, full + s, cb * w, x0 + tap % 3 - 1,
+                tma_load_4d(sa + s * a_bytes, seg ? &tmA1 : &tmA0, full + s, cb * w, x0 + tap % 3 - 1,
                             y0 + tap / 3 - 1, img);
                 tma_load_3d(sb + s * b_bytes, seg ? &tmB1 : &tmB0, full + s, a.woff[seg] + cb * w, tap, 0);
             }
@@ -356,7 +357,7 @@ __global__ void __launch_bounds__(kConvPThreads, 1) k_conv3x3_p(const __grid_con
                 tc_fence_after();
                 const int j = kb % per_tap;
                 const int w = a.kb[j < a.nblk[0] ? 0 : 1];
-                const uint64_t ad = desc_kmajor(smem_u32(sa + s * kABytes), w);
+                const uint64_t ad = desc_kmajor(smem_u32(sa + s * a_bytes), w);
                 const uint64_t bd = desc_kmajor(smem_u32(sb + s * b_bytes), w);
                 // K = 16 channels (32 bytes) per MMA, stepping along the swizzled row
                 for (int kk = 0; kk < w / 16; kk++) umma_bf16(d, ad + 2 * kk, bd + 2 * kk, idesc, (kb | kk) != 0);
@@ -574,7 +575,7 @@ int weight_map(CUtensorMap* tm, const void* base, int k, int rows, int kb = 64) 
 
 int pow2_cols(int n) { return n <= 32 ? 32 : n <= 64 ? 64 : n <= 128 ? 128 : 256; }
 
-int conv_smem(int ncols, int stages) { return stages * (int)(kABytes + ncols * 128) + (2 * stages + 4) * 8 + 16 + 1024; }
+int conv_smem(int stage_bytes, int stages) { return stages * stage_bytes + (2 * stages + 4) * 8 + 16 + 1024; }
 
 }  // namespace
 
@@ -621,8 +622,14 @@ extern "C" int rl_dn_conv3x3(const void* in0, int c0, const void* in1, int c1, i
     // <= 128 columns), each with up to ~100 KB of stages; otherwise one CTA
     // with up to ~200 KB
     const int per_sm = pow2_cols(ncols) <= 128 ? 2 : 1;
-    const int stage_bytes = (int)(kABytes + ncols * 128);
-    a.stages = std::max(2, std::min(8, (per_sm == 2 ? 100 : 200) * 1024 / stage_bytes));
+    // a stage holds the widest block the layer uses: narrow layers get small
+    // stages and a deeper ring (up to 24 K-blocks in flight), which is what
+    // hides the load latency when each K-block carries little work
+    const int kbmax = std::max(kb0, in1 ? kb1 : 0);
+    a.a_stage = 128 * kbmax * 2;
+    a.b_stage = ncols * kbmax * 2;
+    const int stage_bytes = a.a_stage + a.b_stage;
+    a.stages = std::max(2, std::min(24, (per_sm == 2 ? 100 : 200) * 1024 / stage_bytes));
     a.bias = bias;
     a.relu = relu;
     a.slope = slope;
@@ -637,7 +644,7 @@ extern "C" int rl_dn_conv3x3(const void* in0, int c0, const void* in1, int c1, i
     a.mask[0] = (const bf16*)mask0;
     a.mask[1] = (const bf16*)mask1;
     a.err = d_err;
-    const int smem = conv_smem(ncols, a.stages);
+    const int smem = conv_smem(stage_bytes, a.stages);
     static int sms = 0;
     static std::once_flag attr;
     cudaError_t ae = cudaSuccess;

@@ -381,12 +381,16 @@ def _main():
         e1.record()
         e1.synchronize()
         ms.append(e0.elapsed_time(e1))
-    # multiply-adds of the 8 convolutions (MMA shapes, padding included)
+    # multiply-adds of the 8 convolutions as the MMAs run them: K padded to the
+    # kernel's channel blocks (16 or 32 for segments that fit one, else 64s)
+    def kblocks(c):
+        return 16 if c <= 16 else 32 if c <= 32 else _pad64(c)
+
     flops, s = 0, args.side
     sizes = [s, (s + 1) // 2, (s + 3) // 4, (s + 7) // 8]
     levels = [0, 1, 2, 3, 2, 1, 0, 0]
     for (cout, segs), lv in zip(LAYERS, levels):
-        k = 9 * sum(_pad64(c) for c in segs)
+        k = 9 * sum(kblocks(c) for c in segs)
         flops += 2 * sizes[lv] ** 2 * ((cout + 15) // 16 * 16) * k
     print(json.dumps({"side": args.side, "forward_ms": min(ms), "mma_tflops": flops / (min(ms) / 1e3) / 1e12,
                       "status": dn.status()}))

@@ -530,15 +530,13 @@ CUtensorMapSwizzle swizzle_for(int kb) {
     return kb == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : kb == 32 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B;
 }
 
-// Channels per K-block for a segment of c channels: 16 or 32 when the
-// segment fits in one such block, else 64.  Narrower blocks never add
-// K-blocks: each costs a barrier round trip and an MMA issue, which at these
-// channel counts weigh more than the bytes a narrower box saves.
-int block_channels(int c) {
-    if (c <= 16) return 16;
-    if (c <= 32) return 32;
-    return 64;
-}
+// Channels per K-block: 64 for every segment.  The kernel also takes 16- and
+// 32-channel blocks (32 / 64-byte swizzle) for narrow segments, which move a
+// quarter / half of the bytes; measured on the 1024^2 forward pass they were
+// slower (0.97-0.99 ms against 0.85 ms): TMA boxes with 32- or 64-byte rows
+// move less per request than the zero-filled 128-byte ones, and the pipeline
+// is bound by requests in flight, not bytes.
+int block_channels(int) { return 64; }
 
 // NHWC BF16 activations [n][h][w][c] (c a multiple of 8), boxes of `kb`
 // channels x 16 x 8 pixels, swizzled for kb, zero fill outside.

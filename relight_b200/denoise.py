@@ -382,9 +382,9 @@ def _main():
         e1.synchronize()
         ms.append(e0.elapsed_time(e1))
     # multiply-adds of the 8 convolutions as the MMAs run them: K padded to the
-    # kernel's channel blocks (16 or 32 for segments that fit one, else 64s)
+    # kernel's 64-channel blocks
     def kblocks(c):
-        return 16 if c <= 16 else 32 if c <= 32 else _pad64(c)
+        return _pad64(c)
 
     flops, s = 0, args.side
     sizes = [s, (s + 1) // 2, (s + 3) // 4, (s + 7) // 8]

@@ -344,9 +344,10 @@ int rl_obj_mesh_destroy(rl_obj_mesh* mesh);
 
    rl_dn_conv3x3: out = act(conv3x3(concat(in0, in1)) + bias) with zero
    padding; c0 / c1 are the inputs' stored channel counts (multiples of 8).
-   `weights` is BF16 [ncols][9][64*(ceil(c0/64) + ceil(c1/64))], tap =
-   3*(dy+1) + (dx+1), each input segment's channels starting at a multiple
-   of 64 (zero-padded).  Accumulator columns
+   `weights` is BF16 [9][K/8][ncols][8] (16-byte aligned), K = 16*(ceil(c0/16)
+   + ceil(c1/16)): tap = 3*(dy+1) + (dx+1), then blocks of 8 input channels
+   (segment 0's, zero-padded to a multiple of 16, then segment 1's), then
+   output channels, then the 8 channels of the block.  Accumulator columns
    [outK_c0, outK_c0 + outK_cn) go to outK (channel stride outK_cs), times
    (maskK > 0 ? 1 : slope) when maskK is given; relu != 0 applies a leaky
    ReLU of negative slope `slope` (0: ReLU); in1/out1 may be NULL. */

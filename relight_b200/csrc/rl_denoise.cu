@@ -111,14 +111,6 @@ __device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* tm, ui
         : "memory");
 }
 
-__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* tm, uint64_t* bar, int c0, int c1, int c2) {
-    asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, "
-        "%5}], [%2];" ::"r"(smem_u32(dst)),
-        "l"(tm), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2)
-        : "memory");
-}
-
 __device__ __forceinline__ void tmem_alloc(uint32_t* slot, uint32_t ncols) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(slot)), "r"(ncols)
                  : "memory");
@@ -172,16 +164,6 @@ __device__ __forceinline__ uint64_t desc_sw128(uint32_t saddr, uint32_t lbo_byte
            ((uint64_t)((sbo_bytes >> 4) & 0x3FFF) << 32) | (1ull << 46) | (2ull << 61);
 }
 
-// K-major operand whose rows are `kb` BF16 channels (16, 32 or 64: rows of
-// 32, 64 or 128 bytes, TMA's 32 / 64 / 128-byte swizzle): layout type 6 / 4
-// / 2, eight-row groups 8 x row bytes apart.
-__device__ __forceinline__ uint64_t desc_kmajor(uint32_t saddr, int kb) {
-    const uint32_t row = (uint32_t)kb * 2;
-    const uint64_t layout = kb == 64 ? 2ull : kb == 32 ? 4ull : 6ull;
-    return (uint64_t)((saddr >> 4) & 0x3FFF) | (1ull << 16) | ((uint64_t)(((8 * row) >> 4) & 0x3FFF) << 32) |
-           (1ull << 46) | (layout << 61);
-}
-
 // Instruction descriptor of kind::f16: BF16 A and B, FP32 D, M = 128.
 __host__ __device__ constexpr uint32_t idesc_bf16(int n, bool a_mn_major, bool b_mn_major) {
     return (1u << 4) | (1u << 7) | (1u << 10) | ((a_mn_major ? 1u : 0u) << 15) | ((b_mn_major ? 1u : 0u) << 16) |
@@ -194,19 +176,64 @@ __device__ __forceinline__ uint8_t* align1024(uint8_t* p) {
 }
 
 // ------------------------------------------------------- the conv kernel
+//
+// Implicit-GEMM 3x3 convolution over a halo tile.  A tile is 128 output
+// pixels, 16 rows of 8 (TMEM lane m = pixel (m % 8, m / 8) of the tile).
+// Its input halo, 18 rows of 10 pixels, is staged once per tile in shared
+// memory by TMA as one plane per 8 input channels (one 5-D box of 8 channels
+// x 10 x 18 pixels, zero fill outside the image): pixel-major, 16 bytes per
+// pixel, which is the tensor core's unswizzled K-major layout (core matrices
+// of 8 pixels x 8 channels, 128 contiguous bytes).  The nine taps are nine
+// descriptor views of the same halo, started (ky * 10 + kx) pixels in, with
+// rows of 8 pixels 160 bytes apart: a tap reads no global memory.  Weights
+// are packed BF16 [9][K/8][ncols][8] in the same layout (core matrices of 8
+// output x 8 input channels), resident in shared memory when all nine taps
+// fit beside two halo stages, else streamed through a ring of units (a run
+// of one tap's 16-channel K-steps).
+//
+// One tcgen05.mma occupies its issuing thread for about 150 cycles whatever
+// its N, so at these channel counts (N = 16-128) a single issuing thread
+// keeps the tensor pipe mostly idle, while issuers on different SM
+// sub-partitions run concurrently.  Each tile's MMAs (9 taps x K/16) are
+// therefore split among `issuers` threads, one per sub-partition (contiguous
+// runs with resident weights, streamed units round-robin), each accumulating
+// a partial sum in its own TMEM columns; the epilogue adds the partials.
+//
+// Roles (one CTA per SM walks tiles blockIdx.x, blockIdx.x + gridDim.x, ...):
+//   warp 0    tensor memory; the halo loads (HS-stage ring);
+//   warp 1    the weight copies (nine bulk copies once, or one per unit);
+//   warps 2-5 the epilogue (warp w owns TMEM lanes 32 (w % 4) .. +31), which
+//             drains accumulator set i % nbuf while the issuers fill the other;
+//   warps 6-9 the MMA issuers (lane 0 of each; warp 6 + k is issuer k);
+//   warps 10-13 a second epilogue group when there are two accumulator sets:
+//             groups 0 and 1 take the even and odd tiles.
 
-constexpr int kTileW = 16, kTileH = 8;   // 128 output pixels per tile
+constexpr int kTileW = 16, kTileH = 8;    // the weight gradient's pixel tile: 128 pixels
 constexpr uint32_t kABytes = 128 * 128;   // 128 pixels x 64 channels x 2 bytes
+constexpr int kHTileW = 8, kHTileH = 16;  // the convolution's pixel tile
+constexpr int kHaloW = kHTileW + 2, kHaloH = kHTileH + 2;
+constexpr uint32_t kPlaneBox = kHaloW * kHaloH * 16;  // 2880 bytes of one plane
+constexpr uint32_t kPlaneBytes = 2944;                // plane stride: 2880 rounded up to 128 bytes
+constexpr int kMaxIssuers = 4;
+constexpr int kConvThreads = (10 + kMaxIssuers) * 32;
 
 struct ConvArgs {
     int W, H;              // spatial size (input = output)
-    int nblk[2];           // channel blocks per input segment
-    int kb[2];             // channels per block of each segment: 16, 32 or 64
-    int a_stage, b_stage;  // bytes of one ring stage's A and B tiles (the widest block's)
-    int woff[2];           // first weight column (input channel) of each segment
+    int nkc[2];            // 8-channel planes of each input segment (even: segments padded to 16 channels)
+    int nkc_total;
     int ncols;             // MMA N = output channels (multiple of 16, <= 256)
-    int tmem_cols;         // power of two >= max(32, ncols)
-    int stages;
+    int tmem_cols;         // power of two >= max(32, ncols): one partial accumulator
+    int issuers;           // MMA-issuing threads (partial accumulators per tile)
+    int nbuf;              // accumulator sets (1 or 2): nbuf x tmem_cols <= 512 / issuers
+    int pstride;           // TMEM columns between issuers' partials: 512 / issuers
+    int hstages;           // halo ring depth
+    int resident;          // 1: all nine taps of weights loaded once per CTA
+    int bslots;            // streamed weights: ring slots of one unit each
+    int kgroup, ngroups;   // K-steps (16 channels) per unit, units per tap
+    uint32_t unit_bytes;   // one slot: kgroup x ncols x 32
+    uint32_t halo_bytes;   // one halo stage: nkc_total planes
+    uint32_t tap_bytes;    // one tap of packed weights: ncols x K x 2
+    const bf16* wpk;       // packed weights [9][K/8][ncols][8]
     const float* bias;     // [ncols] or null
     int relu;              // leaky ReLU with negative slope `slope` (0: ReLU)
     float slope;
@@ -218,29 +245,91 @@ struct ConvArgs {
     int* err;
 };
 
-// Implicit-GEMM 3x3 convolution (forward, or data gradient with flipped
-// transposed weights): see k_conv3x3_p below.
+__device__ __forceinline__ void tma_load_5d(void* dst, const CUtensorMap* tm, uint64_t* bar, int c0, int c1, int c2,
+                                            int c3, int c4) {
+    asm volatile(
+        "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5, "
+        "%6, %7}], [%2];" ::"r"(smem_u32(dst)),
+        "l"(tm), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4)
+        : "memory");
+}
 
-// Epilogue of one output row of a tile: TMEM columns -> bias, activation,
-// mask -> BF16 stores into the output segments.  taddr addresses this
-// thread's TMEM lane at column 0 of the tile's accumulator.
+// Contiguous global -> shared copy of `bytes` (a multiple of 16, both ends
+// 16-byte aligned), completing on `bar`.
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+// D[tmem] (+)= A * B^T with both shared-memory descriptors given as 32-bit
+// halves: lo = start address (16-byte units, bits 0-13) | leading byte
+// offset (bits 16-29); hi = stride byte offset (bits 0-13) | version (bit
+// 14); layout type 0 (no swizzle).
+__device__ __forceinline__ void umma_lh(uint32_t d, uint32_t alo, uint32_t ahi, uint32_t blo, uint32_t bhi,
+                                        uint32_t idesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t.reg .b64 da, db;\n\t"
+        "setp.ne.b32 p, %5, 0;\n\t"
+        "mov.b64 da, {%1, %2};\n\t"
+        "mov.b64 db, {%3, %4};\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], da, db, %6, p;\n\t}" ::"r"(d),
+        "r"(alo), "r"(ahi), "r"(blo), "r"(bhi), "r"(accumulate), "r"(idesc)
+        : "memory");
+}
+
+// 32 lanes x 16 columns of tensor memory, without waiting (tmem_wait_ld).
+__device__ __forceinline__ void tmem_ld16_async(uint32_t taddr, uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// Orders uses of registers filled by tmem_ld16_async after tmem_wait_ld.
+__device__ __forceinline__ void tmem_regs_ready(uint32_t (&r)[16]) {
+    asm volatile(""
+                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]),
+                   "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]),
+                   "+r"(r[15]));
+}
+
+// Epilogue of one output row of a tile: the partial accumulators' TMEM
+// columns, summed -> bias, activation, mask -> BF16 stores into the output
+// segments.  taddr addresses this thread's TMEM lane at column 0 of the
+// tile's first partial; partial k starts k x pstride columns further.
 __device__ __forceinline__ void conv_epilogue_row(const ConvArgs& a, uint32_t taddr, bool inb, long long pix) {
     for (int c = 0; c < a.ncols; c += 16) {
-        uint32_t r[16];
-        tmem_ld16(taddr + (uint32_t)c, r);
+        uint32_t r[kMaxIssuers][16];
+#pragma unroll
+        for (int k = 0; k < kMaxIssuers; k++)
+            if (k < a.issuers) tmem_ld16_async(taddr + (uint32_t)(k * a.pstride + c), r[k]);
+        tmem_wait_ld();
+#pragma unroll
+        for (int k = 0; k < kMaxIssuers; k++)
+            if (k < a.issuers) tmem_regs_ready(r[k]);
         if (!inb) continue;
+        float v[16];
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+            float x = __uint_as_float(r[0][i]);
+#pragma unroll
+            for (int k = 1; k < kMaxIssuers; k++)
+                if (k < a.issuers) x += __uint_as_float(r[k][i]);
+            if (a.bias) x += a.bias[c + i];
+            if (a.relu && !(x > 0.0f)) x *= a.slope;
+            v[i] = x;
+        }
         for (int o = 0; o < a.nout; o++) {
             if (c < a.out_c0[o] || c >= a.out_c0[o] + a.out_cn[o]) continue;
-            const int oc = c - a.out_c0[o];
-            float v[16];
+            const long long off = pix * a.out_cs[o] + (c - a.out_c0[o]);
+            float m[16];
 #pragma unroll
-            for (int i = 0; i < 16; i++) {
-                float x = __uint_as_float(r[i]);
-                if (a.bias) x += a.bias[c + i];
-                if (a.relu && !(x > 0.0f)) x *= a.slope;
-                v[i] = x;
-            }
-            const long long off = pix * a.out_cs[o] + oc;
+            for (int i = 0; i < 16; i++) m[i] = 1.0f;
             if (a.mask[o]) {
                 const uint4* mp = reinterpret_cast<const uint4*>(a.mask[o] + off);
                 uint4 m0 = mp[0], m1 = mp[1];
@@ -248,8 +337,8 @@ __device__ __forceinline__ void conv_epilogue_row(const ConvArgs& a, uint32_t ta
                 const bf16* mb1 = reinterpret_cast<const bf16*>(&m1);
 #pragma unroll
                 for (int i = 0; i < 8; i++) {
-                    if (!(__bfloat162float(mb0[i]) > 0.0f)) v[i] *= a.slope;
-                    if (!(__bfloat162float(mb1[i]) > 0.0f)) v[8 + i] *= a.slope;
+                    if (!(__bfloat162float(mb0[i]) > 0.0f)) m[i] = a.slope;
+                    if (!(__bfloat162float(mb1[i]) > 0.0f)) m[8 + i] = a.slope;
                 }
             }
             uint4 w0, w1;
@@ -257,8 +346,8 @@ __device__ __forceinline__ void conv_epilogue_row(const ConvArgs& a, uint32_t ta
             __nv_bfloat162* p1 = reinterpret_cast<__nv_bfloat162*>(&w1);
 #pragma unroll
             for (int i = 0; i < 4; i++) {
-                p0[i] = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
-                p1[i] = __floats2bfloat162_rn(v[8 + 2 * i], v[8 + 2 * i + 1]);
+                p0[i] = __floats2bfloat162_rn(v[2 * i] * m[2 * i], v[2 * i + 1] * m[2 * i + 1]);
+                p1[i] = __floats2bfloat162_rn(v[8 + 2 * i] * m[8 + 2 * i], v[8 + 2 * i + 1] * m[8 + 2 * i + 1]);
             }
             uint4* dst = reinterpret_cast<uint4*>(a.out[o] + off);
             dst[0] = w0;
@@ -267,127 +356,220 @@ __device__ __forceinline__ void conv_epilogue_row(const ConvArgs& a, uint32_t ta
     }
 }
 
-// Persistent form of k_conv3x3: one CTA per SM walks tiles blockIdx.x,
-// blockIdx.x + gridDim.x, ...  Warp 0 (lane 0) streams A/B boxes through
-// the stage ring without stopping between tiles; warp 1 (lane 0) issues
-// each tile's MMAs into one of two TMEM accumulators; warps 2-5 drain the
-// other accumulator (warp w owns TMEM lanes 32 (w % 4) .. +31), so the
-// epilogue of tile i overlaps the loads and MMAs of tile i + 1.
-constexpr int kConvPThreads = 192;
+struct TileXY {
+    int x0, y0, img;
+};
+__device__ __forceinline__ TileXY tile_xy(int tile, int tiles_x, int tiles_y) {
+    TileXY t;
+    t.x0 = (tile % tiles_x) * kHTileW;
+    t.y0 = ((tile / tiles_x) % tiles_y) * kHTileH;
+    t.img = tile / (tiles_x * tiles_y);
+    return t;
+}
 
-__global__ void __launch_bounds__(kConvPThreads, 1) k_conv3x3_p(const __grid_constant__ CUtensorMap tmA0,
-                                                               const __grid_constant__ CUtensorMap tmA1,
-                                                               const __grid_constant__ CUtensorMap tmB0,
-                                                               const __grid_constant__ CUtensorMap tmB1,
-                                                               const ConvArgs a, int tiles_x, int tiles_y,
-                                                               int ntiles) {
+__global__ void __launch_bounds__(kConvThreads, 1)
+    k_conv3x3_h(const __grid_constant__ CUtensorMap tmA0, const __grid_constant__ CUtensorMap tmA1, const ConvArgs a,
+                int tiles_x, int tiles_y, int ntiles) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = align1024(smem_raw);
-    const int S = a.stages;
-    const uint32_t a_bytes = (uint32_t)a.a_stage, b_bytes = (uint32_t)a.b_stage;
-    uint8_t* sa = smem;
-    uint8_t* sb = smem + S * a_bytes;
-    uint64_t* full = (uint64_t*)(sb + S * b_bytes);
-    uint64_t* empty = full + S;
-    uint64_t* accf = empty + S;  // accumulator k ready for the epilogue
-    uint64_t* acce = accf + 2;   // accumulator k drained
+    const int HS = a.hstages, BS = a.bslots, NI = a.issuers, NB = a.nbuf;
+    uint8_t* sw = smem;                                                        // weights
+    uint8_t* sh = smem + (a.resident ? 9 * a.tap_bytes : BS * a.unit_bytes);  // halo stages
+    uint64_t* hfull = (uint64_t*)(sh + HS * a.halo_bytes);
+    uint64_t* hempty = hfull + HS;
+    uint64_t* bfull = hempty + HS;
+    uint64_t* bempty = bfull + BS;
+    uint64_t* accf = bempty + BS;  // accumulator set k ready for the epilogue (one commit per issuer)
+    uint64_t* acce = accf + 2;     // accumulator set k drained (128 epilogue threads)
     uint32_t* tmem_slot = (uint32_t*)(acce + 2);
+    const uint32_t tmem_total = 512;  // the issuers' column ranges, 512 / issuers apart
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x == 0) {
-        for (int s = 0; s < S; s++) {
-            mbar_init(full + s, 1);
-            mbar_init(empty + s, 1);
+        for (int s = 0; s < HS; s++) {
+            mbar_init(hfull + s, 1);
+            mbar_init(hempty + s, (uint32_t)NI);
+        }
+        for (int s = 0; s < BS; s++) {
+            mbar_init(bfull + s, 1);
+            mbar_init(bempty + s, 1);
         }
         for (int k = 0; k < 2; k++) {
-            mbar_init(accf + k, 1);
+            mbar_init(accf + k, (uint32_t)NI);
             mbar_init(acce + k, 128);
         }
         fence_barrier_init();
     }
     if (warp == 0) {
-        tmem_alloc(tmem_slot, 2 * a.tmem_cols);
+        tmem_alloc(tmem_slot, tmem_total);
         tmem_relinquish();
     }
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
-    const int per_tap = a.nblk[0] + a.nblk[1];
-    const int total = 9 * per_tap;
+    const int nk16 = a.nkc_total / 2;
+    const int nunits = 9 * a.ngroups;  // a tile's MMA units, in (tap, group) order
 
-    if (warp == 0 && lane == 0) {
-        long long g = 0;  // K-blocks issued by this CTA, over all its tiles
-        bool ok = true;
-        for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
-            const int x0 = (tile % tiles_x) * kTileW, y0 = ((tile / tiles_x) % tiles_y) * kTileH;
-            const int img = tile / (tiles_x * tiles_y);
-            for (int kb = 0; kb < total; kb++, g++) {
-                const int s = (int)(g % S);
-                const uint32_t round = (uint32_t)(g / S);
-                if (!mbar_wait(empty + s, (round & 1) ^ 1, a.err, 1)) {
-                    ok = false;
-                    break;
-                }
-                const int tap = kb / per_tap, j = kb % per_tap;
-                const int seg = j < a.nblk[0] ? 0 : 1, cb = seg ? j - a.nblk[0] : j;
-                const int w = a.kb[seg];
-                mbar_expect_tx(full + s, (uint32_t)(128 * w * 2 + a.ncols * w * 2));
-                tma_load_4d(sa + s * a_bytes, seg ? &tmA1 : &tmA0, full + s, cb * w, x0 + tap % 3 - 1,
-                            y0 + tap / 3 - 1, img);
-                tma_load_3d(sb + s * b_bytes, seg ? &tmB1 : &tmB0, full + s, a.woff[seg] + cb * w, tap, 0);
+    if (warp == 0) {
+        if (lane == 0) {
+            int i = 0;
+            for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, i++) {
+                const int s = i % HS;
+                if (!mbar_wait(hempty + s, (uint32_t)((i / HS) & 1) ^ 1, a.err, 1)) break;
+                const TileXY tx = tile_xy(tile, tiles_x, tiles_y);
+                uint8_t* dst = sh + s * a.halo_bytes;
+                mbar_expect_tx(hfull + s, (uint32_t)a.nkc_total * kPlaneBox);
+                for (int c = 0; c < a.nkc[0]; c++)
+                    tma_load_5d(dst + c * kPlaneBytes, &tmA0, hfull + s, 0, c, tx.x0 - 1, tx.y0 - 1, tx.img);
+                for (int c = 0; c < a.nkc[1]; c++)
+                    tma_load_5d(dst + (a.nkc[0] + c) * kPlaneBytes, &tmA1, hfull + s, 0, c, tx.x0 - 1, tx.y0 - 1,
+                                tx.img);
+            }
+            // no copy may still be landing when the CTA exits
+            for (int k = i > HS ? i - HS : 0; k < i; k++)
+                mbar_wait(hfull + k % HS, (uint32_t)((k / HS) & 1), a.err, 64);
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            const uint8_t* wsrc = reinterpret_cast<const uint8_t*>(a.wpk);
+            if (a.resident) {
+                mbar_expect_tx(bfull, 9 * a.tap_bytes);
+                for (int tap = 0; tap < 9; tap++)
+                    bulk_load(sw + tap * a.tap_bytes, wsrc + (size_t)tap * a.tap_bytes, a.tap_bytes, bfull);
+                mbar_wait(bfull, 0, a.err, 64);
+            } else {
+                const uint32_t step = (uint32_t)a.ncols * 32;  // one K-step of one tap
+                long long g = 0;
+                bool ok = true;
+                for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x)
+                    for (int u = 0; u < nunits; u++, g++) {
+                        const int bs = (int)(g % BS);
+                        if (!mbar_wait(bempty + bs, (uint32_t)((g / BS) & 1) ^ 1, a.err, 1)) {
+                            ok = false;
+                            break;
+                        }
+                        const int tap = u / a.ngroups, k0 = (u - tap * a.ngroups) * a.kgroup;
+                        const uint32_t bytes = (uint32_t)(min(nk16, k0 + a.kgroup) - k0) * step;
+                        mbar_expect_tx(bfull + bs, bytes);
+                        bulk_load(sw + bs * a.unit_bytes, wsrc + (size_t)tap * a.tap_bytes + (size_t)k0 * step, bytes,
+                                  bfull + bs);
+                    }
+                for (long long k = g > BS ? g - BS : 0; k < g; k++)
+                    mbar_wait(bfull + k % BS, (uint32_t)((k / BS) & 1), a.err, 64);
             }
         }
-        for (long long k = g > S ? g - S : 0; k < g; k++) mbar_wait(full + k % S, (uint32_t)((k / S) & 1), a.err, 64);
-    } else if (warp == 1 && lane == 0) {
-        const uint32_t idesc = idesc_bf16(a.ncols, false, false);
-        long long g = 0;
-        int i = 0;
-        bool ok = true;
-        for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, i++) {
-            const int buf = i & 1;
-            if (!mbar_wait(acce + buf, ((uint32_t)(i >> 1) & 1) ^ 1, a.err, 128)) break;
-            tc_fence_after();
-            const uint32_t d = tmem + (uint32_t)(buf * a.tmem_cols);
-            for (int kb = 0; kb < total; kb++, g++) {
-                const int s = (int)(g % S);
-                if (!mbar_wait(full + s, (uint32_t)((g / S) & 1), a.err, 2)) {
-                    ok = false;
-                    break;
-                }
-                tc_fence_after();
-                const int j = kb % per_tap;
-                const int w = a.kb[j < a.nblk[0] ? 0 : 1];
-                const uint64_t ad = desc_kmajor(smem_u32(sa + s * a_bytes), w);
-                const uint64_t bd = desc_kmajor(smem_u32(sb + s * b_bytes), w);
-                // K = 16 channels (32 bytes) per MMA, stepping along the swizzled row
-                for (int kk = 0; kk < w / 16; kk++) umma_bf16(d, ad + 2 * kk, bd + 2 * kk, idesc, (kb | kk) != 0);
-                umma_commit(empty + s);
-            }
-            umma_commit(accf + buf);  // also after a timeout: the epilogue then waits for the issued MMAs
-        }
-    } else if (warp >= 2) {
+    } else if (warp <= 5 || (warp >= 6 + kMaxIssuers && NB == 2)) {
+        // epilogue group 0 (warps 2-5) takes every tile when there is one
+        // accumulator set; with two, group 1 (warps 10-13) takes the odd tiles
+        const int group = warp <= 5 ? 0 : 1, ngroup = NB;
         const uint32_t quarter = (uint32_t)(warp & 3);
         const int row = (int)quarter * 32 + lane;
-        int i = 0;
-        for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, i++) {
-            const int buf = i & 1;
-            const bool ready = mbar_wait(accf + buf, (uint32_t)(i >> 1) & 1, a.err, 4);
+        int i = group;
+        for (int tile = blockIdx.x + group * gridDim.x; tile < ntiles; tile += ngroup * gridDim.x, i += ngroup) {
+            const int buf = i % NB;
+            const bool ready = mbar_wait(accf + buf, (uint32_t)((i / NB) & 1), a.err, 4);
             tc_fence_after();
-            const int x0 = (tile % tiles_x) * kTileW, y0 = ((tile / tiles_x) % tiles_y) * kTileH;
-            const int img = tile / (tiles_x * tiles_y);
-            const int px = x0 + (row % kTileW), py = y0 + (row / kTileW);
+            const TileXY tx = tile_xy(tile, tiles_x, tiles_y);
+            const int px = tx.x0 + (row % kHTileW), py = tx.y0 + (row / kHTileW);
             const bool inb = ready && px < a.W && py < a.H;
-            const long long pix = ((long long)img * a.H + py) * a.W + px;
+            const long long pix = ((long long)tx.img * a.H + py) * a.W + px;
             conv_epilogue_row(a, tmem + (quarter * 32u << 16) + (uint32_t)(buf * a.tmem_cols), inb, pix);
             tc_fence_before();
             mbar_arrive(acce + buf);
             if (!ready) break;
         }
+    } else if (warp >= 6 && warp - 6 < NI) {
+        if (lane == 0) {
+            const int w = warp - 6;
+            const uint32_t idesc = idesc_bf16(a.ncols, false, false);
+            const uint32_t lbo_b = (uint32_t)a.ncols * 16;
+            // descriptor halves (umma_lh): A rows of 8 pixels 160 bytes apart,
+            // planes kPlaneBytes apart; B rows of 8 channels 128 bytes apart,
+            // K-chunks ncols x 16 bytes apart
+            const uint32_t ahi = ((kHaloW * 16) >> 4) | (1u << 14), bhi = (128u >> 4) | (1u << 14);
+            const uint32_t alead = (kPlaneBytes >> 4) << 16, blead = (lbo_b >> 4) << 16;
+            const uint32_t astep = (2 * kPlaneBytes) >> 4, bstep = (2 * lbo_b) >> 4;
+            const uint32_t wbase = smem_u32(sw) >> 4, tapb = a.tap_bytes >> 4;
+            // tap (ky, kx) starts ky * 10 + kx pixels into the halo; ky = tap / 3 = (11 tap) >> 5
+            auto toff = [](int t) { return (uint32_t)(t + (kHaloW - 3) * ((t * 11) >> 5)); };
+            // resident weights: this issuer's run of the tile's 9 x nk16 K-steps
+            const int u0 = w * 9 * nk16 / NI, u1 = (w + 1) * 9 * nk16 / NI;
+            const int tap0 = u0 / nk16, k0s = u0 - tap0 * nk16;
+            bool ok = !a.resident || mbar_wait(bfull, 0, a.err, 2);
+            int i = 0;
+            for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, i++) {
+                const int buf = i % NB, s = i % HS;
+                if (!mbar_wait(acce + buf, (uint32_t)((i / NB) & 1) ^ 1, a.err, 128)) break;
+                if (!mbar_wait(hfull + s, (uint32_t)((i / HS) & 1), a.err, 2)) ok = false;
+                tc_fence_after();
+                const uint32_t d = tmem + (uint32_t)(w * a.pstride + buf * a.tmem_cols);
+                const uint32_t abase = smem_u32(sh + s * a.halo_bytes) >> 4;
+                uint32_t acc = 0;
+                if (a.resident) {
+                    // a contiguous run of the tile's K-steps in (tap, step)
+                    // order, [u0, u1): between two MMAs only two adds, and a
+                    // descriptor reload where the run crosses into the next tap
+                    // (a thread's instructions between MMAs add to its issue
+                    // time)
+                    int tap = tap0, k = k0s;
+                    uint32_t alo = (abase + toff(tap) + (uint32_t)k * astep) | alead;
+                    uint32_t blo = (wbase + (uint32_t)tap * tapb + (uint32_t)k * bstep) | blead;
+                    for (int u = u0; u < u1; u++) {
+                        umma_lh(d, alo, ahi, blo, bhi, idesc, acc);
+                        acc = 1;
+                        if (++k == nk16) {
+                            k = 0;
+                            tap++;
+                            alo = (abase + toff(tap)) | alead;
+                            blo = (wbase + (uint32_t)tap * tapb) | blead;
+                        } else {
+                            alo += astep;
+                            blo += bstep;
+                        }
+                    }
+                } else {
+                    // streamed units u = w, w + NI, ...: each waits for its
+                    // ring slot; (tap, group) as running counters
+                    int tap = 0, grp = w;
+                    while (grp >= a.ngroups) {
+                        grp -= a.ngroups;
+                        tap++;
+                    }
+                    uint32_t g = (uint32_t)i * (uint32_t)nunits + (uint32_t)w;  // ring position
+                    for (int u = w; u < nunits && ok; u += NI) {
+                        const int kb = grp * a.kgroup, ke = min(nk16, kb + a.kgroup);
+                        const int bs = (int)(g % (uint32_t)BS);
+                        if (!mbar_wait(bfull + bs, (g / (uint32_t)BS) & 1, a.err, 2)) {
+                            ok = false;
+                            break;
+                        }
+                        tc_fence_after();
+                        uint32_t blo = (smem_u32(sw + bs * a.unit_bytes) >> 4) | blead;
+                        uint32_t alo = (abase + toff(tap) + (uint32_t)kb * astep) | alead;
+                        for (int k = kb; k < ke; k++) {
+                            umma_lh(d, alo, ahi, blo, bhi, idesc, acc);
+                            acc = 1;
+                            alo += astep;
+                            blo += bstep;
+                        }
+                        umma_commit(bempty + bs);
+                        grp += NI;
+                        while (grp >= a.ngroups) {
+                            grp -= a.ngroups;
+                            tap++;
+                        }
+                        g += (uint32_t)NI;
+                    }
+                }
+                umma_commit(hempty + s);
+                umma_commit(accf + buf);  // also after a timeout: the epilogue then waits for the issued MMAs
+            }
+        }
     }
     __syncwarp();
     tc_fence_before();
     __syncthreads();
-    if (warp == 0) tmem_dealloc(tmem, 2 * a.tmem_cols);
+    if (warp == 0) tmem_dealloc(tmem, tmem_total);
 }
 
 // ------------------------------------------------- the weight gradient
@@ -525,55 +707,42 @@ EncodeTiledFn encode_fn() {
     return fn;
 }
 
-// TMA swizzle for rows of `kb` BF16 channels (the UMMA layouts of desc_kmajor).
-CUtensorMapSwizzle swizzle_for(int kb) {
-    return kb == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : kb == 32 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B;
-}
-
-// Channels per K-block: 64 for every segment.  The kernel also takes 16- and
-// 32-channel blocks (32 / 64-byte swizzle) for narrow segments, which move a
-// quarter / half of the bytes; measured on the 1024^2 forward pass they were
-// slower (0.97-0.99 ms against 0.85 ms): TMA boxes with 32- or 64-byte rows
-// move less per request than the zero-filled 128-byte ones, and the pipeline
-// is bound by requests in flight, not bytes.
-int block_channels(int) { return 64; }
-
-// NHWC BF16 activations [n][h][w][c] (c a multiple of 8), boxes of `kb`
-// channels x 16 x 8 pixels, swizzled for kb, zero fill outside.
-int act_map(CUtensorMap* tm, const void* base, int c, int w, int h, int n, int kb = 64) {
+// NHWC BF16 activations [n][h][w][c] (c a multiple of 8), boxes of 64
+// channels x 16 x 8 pixels, 128-byte swizzle, zero fill outside.
+int act_map(CUtensorMap* tm, const void* base, int c, int w, int h, int n) {
     EncodeTiledFn fn = encode_fn();
     if (!fn) return dn_fail(RL_CUDA_ERROR, "cuTensorMapEncodeTiled unavailable");
     if (c % 8 || ((uintptr_t)base & 15)) return dn_fail(RL_INVALID_CALL, "activation layout: %d channels", c);
     cuuint64_t dims[4] = {(cuuint64_t)c, (cuuint64_t)w, (cuuint64_t)h, (cuuint64_t)n};
     cuuint64_t strides[3] = {(cuuint64_t)c * 2, (cuuint64_t)c * 2 * w, (cuuint64_t)c * 2 * w * h};
-    cuuint32_t box[4] = {(cuuint32_t)kb, kTileW, kTileH, 1};
+    cuuint32_t box[4] = {64, kTileW, kTileH, 1};
     cuuint32_t es[4] = {1, 1, 1, 1};
     CUresult r = fn(tm, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(base), dims, strides, box, es,
-                    CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle_for(kb), CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return dn_fail(RL_CUDA_ERROR, "tensor map (activation) error %d", (int)r);
     return RL_OK;
 }
 
-// Weights [rows][9][k] (k a multiple of 64), boxes of kb x 1 x rows.
-int weight_map(CUtensorMap* tm, const void* base, int k, int rows, int kb = 64) {
+// The convolution's halo planes: NHWC BF16 [n][h][w][c] (c a multiple of 8)
+// seen as [n][h][w][c / 8][8]; a box is one plane of 8 channels x 10 x 18
+// pixels, unswizzled (16 bytes per pixel), zero fill outside.
+int halo_map(CUtensorMap* tm, const void* base, int c, int w, int h, int n) {
     EncodeTiledFn fn = encode_fn();
     if (!fn) return dn_fail(RL_CUDA_ERROR, "cuTensorMapEncodeTiled unavailable");
-    if (k % 64 || rows > 256 || rows % 16) return dn_fail(RL_INVALID_CALL, "weight layout %d x %d", rows, k);
-    cuuint64_t dims[3] = {(cuuint64_t)k, 9, (cuuint64_t)rows};
-    cuuint64_t strides[2] = {(cuuint64_t)k * 2, (cuuint64_t)k * 2 * 9};
-    cuuint32_t box[3] = {(cuuint32_t)kb, 1, (cuuint32_t)rows};
-    cuuint32_t es[3] = {1, 1, 1};
-    CUresult r = fn(tm, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void*>(base), dims, strides, box, es,
-                    CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle_for(kb), CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+    if (c <= 0 || c % 8 || ((uintptr_t)base & 15)) return dn_fail(RL_INVALID_CALL, "activation layout: %d channels", c);
+    cuuint64_t dims[5] = {8, (cuuint64_t)(c / 8), (cuuint64_t)w, (cuuint64_t)h, (cuuint64_t)n};
+    cuuint64_t strides[4] = {16, (cuuint64_t)c * 2, (cuuint64_t)c * 2 * w, (cuuint64_t)c * 2 * w * h};
+    cuuint32_t box[5] = {8, 1, kHaloW, kHaloH, 1};
+    cuuint32_t es[5] = {1, 1, 1, 1, 1};
+    CUresult r = fn(tm, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<void*>(base), dims, strides, box, es,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS) return dn_fail(RL_CUDA_ERROR, "tensor map (weights) error %d", (int)r);
+    if (r != CUDA_SUCCESS) return dn_fail(RL_CUDA_ERROR, "tensor map (halo) error %d", (int)r);
     return RL_OK;
 }
 
 int pow2_cols(int n) { return n <= 32 ? 32 : n <= 64 ? 64 : n <= 128 ? 128 : 256; }
-
-int conv_smem(int stage_bytes, int stages) { return stages * stage_bytes + (2 * stages + 4) * 8 + 16 + 1024; }
 
 }  // namespace
 
@@ -585,49 +754,62 @@ extern "C" int rl_dn_conv3x3(const void* in0, int c0, const void* in1, int c1, i
                              int out0_c0,
                              int out0_cn, int out0_cs, const void* mask0, void* out1, int out1_c0, int out1_cn,
                              int out1_cs, const void* mask1, int* d_err, void* stream) {
-    if (!in0 || !weights || !out0 || width <= 0 || height <= 0 || images <= 0)
+    if (!in0 || !weights || !out0 || width <= 0 || height <= 0 || images <= 0 || c0 <= 0 || (in1 && c1 <= 0))
         return dn_fail(RL_INVALID_CALL, "rl_dn_conv3x3: bad arguments");
     if (ncols < 16 || ncols > 256 || ncols % 16) return dn_fail(RL_INVALID_CALL, "rl_dn_conv3x3: ncols %d", ncols);
-    // K-blocks as wide as each segment's channels need (16, 32 or 64): the
-    // weights keep each segment padded to 64 columns, the boxes read only
-    // the block's own columns
-    const int kb0 = block_channels(c0), kb1 = in1 ? block_channels(c1) : 64;
-    const int nb0 = (c0 + kb0 - 1) / kb0, nb1 = in1 ? (c1 + kb1 - 1) / kb1 : 0;
-    const int kpad = 64 * ((c0 + 63) / 64 + (in1 ? (c1 + 63) / 64 : 0));
+    if ((uintptr_t)weights & 15) return dn_fail(RL_INVALID_CALL, "rl_dn_conv3x3: weights not 16-byte aligned");
     const int nout = out1 ? 2 : 1;
     const int oc0[2] = {out0_c0, out1_c0}, ocn[2] = {out0_cn, out1_cn}, ocs[2] = {out0_cs, out1_cs};
     for (int o = 0; o < nout; o++)
         if (ocn[o] % 16 || ocs[o] % 16 || oc0[o] % 16 || ocn[o] > ocs[o] || oc0[o] + ocn[o] > ncols)
             return dn_fail(RL_INVALID_CALL, "rl_dn_conv3x3: output segment %d", o);
-    CUtensorMap tA0, tA1, tB0, tB1;
-    if (int rc = act_map(&tA0, in0, c0, width, height, images, kb0)) return rc;
-    if (int rc = act_map(&tA1, in1 ? in1 : in0, in1 ? c1 : c0, width, height, images, in1 ? kb1 : kb0)) return rc;
-    if (int rc = weight_map(&tB0, weights, kpad, ncols, kb0)) return rc;
-    if (int rc = weight_map(&tB1, weights, kpad, ncols, kb1)) return rc;
+    CUtensorMap tA0, tA1;
+    if (int rc = halo_map(&tA0, in0, c0, width, height, images)) return rc;
+    if (int rc = halo_map(&tA1, in1 ? in1 : in0, in1 ? c1 : c0, width, height, images)) return rc;
     ConvArgs a;
     memset(&a, 0, sizeof a);
     a.W = width;
     a.H = height;
-    a.nblk[0] = nb0;
-    a.nblk[1] = nb1;
-    a.kb[0] = kb0;
-    a.kb[1] = kb1;
-    a.woff[0] = 0;
-    a.woff[1] = 64 * ((c0 + 63) / 64);
+    a.nkc[0] = (c0 + 15) / 16 * 2;
+    a.nkc[1] = in1 ? (c1 + 15) / 16 * 2 : 0;
+    a.nkc_total = a.nkc[0] + a.nkc[1];
     a.ncols = ncols;
     a.tmem_cols = pow2_cols(ncols);
-    // ring depth: two CTAs per SM while both fit in TMEM (2 x 2 accumulators of
-    // <= 128 columns), each with up to ~100 KB of stages; otherwise one CTA
-    // with up to ~200 KB
-    const int per_sm = pow2_cols(ncols) <= 128 ? 2 : 1;
-    // a stage holds the widest block the layer uses: narrow layers get small
-    // stages and a deeper ring (up to 24 K-blocks in flight), which is what
-    // hides the load latency when each K-block carries little work
-    const int kbmax = std::max(kb0, in1 ? kb1 : 0);
-    a.a_stage = 128 * kbmax * 2;
-    a.b_stage = ncols * kbmax * 2;
-    const int stage_bytes = a.a_stage + a.b_stage;
-    a.stages = std::max(2, std::min(24, (per_sm == 2 ? 100 : 200) * 1024 / stage_bytes));
+    a.halo_bytes = (uint32_t)a.nkc_total * kPlaneBytes;
+    a.tap_bytes = (uint32_t)a.nkc_total * (uint32_t)ncols * 16;
+    a.wpk = (const bf16*)weights;
+    // partial accumulators: four issuers, each in its own 128-column quarter
+    // of tensor memory, double-buffered up to 64 columns; two issuers 256
+    // columns apart for 256
+    a.issuers = a.tmem_cols <= 128 ? 4 : 2;
+    a.pstride = 512 / a.issuers;
+    a.nbuf = 2 * a.tmem_cols <= a.pstride ? 2 : 1;
+    // shared memory: the nine taps of weights resident beside at least two
+    // halo stages when they fit (units of one K-step, dealt to the issuers);
+    // else two or three halo stages and a ring of at least four weight
+    // units, each the widest run of a tap's K-steps that allows it
+    const long long budget = 225 * 1024;
+    const long long halo = a.halo_bytes, tap = a.tap_bytes, step = (long long)ncols * 32;
+    const int nk16 = a.nkc_total / 2;
+    if (9 * tap + 2 * halo <= budget) {
+        a.resident = 1;
+        a.bslots = 1;
+        a.kgroup = 1;
+        a.ngroups = nk16;
+        a.hstages = (int)std::min<long long>(8, (budget - 9 * tap) / halo);
+    } else {
+        a.resident = 0;
+        a.hstages = budget - 3 * halo >= 3 * tap ? 3 : 2;
+        const long long rem = budget - a.hstages * halo;
+        a.kgroup = nk16;
+        while (a.kgroup > 1 && rem / (a.kgroup * step) < 4) a.kgroup = (a.kgroup + 1) / 2;
+        a.ngroups = (nk16 + a.kgroup - 1) / a.kgroup;
+        a.bslots = (int)std::min<long long>(8, rem / (a.kgroup * step));
+        if (a.bslots < 2)
+            return dn_fail(RL_INVALID_CALL, "rl_dn_conv3x3: %d input and %d output channels exceed shared memory",
+                           c0 + (in1 ? c1 : 0), ncols);
+    }
+    a.unit_bytes = (uint32_t)(a.kgroup * step);
     a.bias = bias;
     a.relu = relu;
     a.slope = slope;
@@ -642,25 +824,28 @@ extern "C" int rl_dn_conv3x3(const void* in0, int c0, const void* in1, int c1, i
     a.mask[0] = (const bf16*)mask0;
     a.mask[1] = (const bf16*)mask1;
     a.err = d_err;
-    const int smem = conv_smem(stage_bytes, a.stages);
+    // one CTA per SM: at least 116 KB of shared memory each, so two CTAs
+    // never contend for tensor memory
+    const long long need = (a.resident ? 9 * tap : (long long)a.bslots * a.unit_bytes) + (long long)a.hstages * halo +
+                           (2LL * a.hstages + 2LL * a.bslots + 4) * 8 + 16 + 1024;
+    const int smem = (int)std::max<long long>(need, 116 * 1024);
     static int sms = 0;
     static std::once_flag attr;
     cudaError_t ae = cudaSuccess;
     std::call_once(attr, [&] {
-        ae = cudaFuncSetAttribute(k_conv3x3_p, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        ae = cudaFuncSetAttribute(k_conv3x3_h, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
         int dev = 0;
         if (ae == cudaSuccess) ae = cudaGetDevice(&dev);
         if (ae == cudaSuccess) ae = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     });
     if (ae != cudaSuccess) return dn_fail(RL_CUDA_ERROR, "conv set-up: %s", cudaGetErrorString(ae));
-    const int tiles_x = (width + kTileW - 1) / kTileW, tiles_y = (height + kTileH - 1) / kTileH;
+    const int tiles_x = (width + kHTileW - 1) / kHTileW, tiles_y = (height + kHTileH - 1) / kHTileH;
     const long long ntiles = (long long)tiles_x * tiles_y * images;
     if (ntiles > INT32_MAX) return dn_fail(RL_INVALID_CALL, "rl_dn_conv3x3: too many tiles");
-    const int grid = (int)std::min<long long>(ntiles, (long long)per_sm * std::max(sms, 1));
-    k_conv3x3_p<<<grid, kConvPThreads, smem, (cudaStream_t)stream>>>(tA0, tA1, tB0, tB1, a, tiles_x, tiles_y,
-                                                                    (int)ntiles);
+    const int grid = (int)std::min<long long>(ntiles, std::max(sms, 1));
+    k_conv3x3_h<<<grid, kConvThreads, smem, (cudaStream_t)stream>>>(tA0, tA1, a, tiles_x, tiles_y, (int)ntiles);
     cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return dn_fail(RL_CUDA_ERROR, "k_conv3x3_p: %s", cudaGetErrorString(e));
+    if (e != cudaSuccess) return dn_fail(RL_CUDA_ERROR, "k_conv3x3_h: %s", cudaGetErrorString(e));
     return RL_OK;
 }
 
@@ -870,18 +1055,30 @@ __global__ void k_dn_adam(float* p, float* g, float* m, float* v, long long n, f
     }
 }
 
-// Master weights [cout][9][kpad] -> forward BF16 [ncols][9][kpad] and the
-// data-gradient BF16 [kpad][9][copad] (taps flipped, co contiguous).
-__global__ void k_dn_pack(const float* w, int cout, int ncols, int kpad, int copad, bf16* wp, bf16* wt) {
-    const long long nf = (long long)ncols * 9 * kpad, nt = (long long)kpad * 9 * copad;
+// Master weights [cout][9][kpad] (each input segment's columns from a
+// multiple of 64) -> the convolution's packed BF16 operands, [9][K/8][rows][8]:
+//   forward:       rows = ncols, K = pad16(seg0) + pad16(seg1); K column kk is
+//                  master column kk (segment 0) or pad64(seg0) + kk - pad16(seg0);
+//   data gradient: rows = kpad (the forward's input columns), K = ncols (the
+//                  forward's output channels), taps flipped.
+__global__ void k_dn_pack(const float* w, int cout, int ncols, int seg0, int seg1, int kpad, bf16* wp, bf16* wt) {
+    const int k0 = (seg0 + 15) / 16 * 16, K = k0 + (seg1 + 15) / 16 * 16, s1 = (seg0 + 63) / 64 * 64;
+    const long long nf = 9LL * K * ncols, nt = 9LL * ncols * kpad;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nf + nt; i += (long long)gridDim.x * blockDim.x) {
         if (i < nf) {
-            int k = (int)(i % kpad), t = (int)((i / kpad) % 9), r = (int)(i / (9LL * kpad));
-            wp[i] = __float2bfloat16(r < cout ? w[((long long)r * 9 + t) * kpad + k] : 0.f);
+            const int e = (int)(i & 7);
+            const long long q = i >> 3;
+            const int r = (int)(q % ncols), kc = (int)((q / ncols) % (K / 8)), t = (int)(q / ((long long)ncols * (K / 8)));
+            const int kk = kc * 8 + e;
+            const int col = kk < k0 ? (kk < seg0 ? kk : -1) : (kk - k0 < seg1 ? s1 + kk - k0 : -1);
+            wp[i] = __float2bfloat16(r < cout && col >= 0 ? w[((long long)r * 9 + t) * kpad + col] : 0.f);
         } else {
-            long long j = i - nf;
-            int co = (int)(j % copad), t = (int)((j / copad) % 9), k = (int)(j / (9LL * copad));
-            wt[j] = __float2bfloat16(co < cout ? w[((long long)co * 9 + (8 - t)) * kpad + k] : 0.f);
+            const long long j = i - nf;
+            const int e = (int)(j & 7);
+            const long long q = j >> 3;
+            const int r = (int)(q % kpad), kc = (int)((q / kpad) % (ncols / 8)), t = (int)(q / ((long long)kpad * (ncols / 8)));
+            const int co = kc * 8 + e;
+            wt[j] = __float2bfloat16(co < cout ? w[((long long)co * 9 + (8 - t)) * kpad + r] : 0.f);
         }
     }
 }
@@ -1179,8 +1376,9 @@ int backward(rl_denoiser* d, int n, int h, int w, cudaStream_t st) {
 int pack_all(rl_denoiser* d, cudaStream_t st) {
     for (int l = 0; l < 8; l++) {
         Conv& c = d->conv[l];
-        long long tot = (long long)c.ncols * 9 * c.kpad + (long long)c.kpad * 9 * c.copad;
-        k_dn_pack<<<grid_of(tot, 256), 256, 0, st>>>(c.w, c.cout, c.ncols, c.kpad, c.copad, c.wp, c.wt);
+        const long long K = pad16(c.segs[0]) + (c.segs[1] ? pad16(c.segs[1]) : 0);
+        long long tot = 9LL * K * c.ncols + 9LL * c.ncols * c.kpad;
+        k_dn_pack<<<grid_of(tot, 256), 256, 0, st>>>(c.w, c.cout, c.ncols, c.segs[0], c.segs[1], c.kpad, c.wp, c.wt);
         DN_CK(cudaMemcpyAsync(c.bias, c.b, c.cout * sizeof(float), cudaMemcpyDeviceToDevice, st));
     }
     DN_CK(cudaGetLastError());

@@ -55,6 +55,27 @@ def _pad64(c):
     return (c + 63) // 64 * 64
 
 
+def _pad16(c):
+    return (c + 15) // 16 * 16
+
+
+def pack_conv_weights(w, segs, ncols):
+    """torch fp32 weights [co][sum(segs)][3][3] -> the BF16 operand that
+    rl_dn_conv3x3 takes: [9][K/8][ncols][8] (tap = 3*ky + kx), K = the input
+    segments' channels each padded to 16, rows past co zero."""
+    import torch
+    co = w.shape[0]
+    k = sum(_pad16(c) for c in segs)
+    full = torch.zeros(ncols, 9, k, device=w.device)
+    src = w.permute(0, 2, 3, 1).reshape(co, 9, -1)
+    off = o2 = 0
+    for c in segs:
+        full[:co, :, o2:o2 + c] = src[:, :, off:off + c]
+        off += c
+        o2 += _pad16(c)
+    return full.reshape(ncols, 9, k // 8, 8).permute(1, 2, 0, 3).contiguous().to(torch.bfloat16)
+
+
 class Denoiser:
     """rl_denoiser: the BF16 tensor-core encoder-decoder."""
 
@@ -381,19 +402,16 @@ def _main():
         e1.record()
         e1.synchronize()
         ms.append(e0.elapsed_time(e1))
-    # multiply-adds of the 8 convolutions as the MMAs run them: K padded to the
-    # kernel's 64-channel blocks
-    def kblocks(c):
-        return _pad64(c)
-
-    flops, s = 0, args.side
+    # multiply-adds of the 8 convolutions as the MMAs run them (K padded to
+    # 16 per input segment, N to 16) and as the network defines them
+    flops, real, s = 0, 0, args.side
     sizes = [s, (s + 1) // 2, (s + 3) // 4, (s + 7) // 8]
     levels = [0, 1, 2, 3, 2, 1, 0, 0]
     for (cout, segs), lv in zip(LAYERS, levels):
-        k = 9 * sum(kblocks(c) for c in segs)
-        flops += 2 * sizes[lv] ** 2 * ((cout + 15) // 16 * 16) * k
+        flops += 2 * sizes[lv] ** 2 * _pad16(cout) * 9 * sum(_pad16(c) for c in segs)
+        real += 2 * sizes[lv] ** 2 * cout * 9 * sum(segs)
     print(json.dumps({"side": args.side, "forward_ms": min(ms), "mma_tflops": flops / (min(ms) / 1e3) / 1e12,
-                      "status": dn.status()}))
+                      "network_tflops": real / (min(ms) / 1e3) / 1e12, "status": dn.status()}))
 
 
 if __name__ == "__main__":

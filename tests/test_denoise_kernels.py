@@ -17,18 +17,9 @@ def _bf(t):
 
 
 def _pack_w(w, segs, ncols):
-    """torch [co][ci][3][3] -> BF16 [ncols][9][sum pad64(seg)] (tap = 3*ky + kx)."""
-    import torch
-    co, ci = w.shape[:2]
-    kp = sum((c + 63) // 64 * 64 for c in segs)
-    out = torch.zeros(ncols, 9, kp, device=w.device)
-    src = w.permute(0, 2, 3, 1).reshape(co, 9, ci)
-    off, o2 = 0, 0
-    for c in segs:
-        out[:co, :, o2:o2 + c] = src[:, :, off:off + c]
-        off += c
-        o2 += (c + 63) // 64 * 64
-    return _bf(out).contiguous()
+    """torch [co][ci][3][3] -> the convolution's BF16 operand [9][K/8][ncols][8]."""
+    from relight_b200 import denoise as D
+    return D.pack_conv_weights(w, segs, ncols)
 
 
 def _close(got, ref, rel=1e-2):

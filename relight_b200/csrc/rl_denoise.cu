@@ -298,62 +298,96 @@ __device__ __forceinline__ void tmem_regs_ready(uint32_t (&r)[16]) {
                    "+r"(r[15]));
 }
 
-// Epilogue of one output row of a tile: the partial accumulators' TMEM
-// columns, summed -> bias, activation, mask -> BF16 stores into the output
-// segments.  taddr addresses this thread's TMEM lane at column 0 of the
-// tile's first partial; partial k starts k x pstride columns further.
-__device__ __forceinline__ void conv_epilogue_row(const ConvArgs& a, uint32_t taddr, bool inb, long long pix) {
-    for (int c = 0; c < a.ncols; c += 16) {
-        uint32_t r[kMaxIssuers][16];
+// One 16-column chunk of an output row: the summed accumulator values x[16]
+// of columns [c, c + 16) -> bias, activation (in place), mask -> BF16 stores
+// into the output segments that hold those columns.
+__device__ __forceinline__ void conv_store_chunk(const ConvArgs& a, int c, float (&x)[16], long long pix) {
 #pragma unroll
-        for (int k = 0; k < kMaxIssuers; k++)
-            if (k < a.issuers) tmem_ld16_async(taddr + (uint32_t)(k * a.pstride + c), r[k]);
+    for (int i = 0; i < 16; i++) {
+        float t = x[i];
+        if (a.bias) t += a.bias[c + i];
+        if (a.relu && !(t > 0.0f)) t *= a.slope;
+        x[i] = t;
+    }
+    for (int o = 0; o < a.nout; o++) {
+        if (c < a.out_c0[o] || c >= a.out_c0[o] + a.out_cn[o]) continue;
+        const long long off = pix * a.out_cs[o] + (c - a.out_c0[o]);
+        uint4 m0 = make_uint4(0x3F803F80u, 0x3F803F80u, 0x3F803F80u, 0x3F803F80u), m1 = m0;  // BF16 1.0
+        if (a.mask[o]) {
+            const uint4* mp = reinterpret_cast<const uint4*>(a.mask[o] + off);
+            m0 = mp[0];
+            m1 = mp[1];
+        }
+        const bf16* mb0 = reinterpret_cast<const bf16*>(&m0);
+        const bf16* mb1 = reinterpret_cast<const bf16*>(&m1);
+        uint4 w0, w1;
+        __nv_bfloat162* p0 = reinterpret_cast<__nv_bfloat162*>(&w0);
+        __nv_bfloat162* p1 = reinterpret_cast<__nv_bfloat162*>(&w1);
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const float f0 = __bfloat162float(mb0[2 * i]) > 0.0f ? 1.0f : a.slope;
+            const float f1 = __bfloat162float(mb0[2 * i + 1]) > 0.0f ? 1.0f : a.slope;
+            const float f2 = __bfloat162float(mb1[2 * i]) > 0.0f ? 1.0f : a.slope;
+            const float f3 = __bfloat162float(mb1[2 * i + 1]) > 0.0f ? 1.0f : a.slope;
+            p0[i] = __floats2bfloat162_rn(x[2 * i] * f0, x[2 * i + 1] * f1);
+            p1[i] = __floats2bfloat162_rn(x[8 + 2 * i] * f2, x[8 + 2 * i + 1] * f3);
+        }
+        uint4* dst = reinterpret_cast<uint4*>(a.out[o] + off);
+        dst[0] = w0;
+        dst[1] = w1;
+    }
+}
+
+// The partial accumulators' 16 columns at `col` of this thread's TMEM lane
+// (taddr = lane, column 0 of the tile's first partial; partial k starts k x
+// pstride columns further), summed; two partials per load round keep the
+// registers in use at 32.
+__device__ __forceinline__ void conv_sum_chunk(const ConvArgs& a, uint32_t taddr, int col, float (&x)[16]) {
+#pragma unroll
+    for (int k0 = 0; k0 < kMaxIssuers; k0 += 2) {
+        if (k0 >= a.issuers) break;
+        uint32_t r0[16], r1[16];
+        tmem_ld16_async(taddr + (uint32_t)(k0 * a.pstride + col), r0);
+        if (k0 + 1 < a.issuers) tmem_ld16_async(taddr + (uint32_t)((k0 + 1) * a.pstride + col), r1);
         tmem_wait_ld();
-#pragma unroll
-        for (int k = 0; k < kMaxIssuers; k++)
-            if (k < a.issuers) tmem_regs_ready(r[k]);
-        if (!inb) continue;
-        float v[16];
+        tmem_regs_ready(r0);
+        if (k0 + 1 < a.issuers) tmem_regs_ready(r1);
 #pragma unroll
         for (int i = 0; i < 16; i++) {
-            float x = __uint_as_float(r[0][i]);
-#pragma unroll
-            for (int k = 1; k < kMaxIssuers; k++)
-                if (k < a.issuers) x += __uint_as_float(r[k][i]);
-            if (a.bias) x += a.bias[c + i];
-            if (a.relu && !(x > 0.0f)) x *= a.slope;
-            v[i] = x;
-        }
-        for (int o = 0; o < a.nout; o++) {
-            if (c < a.out_c0[o] || c >= a.out_c0[o] + a.out_cn[o]) continue;
-            const long long off = pix * a.out_cs[o] + (c - a.out_c0[o]);
-            float m[16];
-#pragma unroll
-            for (int i = 0; i < 16; i++) m[i] = 1.0f;
-            if (a.mask[o]) {
-                const uint4* mp = reinterpret_cast<const uint4*>(a.mask[o] + off);
-                uint4 m0 = mp[0], m1 = mp[1];
-                const bf16* mb0 = reinterpret_cast<const bf16*>(&m0);
-                const bf16* mb1 = reinterpret_cast<const bf16*>(&m1);
-#pragma unroll
-                for (int i = 0; i < 8; i++) {
-                    if (!(__bfloat162float(mb0[i]) > 0.0f)) m[i] = a.slope;
-                    if (!(__bfloat162float(mb1[i]) > 0.0f)) m[8 + i] = a.slope;
-                }
-            }
-            uint4 w0, w1;
-            __nv_bfloat162* p0 = reinterpret_cast<__nv_bfloat162*>(&w0);
-            __nv_bfloat162* p1 = reinterpret_cast<__nv_bfloat162*>(&w1);
-#pragma unroll
-            for (int i = 0; i < 4; i++) {
-                p0[i] = __floats2bfloat162_rn(v[2 * i] * m[2 * i], v[2 * i + 1] * m[2 * i + 1]);
-                p1[i] = __floats2bfloat162_rn(v[8 + 2 * i] * m[8 + 2 * i], v[8 + 2 * i + 1] * m[8 + 2 * i + 1]);
-            }
-            uint4* dst = reinterpret_cast<uint4*>(a.out[o] + off);
-            dst[0] = w0;
-            dst[1] = w1;
+            float t = __uint_as_float(r0[i]);
+            if (k0 + 1 < a.issuers) t += __uint_as_float(r1[i]);
+            x[i] = k0 == 0 ? t : x[i] + t;
         }
     }
+}
+
+// Epilogue of one output row of a tile, then the accumulator set's release
+// (`drained`).  Up to 32 columns, the sums are held in registers and the set
+// is released before the global stores, so the release (which orders this
+// thread's earlier memory operations) does not wait for them; wider rows are
+// stored chunk by chunk and released after.
+__device__ __forceinline__ void conv_epilogue_row(const ConvArgs& a, uint32_t taddr, bool inb, long long pix,
+                                                  uint64_t* drained) {
+    if (a.ncols <= 32) {
+        float x[2][16];
+#pragma unroll
+        for (int j = 0; j < 2; j++)
+            if (16 * j < a.ncols) conv_sum_chunk(a, taddr, 16 * j, x[j]);
+        tc_fence_before();
+        mbar_arrive(drained);
+        if (!inb) return;
+#pragma unroll
+        for (int j = 0; j < 2; j++)
+            if (16 * j < a.ncols) conv_store_chunk(a, 16 * j, x[j], pix);
+        return;
+    }
+    for (int c = 0; c < a.ncols; c += 16) {
+        float x[16];
+        conv_sum_chunk(a, taddr, c, x);
+        if (inb) conv_store_chunk(a, c, x, pix);
+    }
+    tc_fence_before();
+    mbar_arrive(drained);
 }
 
 struct TileXY {
@@ -473,9 +507,7 @@ __global__ void __launch_bounds__(kConvThreads, 1)
             const int px = tx.x0 + (row % kHTileW), py = tx.y0 + (row / kHTileW);
             const bool inb = ready && px < a.W && py < a.H;
             const long long pix = ((long long)tx.img * a.H + py) * a.W + px;
-            conv_epilogue_row(a, tmem + (quarter * 32u << 16) + (uint32_t)(buf * a.tmem_cols), inb, pix);
-            tc_fence_before();
-            mbar_arrive(acce + buf);
+            conv_epilogue_row(a, tmem + (quarter * 32u << 16) + (uint32_t)(buf * a.tmem_cols), inb, pix, acce + buf);
             if (!ready) break;
         }
     } else if (warp >= 6 && warp - 6 < NI) {
@@ -924,20 +956,22 @@ union Pack8 {
 
 // 2x2 average pooling; odd edges average the children that exist.
 __global__ void k_dn_pool(const bf16* in, bf16* out, int C, int W, int H, int N) {
+    // one thread per output pixel and 8-channel group; 32-bit index arithmetic
+    // (the host launches this only below 2^31 elements)
     const int W2 = (W + 1) / 2, H2 = (H + 1) / 2, G = C / 8;
-    const long long total = (long long)N * H2 * W2 * G;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
-        int g = (int)(i % G);
-        long long p = i / G;
-        int x = (int)(p % W2), y = (int)((p / W2) % H2), n = (int)(p / ((long long)W2 * H2));
+    const unsigned total = (unsigned)N * H2 * W2 * G;
+    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+        const unsigned g = i % G, p = i / G;
+        const unsigned x = p % W2, q = p / W2;
+        const unsigned y = q % H2, n = q / H2;
         float s[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         int cnt = 0;
         for (int dy = 0; dy < 2; dy++)
             for (int dx = 0; dx < 2; dx++) {
-                int xx = 2 * x + dx, yy = 2 * y + dy;
-                if (xx < W && yy < H) {
+                const unsigned xx = 2 * x + dx, yy = 2 * y + dy;
+                if (xx < (unsigned)W && yy < (unsigned)H) {
                     Pack8 v;
-                    v.u = reinterpret_cast<const uint4*>(in + (((long long)n * H + yy) * W + xx) * C)[g];
+                    v.u = reinterpret_cast<const uint4*>(in + (((size_t)n * H + yy) * W + xx) * C)[g];
 #pragma unroll
                     for (int k = 0; k < 8; k++) s[k] += bf(v.h[k]);
                     cnt++;
@@ -950,7 +984,6 @@ __global__ void k_dn_pool(const bf16* in, bf16* out, int C, int W, int H, int N)
     }
 }
 
-// gin += (gout / children) * (mask > 0 ? 1 : slope), gin and mask at the fine size.
 __global__ void k_dn_pool_bwd(const bf16* gout, const bf16* mask, bf16* gin, int C, int W, int H, int N, float slope) {
     const int W2 = (W + 1) / 2, H2 = (H + 1) / 2, G = C / 8;
     const long long total = (long long)N * H * W * G;
@@ -976,18 +1009,26 @@ __global__ void k_dn_pool_bwd(const bf16* gout, const bf16* mask, bf16* gin, int
 
 // Nearest 2x upsampling to W x H.
 __global__ void k_dn_up(const bf16* in, bf16* out, int C, int W, int H, int N) {
+    // one thread per source pixel and 8-channel group: one 16-byte read, up
+    // to four 16-byte writes; 32-bit index arithmetic (launched only below
+    // 2^31 source elements)
     const int W2 = (W + 1) / 2, H2 = (H + 1) / 2, G = C / 8;
-    const long long total = (long long)N * H * W * G;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
-        int g = (int)(i % G);
-        long long p = i / G;
-        int x = (int)(p % W), y = (int)((p / W) % H), n = (int)(p / ((long long)W * H));
-        reinterpret_cast<uint4*>(out)[i] =
-            reinterpret_cast<const uint4*>(in + (((long long)n * H2 + y / 2) * W2 + x / 2) * C)[g];
+    const unsigned total = (unsigned)N * H2 * W2 * G;
+    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+        const unsigned g = i % G, p = i / G;
+        const unsigned x = p % W2, q = p / W2;
+        const unsigned y = q % H2, n = q / H2;
+        const uint4 v = reinterpret_cast<const uint4*>(in)[i];
+        for (int dy = 0; dy < 2; dy++) {
+            const unsigned yy = 2 * y + dy;
+            if (yy >= (unsigned)H) break;
+            uint4* row = reinterpret_cast<uint4*>(out + (((size_t)n * H + yy) * W + 2 * x) * C) + g;
+            row[0] = v;
+            if (2 * x + 1 < (unsigned)W) row[G] = v;
+        }
     }
 }
 
-// gin (coarse) = sum of the gradients of its children.
 __global__ void k_dn_up_bwd(const bf16* gout, bf16* gin, int C, int W, int H, int N) {
     const int W2 = (W + 1) / 2, H2 = (H + 1) / 2, G = C / 8;
     const long long total = (long long)N * H2 * W2 * G;
@@ -1296,6 +1337,8 @@ int conv_wgrad(rl_denoiser* d, int l, const bf16* gout, const bf16* in0, const b
 }
 
 int forward(rl_denoiser* d, int n, int h, int w, cudaStream_t st) {
+    // the resampling kernels index 16-byte elements in 32 bits
+    if ((long long)n * h * w * 16 > INT32_MAX) return dn_fail(RL_INVALID_CALL, "denoiser: %d x %d x %d too large", n, h, w);
     Level L[4];
     L[0] = {w, h};
     for (int k = 1; k < 4; k++) L[k] = {(L[k - 1].w + 1) / 2, (L[k - 1].h + 1) / 2};
@@ -1304,7 +1347,7 @@ int forward(rl_denoiser* d, int n, int h, int w, cudaStream_t st) {
         k_dn_pool<<<grid_of(tot, 256), 256, 0, st>>>(in, out, c, L[lvl].w, L[lvl].h, n);
     };
     auto up = [&](const bf16* in, bf16* out, int c, int lvl) {
-        long long tot = (long long)n * L[lvl].w * L[lvl].h * (c / 8);
+        long long tot = (long long)n * L[lvl + 1].w * L[lvl + 1].h * (c / 8);
         k_dn_up<<<grid_of(tot, 256), 256, 0, st>>>(in, out, c, L[lvl].w, L[lvl].h, n);
     };
     int rc;

@@ -177,15 +177,17 @@ __device__ __forceinline__ uint8_t* align1024(uint8_t* p) {
 
 // ------------------------------------------------------- the conv kernel
 //
-// Implicit-GEMM 3x3 convolution over a halo tile.  A tile is 128 output
-// pixels, 16 rows of 8 (TMEM lane m = pixel (m % 8, m / 8) of the tile).
-// Its input halo, 18 rows of 10 pixels, is staged once per tile in shared
+// Implicit-GEMM 3x3 convolution over a halo tile.  A tile is 16 rows of 8
+// pixels (one half, M = 128: TMEM lane m = pixel (m % 8, m / 8)) or of 16
+// pixels (two halves side by side, one accumulator each).  Its input halo,
+// 18 rows of halo_w = 8 halves + 2 pixels, is staged once per tile in shared
 // memory by TMA as one plane per 8 input channels (one 5-D box of 8 channels
-// x 10 x 18 pixels, zero fill outside the image): pixel-major, 16 bytes per
-// pixel, which is the tensor core's unswizzled K-major layout (core matrices
-// of 8 pixels x 8 channels, 128 contiguous bytes).  The nine taps are nine
-// descriptor views of the same halo, started (ky * 10 + kx) pixels in, with
-// rows of 8 pixels 160 bytes apart: a tap reads no global memory.  Weights
+// x halo_w x 18 pixels, zero fill outside the image): pixel-major, 16 bytes
+// per pixel, which is the tensor core's unswizzled K-major layout (core
+// matrices of 8 pixels x 8 channels, 128 contiguous bytes).  The nine taps
+// (and the two halves) are descriptor views of the same halo, started
+// (ky * halo_w + kx + 8 h) pixels in, with rows of 8 pixels halo_w x 16 bytes
+// apart: a tap reads no global memory.  Weights
 // are packed BF16 [9][K/8][ncols][8] in the same layout (core matrices of 8
 // output x 8 input channels), resident in shared memory when all nine taps
 // fit beside two halo stages, else streamed through a ring of units (a run
@@ -203,17 +205,15 @@ __device__ __forceinline__ uint8_t* align1024(uint8_t* p) {
 //   warp 0    tensor memory; the halo loads (HS-stage ring);
 //   warp 1    the weight copies (nine bulk copies once, or one per unit);
 //   warps 2-5 the epilogue (warp w owns TMEM lanes 32 (w % 4) .. +31), which
-//             drains accumulator set i % nbuf while the issuers fill the other;
+//             drains accumulator set i % nbuf while the issuers fill the others;
 //   warps 6-9 the MMA issuers (lane 0 of each; warp 6 + k is issuer k);
 //   warps 10-13 a second epilogue group when there are two accumulator sets:
 //             groups 0 and 1 take the even and odd tiles.
 
 constexpr int kTileW = 16, kTileH = 8;    // the weight gradient's pixel tile: 128 pixels
 constexpr uint32_t kABytes = 128 * 128;   // 128 pixels x 64 channels x 2 bytes
-constexpr int kHTileW = 8, kHTileH = 16;  // the convolution's pixel tile
-constexpr int kHaloW = kHTileW + 2, kHaloH = kHTileH + 2;
-constexpr uint32_t kPlaneBox = kHaloW * kHaloH * 16;  // 2880 bytes of one plane
-constexpr uint32_t kPlaneBytes = 2944;                // plane stride: 2880 rounded up to 128 bytes
+constexpr int kHTileH = 16;               // the convolution's tile: 16 rows of 8 pixels per half
+constexpr int kHaloH = kHTileH + 2;
 constexpr int kMaxIssuers = 4;
 constexpr int kConvThreads = (10 + kMaxIssuers) * 32;
 
@@ -223,8 +223,12 @@ struct ConvArgs {
     int nkc_total;
     int ncols;             // MMA N = output channels (multiple of 16, <= 256)
     int tmem_cols;         // power of two >= max(32, ncols): one partial accumulator
+    int halves;            // 8-pixel-wide halves per tile (1 or 2): a tile is 16 rows x 8 halves pixels
+    int halo_w;            // halo width: 8 halves + 2 pixels
+    uint32_t plane_box;    // bytes TMA writes per plane: halo_w x 18 x 16
+    uint32_t plane_bytes;  // plane stride: plane_box rounded up to 128
     int issuers;           // MMA-issuing threads (partial accumulators per tile)
-    int nbuf;              // accumulator sets (1 or 2): nbuf x tmem_cols <= 512 / issuers
+    int nbuf;              // accumulator sets (1 to 4): nbuf x halves x tmem_cols <= 512 / issuers
     int pstride;           // TMEM columns between issuers' partials: 512 / issuers
     int hstages;           // halo ring depth
     int resident;          // 1: all nine taps of weights loaded once per CTA
@@ -361,46 +365,89 @@ __device__ __forceinline__ void conv_sum_chunk(const ConvArgs& a, uint32_t taddr
     }
 }
 
-// Epilogue of one output row of a tile, then the accumulator set's release
-// (`drained`).  Up to 32 columns, the sums are held in registers and the set
-// is released before the global stores, so the release (which orders this
-// thread's earlier memory operations) does not wait for them; wider rows are
-// stored chunk by chunk and released after.
-__device__ __forceinline__ void conv_epilogue_row(const ConvArgs& a, uint32_t taddr, bool inb, long long pix,
-                                                  uint64_t* drained) {
-    if (a.ncols <= 32) {
-        float x[2][16];
-#pragma unroll
-        for (int j = 0; j < 2; j++)
-            if (16 * j < a.ncols) conv_sum_chunk(a, taddr, 16 * j, x[j]);
-        tc_fence_before();
-        mbar_arrive(drained);
-        if (!inb) return;
-#pragma unroll
-        for (int j = 0; j < 2; j++)
-            if (16 * j < a.ncols) conv_store_chunk(a, 16 * j, x[j], pix);
-        return;
-    }
-    for (int c = 0; c < a.ncols; c += 16) {
-        float x[16];
-        conv_sum_chunk(a, taddr, c, x);
-        if (inb) conv_store_chunk(a, c, x, pix);
-    }
-    tc_fence_before();
-    mbar_arrive(drained);
-}
-
 struct TileXY {
     int x0, y0, img;
 };
-__device__ __forceinline__ TileXY tile_xy(int tile, int tiles_x, int tiles_y) {
+__device__ __forceinline__ TileXY tile_xy(int tile, int tiles_x, int tiles_y, int tile_w) {
     TileXY t;
-    t.x0 = (tile % tiles_x) * kHTileW;
+    t.x0 = (tile % tiles_x) * tile_w;
     t.y0 = ((tile / tiles_x) % tiles_y) * kHTileH;
     t.img = tile / (tiles_x * tiles_y);
     return t;
 }
 
+// Epilogue of one tile for this thread's TMEM lane (pixel row % 8, row / 8 of
+// each 8-pixel half; half h's accumulator starts h x tmem_cols columns on),
+// then the accumulator set's release (`drained`).  When the tile has at most
+// 64 columns in all (halves x ncols) and no mask, the finished BF16 values
+// are held in registers and the set is released before the global stores, so
+// the release (which orders this thread's earlier memory operations) does not
+// wait for them; otherwise the row is stored chunk by chunk and released
+// after.
+template <int kHalves>
+__device__ __forceinline__ void conv_epilogue_tile(const ConvArgs& a, uint32_t taddr, const TileXY& tx, int row,
+                                                   bool ready, uint64_t* drained) {
+    const int cpc = a.ncols / 16;  // 16-column chunks per half
+    auto pixel = [&](int h, long long& pix) {
+        const int px = tx.x0 + 8 * h + (row & 7), py = tx.y0 + (row >> 3);
+        pix = ((long long)tx.img * a.H + py) * a.W + px;
+        return ready && px < a.W && py < a.H;
+    };
+    if (kHalves * a.ncols <= 64 && !a.mask[0] && !a.mask[1]) {
+        // finished BF16 values, 16 bytes per 8 columns
+        uint4 q[4][2];
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+            if (j < kHalves * cpc) {
+                const int h = j / cpc, c = 16 * (j - h * cpc);
+                float x[16];
+                conv_sum_chunk(a, taddr + (uint32_t)(h * a.tmem_cols), c, x);
+                __nv_bfloat162* p0 = reinterpret_cast<__nv_bfloat162*>(&q[j][0]);
+                __nv_bfloat162* p1 = reinterpret_cast<__nv_bfloat162*>(&q[j][1]);
+#pragma unroll
+                for (int i = 0; i < 16; i++) {
+                    float t = x[i];
+                    if (a.bias) t += a.bias[c + i];
+                    if (a.relu && !(t > 0.0f)) t *= a.slope;
+                    x[i] = t;
+                }
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    p0[i] = __floats2bfloat162_rn(x[2 * i], x[2 * i + 1]);
+                    p1[i] = __floats2bfloat162_rn(x[8 + 2 * i], x[8 + 2 * i + 1]);
+                }
+            }
+        tc_fence_before();
+        mbar_arrive(drained);
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+            if (j < kHalves * cpc) {
+                const int h = j / cpc, c = 16 * (j - h * cpc);
+                long long pix;
+                if (!pixel(h, pix)) continue;
+                for (int o = 0; o < a.nout; o++) {
+                    if (c < a.out_c0[o] || c >= a.out_c0[o] + a.out_cn[o]) continue;
+                    uint4* dst = reinterpret_cast<uint4*>(a.out[o] + pix * a.out_cs[o] + (c - a.out_c0[o]));
+                    dst[0] = q[j][0];
+                    dst[1] = q[j][1];
+                }
+            }
+        return;
+    }
+    for (int h = 0; h < kHalves; h++) {
+        long long pix;
+        const bool inb = pixel(h, pix);
+        for (int c = 0; c < a.ncols; c += 16) {
+            float x[16];
+            conv_sum_chunk(a, taddr + (uint32_t)(h * a.tmem_cols), c, x);
+            if (inb) conv_store_chunk(a, c, x, pix);
+        }
+    }
+    tc_fence_before();
+    mbar_arrive(drained);
+}
+
+template <int kHalves>
 __global__ void __launch_bounds__(kConvThreads, 1)
     k_conv3x3_h(const __grid_constant__ CUtensorMap tmA0, const __grid_constant__ CUtensorMap tmA1, const ConvArgs a,
                 int tiles_x, int tiles_y, int ntiles) {
@@ -414,8 +461,8 @@ __global__ void __launch_bounds__(kConvThreads, 1)
     uint64_t* bfull = hempty + HS;
     uint64_t* bempty = bfull + BS;
     uint64_t* accf = bempty + BS;  // accumulator set k ready for the epilogue (one commit per issuer)
-    uint64_t* acce = accf + 2;     // accumulator set k drained (128 epilogue threads)
-    uint32_t* tmem_slot = (uint32_t*)(acce + 2);
+    uint64_t* acce = accf + 4;     // accumulator set k drained (128 epilogue threads)
+    uint32_t* tmem_slot = (uint32_t*)(acce + 4);
     const uint32_t tmem_total = 512;  // the issuers' column ranges, 512 / issuers apart
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x == 0) {
@@ -427,7 +474,7 @@ __global__ void __launch_bounds__(kConvThreads, 1)
             mbar_init(bfull + s, 1);
             mbar_init(bempty + s, 1);
         }
-        for (int k = 0; k < 2; k++) {
+        for (int k = 0; k < 4; k++) {
             mbar_init(accf + k, (uint32_t)NI);
             mbar_init(acce + k, 128);
         }
@@ -450,13 +497,13 @@ __global__ void __launch_bounds__(kConvThreads, 1)
             for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, i++) {
                 const int s = i % HS;
                 if (!mbar_wait(hempty + s, (uint32_t)((i / HS) & 1) ^ 1, a.err, 1)) break;
-                const TileXY tx = tile_xy(tile, tiles_x, tiles_y);
+                const TileXY tx = tile_xy(tile, tiles_x, tiles_y, 8 * kHalves);
                 uint8_t* dst = sh + s * a.halo_bytes;
-                mbar_expect_tx(hfull + s, (uint32_t)a.nkc_total * kPlaneBox);
+                mbar_expect_tx(hfull + s, (uint32_t)a.nkc_total * a.plane_box);
                 for (int c = 0; c < a.nkc[0]; c++)
-                    tma_load_5d(dst + c * kPlaneBytes, &tmA0, hfull + s, 0, c, tx.x0 - 1, tx.y0 - 1, tx.img);
+                    tma_load_5d(dst + c * a.plane_bytes, &tmA0, hfull + s, 0, c, tx.x0 - 1, tx.y0 - 1, tx.img);
                 for (int c = 0; c < a.nkc[1]; c++)
-                    tma_load_5d(dst + (a.nkc[0] + c) * kPlaneBytes, &tmA1, hfull + s, 0, c, tx.x0 - 1, tx.y0 - 1,
+                    tma_load_5d(dst + (a.nkc[0] + c) * a.plane_bytes, &tmA1, hfull + s, 0, c, tx.x0 - 1, tx.y0 - 1,
                                 tx.img);
             }
             // no copy may still be landing when the CTA exits
@@ -492,10 +539,10 @@ __global__ void __launch_bounds__(kConvThreads, 1)
                     mbar_wait(bfull + k % BS, (uint32_t)((k / BS) & 1), a.err, 64);
             }
         }
-    } else if (warp <= 5 || (warp >= 6 + kMaxIssuers && NB == 2)) {
+    } else if (warp <= 5 || (warp >= 6 + kMaxIssuers && NB >= 2)) {
         // epilogue group 0 (warps 2-5) takes every tile when there is one
         // accumulator set; with two, group 1 (warps 10-13) takes the odd tiles
-        const int group = warp <= 5 ? 0 : 1, ngroup = NB;
+        const int group = warp <= 5 ? 0 : 1, ngroup = NB >= 2 ? 2 : 1;
         const uint32_t quarter = (uint32_t)(warp & 3);
         const int row = (int)quarter * 32 + lane;
         int i = group;
@@ -503,11 +550,9 @@ __global__ void __launch_bounds__(kConvThreads, 1)
             const int buf = i % NB;
             const bool ready = mbar_wait(accf + buf, (uint32_t)((i / NB) & 1), a.err, 4);
             tc_fence_after();
-            const TileXY tx = tile_xy(tile, tiles_x, tiles_y);
-            const int px = tx.x0 + (row % kHTileW), py = tx.y0 + (row / kHTileW);
-            const bool inb = ready && px < a.W && py < a.H;
-            const long long pix = ((long long)tx.img * a.H + py) * a.W + px;
-            conv_epilogue_row(a, tmem + (quarter * 32u << 16) + (uint32_t)(buf * a.tmem_cols), inb, pix, acce + buf);
+            const TileXY tx = tile_xy(tile, tiles_x, tiles_y, 8 * kHalves);
+            conv_epilogue_tile<kHalves>(a, tmem + (quarter * 32u << 16) + (uint32_t)(buf * kHalves * a.tmem_cols), tx,
+                                        row, ready, acce + buf);
             if (!ready) break;
         }
     } else if (warp >= 6 && warp - 6 < NI) {
@@ -515,15 +560,18 @@ __global__ void __launch_bounds__(kConvThreads, 1)
             const int w = warp - 6;
             const uint32_t idesc = idesc_bf16(a.ncols, false, false);
             const uint32_t lbo_b = (uint32_t)a.ncols * 16;
-            // descriptor halves (umma_lh): A rows of 8 pixels 160 bytes apart,
-            // planes kPlaneBytes apart; B rows of 8 channels 128 bytes apart,
-            // K-chunks ncols x 16 bytes apart
-            const uint32_t ahi = ((kHaloW * 16) >> 4) | (1u << 14), bhi = (128u >> 4) | (1u << 14);
-            const uint32_t alead = (kPlaneBytes >> 4) << 16, blead = (lbo_b >> 4) << 16;
-            const uint32_t astep = (2 * kPlaneBytes) >> 4, bstep = (2 * lbo_b) >> 4;
+            // descriptor halves (umma_lh): A rows of 8 pixels halo_w x 16 bytes
+            // apart, planes plane_bytes apart; B rows of 8 channels 128 bytes
+            // apart, K-chunks ncols x 16 bytes apart
+            const uint32_t ahi = (uint32_t)a.halo_w | (1u << 14), bhi = (128u >> 4) | (1u << 14);
+            const uint32_t alead = (a.plane_bytes >> 4) << 16, blead = (lbo_b >> 4) << 16;
+            const uint32_t astep = (2 * a.plane_bytes) >> 4, bstep = (2 * lbo_b) >> 4;
             const uint32_t wbase = smem_u32(sw) >> 4, tapb = a.tap_bytes >> 4;
-            // tap (ky, kx) starts ky * 10 + kx pixels into the halo; ky = tap / 3 = (11 tap) >> 5
-            auto toff = [](int t) { return (uint32_t)(t + (kHaloW - 3) * ((t * 11) >> 5)); };
+            const uint32_t hcol = (uint32_t)a.tmem_cols;  // the second half's accumulator, 8 pixels on
+            constexpr bool two = kHalves == 2;
+            // tap (ky, kx) starts ky * halo_w + kx pixels into the halo; ky = tap / 3 = (11 tap) >> 5
+            const int hw = a.halo_w;
+            auto toff = [hw](int t) { return (uint32_t)(t + (hw - 3) * ((t * 11) >> 5)); };
             // resident weights: this issuer's run of the tile's 9 x nk16 K-steps
             const int u0 = w * 9 * nk16 / NI, u1 = (w + 1) * 9 * nk16 / NI;
             const int tap0 = u0 / nk16, k0s = u0 - tap0 * nk16;
@@ -534,7 +582,7 @@ __global__ void __launch_bounds__(kConvThreads, 1)
                 if (!mbar_wait(acce + buf, (uint32_t)((i / NB) & 1) ^ 1, a.err, 128)) break;
                 if (!mbar_wait(hfull + s, (uint32_t)((i / HS) & 1), a.err, 2)) ok = false;
                 tc_fence_after();
-                const uint32_t d = tmem + (uint32_t)(w * a.pstride + buf * a.tmem_cols);
+                const uint32_t d = tmem + (uint32_t)(w * a.pstride + buf * kHalves * a.tmem_cols);
                 const uint32_t abase = smem_u32(sh + s * a.halo_bytes) >> 4;
                 uint32_t acc = 0;
                 if (a.resident) {
@@ -548,6 +596,7 @@ __global__ void __launch_bounds__(kConvThreads, 1)
                     uint32_t blo = (wbase + (uint32_t)tap * tapb + (uint32_t)k * bstep) | blead;
                     for (int u = u0; u < u1; u++) {
                         umma_lh(d, alo, ahi, blo, bhi, idesc, acc);
+                        if (two) umma_lh(d + hcol, alo + 8, ahi, blo, bhi, idesc, acc);
                         acc = 1;
                         if (++k == nk16) {
                             k = 0;
@@ -580,6 +629,7 @@ __global__ void __launch_bounds__(kConvThreads, 1)
                         uint32_t alo = (abase + toff(tap) + (uint32_t)kb * astep) | alead;
                         for (int k = kb; k < ke; k++) {
                             umma_lh(d, alo, ahi, blo, bhi, idesc, acc);
+                            if (two) umma_lh(d + hcol, alo + 8, ahi, blo, bhi, idesc, acc);
                             acc = 1;
                             alo += astep;
                             blo += bstep;
@@ -757,15 +807,15 @@ int act_map(CUtensorMap* tm, const void* base, int c, int w, int h, int n) {
 }
 
 // The convolution's halo planes: NHWC BF16 [n][h][w][c] (c a multiple of 8)
-// seen as [n][h][w][c / 8][8]; a box is one plane of 8 channels x 10 x 18
-// pixels, unswizzled (16 bytes per pixel), zero fill outside.
-int halo_map(CUtensorMap* tm, const void* base, int c, int w, int h, int n) {
+// seen as [n][h][w][c / 8][8]; a box is one plane of 8 channels x halo_w x
+// 18 pixels, unswizzled (16 bytes per pixel), zero fill outside.
+int halo_map(CUtensorMap* tm, const void* base, int c, int w, int h, int n, int halo_w) {
     EncodeTiledFn fn = encode_fn();
     if (!fn) return dn_fail(RL_CUDA_ERROR, "cuTensorMapEncodeTiled unavailable");
     if (c <= 0 || c % 8 || ((uintptr_t)base & 15)) return dn_fail(RL_INVALID_CALL, "activation layout: %d channels", c);
     cuuint64_t dims[5] = {8, (cuuint64_t)(c / 8), (cuuint64_t)w, (cuuint64_t)h, (cuuint64_t)n};
     cuuint64_t strides[4] = {16, (cuuint64_t)c * 2, (cuuint64_t)c * 2 * w, (cuuint64_t)c * 2 * w * h};
-    cuuint32_t box[5] = {8, 1, kHaloW, kHaloH, 1};
+    cuuint32_t box[5] = {8, 1, (cuuint32_t)halo_w, kHaloH, 1};
     cuuint32_t es[5] = {1, 1, 1, 1, 1};
     CUresult r = fn(tm, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<void*>(base), dims, strides, box, es,
                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
@@ -795,9 +845,6 @@ extern "C" int rl_dn_conv3x3(const void* in0, int c0, const void* in1, int c1, i
     for (int o = 0; o < nout; o++)
         if (ocn[o] % 16 || ocs[o] % 16 || oc0[o] % 16 || ocn[o] > ocs[o] || oc0[o] + ocn[o] > ncols)
             return dn_fail(RL_INVALID_CALL, "rl_dn_conv3x3: output segment %d", o);
-    CUtensorMap tA0, tA1;
-    if (int rc = halo_map(&tA0, in0, c0, width, height, images)) return rc;
-    if (int rc = halo_map(&tA1, in1 ? in1 : in0, in1 ? c1 : c0, width, height, images)) return rc;
     ConvArgs a;
     memset(&a, 0, sizeof a);
     a.W = width;
@@ -807,22 +854,38 @@ extern "C" int rl_dn_conv3x3(const void* in0, int c0, const void* in1, int c1, i
     a.nkc_total = a.nkc[0] + a.nkc[1];
     a.ncols = ncols;
     a.tmem_cols = pow2_cols(ncols);
-    a.halo_bytes = (uint32_t)a.nkc_total * kPlaneBytes;
     a.tap_bytes = (uint32_t)a.nkc_total * (uint32_t)ncols * 16;
     a.wpk = (const bf16*)weights;
     // partial accumulators: four issuers, each in its own 128-column quarter
-    // of tensor memory, double-buffered up to 64 columns; two issuers 256
-    // columns apart for 256
+    // of tensor memory; two issuers 256 columns apart for 256 columns
     a.issuers = a.tmem_cols <= 128 ? 4 : 2;
     a.pstride = 512 / a.issuers;
-    a.nbuf = 2 * a.tmem_cols <= a.pstride ? 2 : 1;
     // shared memory: the nine taps of weights resident beside at least two
     // halo stages when they fit (units of one K-step, dealt to the issuers);
     // else two or three halo stages and a ring of at least four weight
-    // units, each the widest run of a tap's K-steps that allows it
+    // units, each the widest run of a tap's K-steps that allows it.  Tiles
+    // are 16 x 16 pixels (two halves: twice the MMAs per barrier wait and
+    // commit) for layers of at most 32 input channels whose weights are
+    // resident and whose two halves still leave each issuer two accumulator
+    // sets (measured at 1024^2: 16 -> 32 channels 69 -> 63 us, 32 -> 3
+    // channels 70 -> 54 us; with more input channels, or with one accumulator
+    // set, the wider tile was slower); otherwise 16 x 8.
     const long long budget = 225 * 1024;
-    const long long halo = a.halo_bytes, tap = a.tap_bytes, step = (long long)ncols * 32;
+    const long long tap = a.tap_bytes, step = (long long)ncols * 32;
     const int nk16 = a.nkc_total / 2;
+    auto plane_of = [](int halo_w) { return (uint32_t)((halo_w * kHaloH * 16 + 127) / 128 * 128); };
+    a.halves = (nk16 <= 2 && 4 * a.tmem_cols <= a.pstride && 9 * tap + 2LL * a.nkc_total * plane_of(18) <= budget)
+                   ? 2
+                   : 1;
+    a.halo_w = 8 * a.halves + 2;
+    a.plane_box = (uint32_t)(a.halo_w * kHaloH * 16);
+    a.plane_bytes = plane_of(a.halo_w);
+    a.halo_bytes = (uint32_t)a.nkc_total * a.plane_bytes;
+    a.nbuf = std::min(4, a.pstride / (a.halves * a.tmem_cols));
+    const long long halo = a.halo_bytes;
+    CUtensorMap tA0, tA1;
+    if (int rc = halo_map(&tA0, in0, c0, width, height, images, a.halo_w)) return rc;
+    if (int rc = halo_map(&tA1, in1 ? in1 : in0, in1 ? c1 : c0, width, height, images, a.halo_w)) return rc;
     if (9 * tap + 2 * halo <= budget) {
         a.resident = 1;
         a.bslots = 1;
@@ -859,23 +922,29 @@ extern "C" int rl_dn_conv3x3(const void* in0, int c0, const void* in1, int c1, i
     // one CTA per SM: at least 116 KB of shared memory each, so two CTAs
     // never contend for tensor memory
     const long long need = (a.resident ? 9 * tap : (long long)a.bslots * a.unit_bytes) + (long long)a.hstages * halo +
-                           (2LL * a.hstages + 2LL * a.bslots + 4) * 8 + 16 + 1024;
+                           (2LL * a.hstages + 2LL * a.bslots + 8) * 8 + 16 + 1024;
     const int smem = (int)std::max<long long>(need, 116 * 1024);
     static int sms = 0;
     static std::once_flag attr;
     cudaError_t ae = cudaSuccess;
     std::call_once(attr, [&] {
-        ae = cudaFuncSetAttribute(k_conv3x3_h, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        ae = cudaFuncSetAttribute(k_conv3x3_h<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        if (ae == cudaSuccess)
+            ae = cudaFuncSetAttribute(k_conv3x3_h<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
         int dev = 0;
         if (ae == cudaSuccess) ae = cudaGetDevice(&dev);
         if (ae == cudaSuccess) ae = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     });
     if (ae != cudaSuccess) return dn_fail(RL_CUDA_ERROR, "conv set-up: %s", cudaGetErrorString(ae));
-    const int tiles_x = (width + kHTileW - 1) / kHTileW, tiles_y = (height + kHTileH - 1) / kHTileH;
+    const int tile_w = 8 * a.halves;
+    const int tiles_x = (width + tile_w - 1) / tile_w, tiles_y = (height + kHTileH - 1) / kHTileH;
     const long long ntiles = (long long)tiles_x * tiles_y * images;
     if (ntiles > INT32_MAX) return dn_fail(RL_INVALID_CALL, "rl_dn_conv3x3: too many tiles");
     const int grid = (int)std::min<long long>(ntiles, std::max(sms, 1));
-    k_conv3x3_h<<<grid, kConvThreads, smem, (cudaStream_t)stream>>>(tA0, tA1, a, tiles_x, tiles_y, (int)ntiles);
+    if (a.halves == 2)
+        k_conv3x3_h<2><<<grid, kConvThreads, smem, (cudaStream_t)stream>>>(tA0, tA1, a, tiles_x, tiles_y, (int)ntiles);
+    else
+        k_conv3x3_h<1><<<grid, kConvThreads, smem, (cudaStream_t)stream>>>(tA0, tA1, a, tiles_x, tiles_y, (int)ntiles);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return dn_fail(RL_CUDA_ERROR, "k_conv3x3_h: %s", cudaGetErrorString(e));
     return RL_OK;

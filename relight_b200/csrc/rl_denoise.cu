@@ -73,6 +73,15 @@ __device__ __forceinline__ void fence_barrier_init() {
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 
+// Programmatic dependent launch: a kernel launched with programmatic stream
+// serialisation may start while its predecessor in the stream is finishing;
+// pdl_wait() blocks until the predecessor has completed and its writes are
+// visible (at once when launched normally), so everything before it must
+// touch no global memory the predecessor may write.  pdl_trigger() lets the
+// successor launch as soon as this grid's CTAs are all running.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
                  : "memory");
@@ -465,6 +474,7 @@ __global__ void __launch_bounds__(kConvThreads, 1)
     uint32_t* tmem_slot = (uint32_t*)(acce + 4);
     const uint32_t tmem_total = 512;  // the issuers' column ranges, 512 / issuers apart
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    pdl_trigger();
     if (threadIdx.x == 0) {
         for (int s = 0; s < HS; s++) {
             mbar_init(hfull + s, 1);
@@ -487,6 +497,9 @@ __global__ void __launch_bounds__(kConvThreads, 1)
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
+    // set-up above overlaps the predecessor's tail; inputs, weights and
+    // outputs are touched only after it has completed
+    pdl_wait();
     const uint32_t tmem = *tmem_slot;
     const int nk16 = a.nkc_total / 2;
     const int nunits = 9 * a.ngroups;  // a tile's MMA units, in (tap, group) order
@@ -770,6 +783,22 @@ __global__ void __launch_bounds__(128, 1) k_conv3x3_wgrad(const __grid_constant_
     if (warp == 0) tmem_dealloc(tmem, tcols);
 }
 
+// Launch with programmatic stream serialisation (see pdl_wait).
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, args...);
+}
+
 // ------------------------------------------------------ tensor maps (host)
 
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
@@ -941,11 +970,9 @@ extern "C" int rl_dn_conv3x3(const void* in0, int c0, const void* in1, int c1, i
     const long long ntiles = (long long)tiles_x * tiles_y * images;
     if (ntiles > INT32_MAX) return dn_fail(RL_INVALID_CALL, "rl_dn_conv3x3: too many tiles");
     const int grid = (int)std::min<long long>(ntiles, std::max(sms, 1));
-    if (a.halves == 2)
-        k_conv3x3_h<2><<<grid, kConvThreads, smem, (cudaStream_t)stream>>>(tA0, tA1, a, tiles_x, tiles_y, (int)ntiles);
-    else
-        k_conv3x3_h<1><<<grid, kConvThreads, smem, (cudaStream_t)stream>>>(tA0, tA1, a, tiles_x, tiles_y, (int)ntiles);
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e = launch_pdl(a.halves == 2 ? k_conv3x3_h<2> : k_conv3x3_h<1>, dim3(grid), dim3(kConvThreads),
+                               (size_t)smem, (cudaStream_t)stream, tA0, tA1, a, tiles_x, tiles_y, (int)ntiles);
+    if (e == cudaSuccess) e = cudaGetLastError();
     if (e != cudaSuccess) return dn_fail(RL_CUDA_ERROR, "k_conv3x3_h: %s", cudaGetErrorString(e));
     return RL_OK;
 }
@@ -1025,6 +1052,8 @@ union Pack8 {
 
 // 2x2 average pooling; odd edges average the children that exist.
 __global__ void k_dn_pool(const bf16* in, bf16* out, int C, int W, int H, int N) {
+    pdl_trigger();
+    pdl_wait();
     // one thread per output pixel and 8-channel group; 32-bit index arithmetic
     // (the host launches this only below 2^31 elements)
     const int W2 = (W + 1) / 2, H2 = (H + 1) / 2, G = C / 8;
@@ -1078,6 +1107,8 @@ __global__ void k_dn_pool_bwd(const bf16* gout, const bf16* mask, bf16* gin, int
 
 // Nearest 2x upsampling to W x H.
 __global__ void k_dn_up(const bf16* in, bf16* out, int C, int W, int H, int N) {
+    pdl_trigger();
+    pdl_wait();
     // one thread per source pixel and 8-channel group: one 16-byte read, up
     // to four 16-byte writes; 32-bit index arithmetic (launched only below
     // 2^31 source elements)
@@ -1413,11 +1444,11 @@ int forward(rl_denoiser* d, int n, int h, int w, cudaStream_t st) {
     for (int k = 1; k < 4; k++) L[k] = {(L[k - 1].w + 1) / 2, (L[k - 1].h + 1) / 2};
     auto pool = [&](const bf16* in, bf16* out, int c, int lvl) {
         long long tot = (long long)n * L[lvl + 1].w * L[lvl + 1].h * (c / 8);
-        k_dn_pool<<<grid_of(tot, 256), 256, 0, st>>>(in, out, c, L[lvl].w, L[lvl].h, n);
+        launch_pdl(k_dn_pool, dim3(grid_of(tot, 256)), dim3(256), 0, st, in, out, c, L[lvl].w, L[lvl].h, n);
     };
     auto up = [&](const bf16* in, bf16* out, int c, int lvl) {
         long long tot = (long long)n * L[lvl + 1].w * L[lvl + 1].h * (c / 8);
-        k_dn_up<<<grid_of(tot, 256), 256, 0, st>>>(in, out, c, L[lvl].w, L[lvl].h, n);
+        launch_pdl(k_dn_up, dim3(grid_of(tot, 256)), dim3(256), 0, st, in, out, c, L[lvl].w, L[lvl].h, n);
     };
     int rc;
     if ((rc = conv_fwd(d, 0, d->x, nullptr, L[0].w, L[0].h, n, d->e0, true, st))) return rc;

@@ -109,3 +109,32 @@ def test_conv3x3_wgrad(cuda, shape):
     e = (dw[..., 5:] - ref).abs().max().item()
     assert e <= 2e-3 * ref.abs().max().item(), (e, ref.abs().max().item())
     assert not dw[..., :5].any()
+
+
+@pytest.mark.parametrize("c0,c1,co", [(96, 64, 64), (128, 96, 96), (64, 0, 256), (16, 0, 3)])
+def test_conv3x3_tile_plans(cuda, c0, c1, co):
+    """Each of the convolution's shared-memory plans on odd sizes: weights
+    streamed through the ring (96 + 64 -> 64, 128 + 96 -> 96), two issuers of
+    256-column accumulators (64 -> 256), and 16 x 16 tiles with a half tile
+    past the image's edge (16 -> 3)."""
+    import torch
+    from relight_b200 import denoise as D
+    n, h, w = 1, 21, 27
+    g = torch.Generator(device="cuda").manual_seed(4)
+    x0 = _bf(torch.randn(n, h, w, c0, device="cuda", generator=g))
+    x1 = _bf(torch.randn(n, h, w, c1, device="cuda", generator=g)) if c1 else None
+    wt = _bf(torch.randn(co, c0 + c1, 3, 3, device="cuda", generator=g) * 0.05).float()
+    b = torch.randn(co, device="cuda", generator=g)
+    ncols = (co + 15) // 16 * 16
+    wp = _pack_w(wt, [c for c in (c0, c1) if c], ncols)
+    bias = torch.zeros(ncols, device="cuda")
+    bias[:co] = b
+    out = torch.zeros(n, h, w, ncols, dtype=torch.bfloat16, device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    D.conv3x3(x0, wp, ncols, bias=bias, relu=True, in1=x1, out0=out, err=err, slope=0.1)
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    x = torch.cat([x0.float()] + ([x1.float()] if c1 else []), -1).permute(0, 3, 1, 2)
+    ref = torch.nn.functional.leaky_relu(torch.nn.functional.conv2d(x, wt, b, padding=1), 0.1)
+    ok, e, m = _close(out[..., :co].permute(0, 3, 1, 2), ref)
+    assert ok, (e, m)

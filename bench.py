@@ -173,9 +173,13 @@ def gpu_arm(args, rank, world, local_rank):
         # k_knn_bounds, k_knn_grid, k_knn_keys, radix sort (counted as one), k_knn_scatter, k_knn_start, k_knn_query
         launches_per_step += 7
 
-    def step(seed, fg_events=None, knn_events=None):
+    def step(seed, fg_events=None, knn_events=None, lmap_ready=None):
+        """One bake: photons, gather, final gather.  lmap_ready: an event the
+        lightmap's inputs land on (uploaded on another stream); the lightmap is
+        then cleared and baked only after it, while photons and the gather run."""
         _abi.check(L.rl_map_clear(pmap.handle, 1, 1, sh))
-        _abi.check(L.rl_map_clear(lmap.handle, 1, 0, sh))
+        if lmap_ready is None:
+            _abi.check(L.rl_map_clear(lmap.handle, 1, 0, sh))
         if split:
             parallel.emit_photons_distributed(rl, w.scene, st, seed)
             if fg_events:
@@ -199,6 +203,9 @@ def gpu_arm(args, rank, world, local_rank):
             records.gather_knn(pmap, 0, KNN_K, KNN_RADIUS, sh)
             if knn_events:
                 knn_events[1].record(stream)
+        if lmap_ready is not None:
+            stream.wait_event(lmap_ready)
+            _abi.check(L.rl_map_clear(lmap.handle, 1, 0, sh))
         if fg_events:
             fg_events[0].record(stream)
         _abi.check(L.rl_bake_indirect(ds.handle, lmap.handle, maps, 1, st.final_gather_samples,
@@ -253,14 +260,23 @@ def gpu_arm(args, rank, world, local_rank):
     h2d = sum(t.numel() * t.element_size() for t in pin.values())
     d2h = out_color.numel() * 4
 
+    # the lightmap's inputs go up on a second stream while the photonmap's
+    # inputs, the photons and the gather run on the first; the final gather
+    # waits for them (every copy still lies between the step's two events)
+    side = torch.cuda.Stream(device=dev)
+
     def e2e_step(seed):
+        started, lmap_ready = torch.cuda.Event(), torch.cuda.Event()
+        started.record(stream)
+        side.wait_event(started)
         _abi.check(L.rl_map_upload(lmap.handle, C.c_void_p(pin["lflags"].data_ptr()), None,
                                    C.c_void_p(pin["lposition"].data_ptr()), C.c_void_p(pin["lnormal"].data_ptr()),
-                                   None, None, None, sh))
+                                   None, None, None, C.c_void_p(side.cuda_stream)))
+        lmap_ready.record(side)
         _abi.check(L.rl_map_upload(pmap.handle, C.c_void_p(pin["pflags"].data_ptr()), None,
                                    C.c_void_p(pin["pposition"].data_ptr()), C.c_void_p(pin["pnormal"].data_ptr()),
                                    None, None, None, sh))
-        step(seed)
+        step(seed, lmap_ready=lmap_ready)
         _abi.check(L.rl_map_download(lmap.handle, None, None, None, None, C.c_void_p(out_color.data_ptr()), None,
                                      None, sh))
 

@@ -1994,6 +1994,10 @@ extern "C" int rl_ff_hemisphere_device(const rl_scene* s, int n, const float* d_
 // unused ([n][4], one 16-byte gather, kB = 1).
 template <int kB>
 __device__ __forceinline__ float3 patch_b(const float* __restrict__ B, int c) {
+    if (kB == 2) {  // [n][3] staged in shared memory
+        const float* x = B + 3 * (size_t)c;
+        return make_float3(x[0], x[1], x[2]);
+    }
     if (kB == 1) {
         const float4 v = __ldg(reinterpret_cast<const float4*>(B) + c);
         return make_float3(v.x, v.y, v.z);
@@ -2128,6 +2132,77 @@ __global__ void k_jacobi4(int n, const int64_t* row_ptr, const int32_t* cols, co
     }
 }
 
+// k_jacobi4 with the whole iterate staged in shared memory as [n][3] floats
+// (12 n bytes: up to kJacobiSmemPatches patches) by every block, the blocks
+// then taking rows blockIdx.x * warps + warp, + gridDim.x * warps, ...  The
+// column gathers (one per nonzero, scattered over the iterate) then read
+// shared memory instead of 32-byte L2 sectors; the row arithmetic is
+// k_jacobi4's, so the bits are the same.
+constexpr int kJacobiSmemPatches = (224 * 1024) / 12;
+template <bool kQuads>
+__global__ void __launch_bounds__(1024, 1) k_jacobi4_smem(int n, const int64_t* row_ptr, const int32_t* cols,
+                                                          const float* vals, const float* E, const float* rho,
+                                                          const float4* B, float4* Bn) {
+    extern __shared__ float sb[];
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const float4 v = __ldg(B + i);
+        sb[3 * i] = v.x;
+        sb[3 * i + 1] = v.y;
+        sb[3 * i + 2] = v.z;
+    }
+    __syncthreads();
+    const int warps = blockDim.x >> 5, lane = threadIdx.x & 31;
+    for (int row = blockIdx.x * warps + (threadIdx.x >> 5); row < n; row += gridDim.x * warps) {
+        float s0, s1, s2;
+        if (kQuads)
+            row_dot3_quads<2>(row_ptr[row], row_ptr[row + 1], lane, cols, vals, sb, s0, s1, s2);
+        else
+            row_dot3<2>(row_ptr[row], row_ptr[row + 1], lane, cols, vals, sb, s0, s1, s2);
+        if (lane == 0) {
+            size_t i = 3 * (size_t)row;
+            Bn[row] = make_float4(__fmaf_rn(rho[i], s0, E[i]), __fmaf_rn(rho[i + 1], s1, E[i + 1]),
+                                  __fmaf_rn(rho[i + 2], s2, E[i + 2]), 0.f);
+        }
+    }
+}
+
+// One Jacobi step of rl_radiosity_solve (and its no-allocation form): the
+// shared-memory kernel when the iterate fits, else k_jacobi4.
+static int jacobi4_step(int n, const int64_t* row_ptr, const int32_t* cols, const float* vals, const float* E,
+                 const float* rho, const float4* B, float4* Bn, cudaStream_t st) {
+    const bool quads = ((uintptr_t)cols % 16) == 0 && ((uintptr_t)vals % 16) == 0;
+    if (n <= kJacobiSmemPatches) {
+        static int sms = 0;
+        static std::once_flag once;
+        cudaError_t ae = cudaSuccess;
+        std::call_once(once, [&] {
+            ae = cudaFuncSetAttribute(k_jacobi4_smem<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+            if (ae == cudaSuccess)
+                ae = cudaFuncSetAttribute(k_jacobi4_smem<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          227 * 1024);
+            int dev = 0;
+            if (ae == cudaSuccess) ae = cudaGetDevice(&dev);
+            if (ae == cudaSuccess) ae = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        });
+        if (ae != cudaSuccess) return fail(RL_CUDA_ERROR, "jacobi set-up: %s", cudaGetErrorString(ae));
+        const int grid = std::max(1, std::min(sms, (n + 31) / 32));
+        const size_t smem = 12 * (size_t)n;
+        if (quads)
+            k_jacobi4_smem<true><<<grid, 1024, smem, st>>>(n, row_ptr, cols, vals, E, rho, B, Bn);
+        else
+            k_jacobi4_smem<false><<<grid, 1024, smem, st>>>(n, row_ptr, cols, vals, E, rho, B, Bn);
+        CK_LAUNCH("k_jacobi4_smem");
+        return RL_OK;
+    }
+    const unsigned grid = blocks_for((long long)n * 32, 256);
+    if (quads)
+        k_jacobi4<true><<<grid, 256, 0, st>>>(n, row_ptr, cols, vals, E, rho, B, Bn);
+    else
+        k_jacobi4<false><<<grid, 256, 0, st>>>(n, row_ptr, cols, vals, E, rho, B, Bn);
+    CK_LAUNCH("k_jacobi4");
+    return RL_OK;
+}
+
 // [n][3] <-> [n][4] (w = 0).
 __global__ void k_pack4(int n, const float* src, float4* dst) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -2202,14 +2277,8 @@ extern "C" int rl_radiosity_solve(int n, const int64_t* d_row_ptr, const int32_t
     if (rc) return rc;
     k_pack4<<<blocks_for(n, 256), 256, 0, st>>>(n, d_E, src);
     CK_LAUNCH("k_pack4");
-    unsigned grid = blocks_for((long long)n * 32, 256);
-    const bool quads = ((uintptr_t)d_cols % 16) == 0 && ((uintptr_t)d_vals % 16) == 0;
     for (int it = 0; it < iters; it++) {
-        if (quads)
-            k_jacobi4<true><<<grid, 256, 0, st>>>(n, d_row_ptr, d_cols, d_vals, d_E, d_rho, src, dst);
-        else
-            k_jacobi4<false><<<grid, 256, 0, st>>>(n, d_row_ptr, d_cols, d_vals, d_E, d_rho, src, dst);
-        CK_LAUNCH("k_jacobi4");
+        if (int rc2 = jacobi4_step(n, d_row_ptr, d_cols, d_vals, d_E, d_rho, src, dst, st)) return rc2;
         std::swap(src, dst);
     }
     k_unpack4<<<blocks_for(n, 256), 256, 0, st>>>(n, src, d_B);
@@ -3026,14 +3095,8 @@ extern "C" int rl_radiosity_solve_noalloc(int n, const int64_t* d_row_ptr, const
     float4* dst = scratch_base + RL_SOLVE_NOALLOC_MAX_PATCHES;
     k_pack4<<<blocks_for(n, 256), 256, 0, st>>>(n, d_E, src);
     CK_LAUNCH("k_pack4");
-    unsigned grid = blocks_for((long long)n * 32, 256);
-    const bool quads = ((uintptr_t)d_cols % 16) == 0 && ((uintptr_t)d_vals % 16) == 0;
     for (int it = 0; it < iters; it++) {
-        if (quads)
-            k_jacobi4<true><<<grid, 256, 0, st>>>(n, d_row_ptr, d_cols, d_vals, d_E, d_rho, src, dst);
-        else
-            k_jacobi4<false><<<grid, 256, 0, st>>>(n, d_row_ptr, d_cols, d_vals, d_E, d_rho, src, dst);
-        CK_LAUNCH("k_jacobi4");
+        if (int rc2 = jacobi4_step(n, d_row_ptr, d_cols, d_vals, d_E, d_rho, src, dst, st)) return rc2;
         std::swap(src, dst);
     }
     k_unpack4<<<blocks_for(n, 256), 256, 0, st>>>(n, src, d_B);

@@ -1152,7 +1152,7 @@ def radiosity_arm(args):
         "e2e": {"value": e2e_value, "unit": "Grays/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": sum(e2e_ms) / steps,
                 "note": "patch positions and normals, E and rho up from pinned memory; form factors and solve; B down"},
-        "roofline": {"kernel": "k_jacobi4 (50 iterations)", "bound": jac_bound, "achieved": achieved,
+        "roofline": {"kernel": "k_jacobi4_smem (50 iterations; the iterate staged in shared memory per block)", "bound": jac_bound, "achieved": achieved,
                      "peak": l2.value if jac_bound == "l2" else peak, "unit": "GB/s",
                      "frac": achieved / (l2.value if jac_bound == "l2" else peak),
                      "peak_source": ("L2 read bandwidth measured in this run by the library's probe "

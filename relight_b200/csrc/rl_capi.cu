@@ -600,7 +600,7 @@ static int device_pool(cudaMemPool_t* out) {
 }
 
 static int pool_alloc(void** p, size_t bytes, cudaStream_t st) {
-    cudaMemPool_t pool;
+    cudaMemPool_t pool = nullptr;
     if (int rc = device_pool(&pool)) return rc;
     cudaError_t e = cudaMallocFromPoolAsync(p, bytes, pool, st);
     if (e != cudaSuccess)
@@ -612,14 +612,14 @@ static int pool_alloc(void** p, size_t bytes, cudaStream_t st) {
 int rl_internal_pool_alloc(void** p, size_t bytes, cudaStream_t st) { return pool_alloc(p, bytes, st); }
 
 extern "C" int rl_pool_trim(int64_t keep_bytes) {
-    cudaMemPool_t pool;
+    cudaMemPool_t pool = nullptr;
     if (int rc = device_pool(&pool)) return rc;
     CK(cudaMemPoolTrimTo(pool, keep_bytes < 0 ? 0 : (size_t)keep_bytes));
     return RL_OK;
 }
 
 extern "C" int rl_pool_bytes(int64_t* reserved, int64_t* used) {
-    cudaMemPool_t pool;
+    cudaMemPool_t pool = nullptr;
     if (int rc = device_pool(&pool)) return rc;
     uint64_t r = 0, u = 0;
     CK(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &r));

@@ -923,12 +923,18 @@ extern "C" int rl_dn_conv3x3(const void* in0, int c0, const void* in1, int c1, i
         a.hstages = (int)std::min<long long>(8, (budget - 9 * tap) / halo);
     } else {
         a.resident = 0;
-        a.hstages = budget - 3 * halo >= 3 * tap ? 3 : 2;
+        // with at most four tiles per SM there is little halo load to hide:
+        // one halo stage leaves room for twice the weight bytes in flight,
+        // which is what bounds these layers (measured on the 128 + 96 -> 96
+        // layer at 256^2: 77 -> 52 us)
+        const long long tiles = (long long)((width + 7) / 8) * ((height + 15) / 16) * images;
+        const bool few = tiles <= 4LL * 148;
+        a.hstages = few ? 1 : (budget - 3 * halo >= 3 * tap ? 3 : 2);
         const long long rem = budget - a.hstages * halo;
         a.kgroup = nk16;
         while (a.kgroup > 1 && rem / (a.kgroup * step) < 4) a.kgroup = (a.kgroup + 1) / 2;
         a.ngroups = (nk16 + a.kgroup - 1) / a.kgroup;
-        a.bslots = (int)std::min<long long>(8, rem / (a.kgroup * step));
+        a.bslots = (int)std::min<long long>(few ? 16 : 8, rem / (a.kgroup * step));
         if (a.bslots < 2)
             return dn_fail(RL_INVALID_CALL, "rl_dn_conv3x3: %d input and %d output channels exceed shared memory",
                            c0 + (in1 ? c1 : 0), ncols);

@@ -216,8 +216,8 @@ __device__ __forceinline__ uint8_t* align1024(uint8_t* p) {
 //   warps 2-5 the epilogue (warp w owns TMEM lanes 32 (w % 4) .. +31), which
 //             drains accumulator set i % nbuf while the issuers fill the others;
 //   warps 6-9 the MMA issuers (lane 0 of each; warp 6 + k is issuer k);
-//   warps 10-13 a second epilogue group when there are two accumulator sets:
-//             groups 0 and 1 take the even and odd tiles.
+//   warps 10-13 a second epilogue group when there are two or more
+//             accumulator sets: groups 0 and 1 take the even and odd tiles.
 
 constexpr int kTileW = 16, kTileH = 8;    // the weight gradient's pixel tile: 128 pixels
 constexpr uint32_t kABytes = 128 * 128;   // 128 pixels x 64 channels x 2 bytes
